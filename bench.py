@@ -1,0 +1,297 @@
+"""Benchmark of the B200 H*psi sweep (RSPACE kukan hot path).
+
+Workload (Si512): 4x4x4 diamond supercell of silicon, a = 41.04 bohr, 128^3
+grid (h = 0.3206 bohr), 512 atoms jittered by sigma = 0.05 bohr (seed 4),
+1100 bands, Si PAW projector tables (12 projectors per atom), FP32 psi.  One
+step applies the fused H (stencil + veff + nonlocal D term, with stored
+<p|psi>) to all 1100 bands -- kukan's rayleighritz_hamiltonian sweep.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  --impl reference times the CPU oracle (the
+FP64 restatement of kukan's loops) on this host's cores on a bounded sample
+of the same sweep.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NB = 1100
+GRID = 128
+A_SI = 10.26
+NCELL = 4
+SIGMA, SEED = 0.05, 4
+E2E_BANDS = 128
+CPU_SAMPLE_BANDS = None  # one band per host thread (4..64)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_cell():
+    from rspacedist_b200 import system as S
+    ds = S.load_dataset("si_paw")
+    pos = S.diamond_positions(NCELL, A_SI, SIGMA, SEED)
+    return S.make_cell(NCELL * A_SI, GRID, pos, ds)
+
+
+def algorithmic_bytes(cell, nb, entries, s=4, s_p=4):
+    """Bytes a perfect H*psi sweep must move: psi read + hpsi write, veff,
+    the nonzero projector entries (values + atom index) and the inverse-list
+    offsets, each once per call."""
+    N = cell.N
+    return N * nb * 2 * s + N * s + entries * (cell.nprjmx * s_p + 4) + (N + 1) * 4
+
+
+def measured_peak():
+    for p in (os.path.join(ROOT, "MEASURED_PEAKS.json"),):
+        if os.path.exists(p):
+            d = json.load(open(p))
+            return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for nm, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    from rspacedist_b200 import kukan as K
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+
+    t0 = time.time()
+    cell = make_cell()
+    g = K.Geometry(cell)
+    log(f"[rank {rank}] set-up {time.time() - t0:.1f}s  entries={g.entries} "
+        f"num_list={cell.num_list} natinf={int(cell.natinf.mean())}")
+    from rspacedist_b200 import system as S
+    veff = torch.tensor(S.smooth_veff(cell, 1), dtype=torch.float32, device=dev)
+    dij = torch.tensor(cell.dij, dtype=torch.float64, device=dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    psi = torch.randn((NB, cell.N), generator=gen, dtype=torch.float32, device=dev) * 0.1
+    rp = K.nonlocaloperation_01(g, psi)
+    hpsi = torch.empty_like(psi)
+    nbytes = algorithmic_bytes(cell, NB, g.entries)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        K.hpsi(g, veff, dij, rp, psi, out=hpsi)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+        dist.barrier()
+    value = nbytes * world / (ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    kernel_gbs = nbytes / (ms * 1e-3) / 1e9
+
+    # end to end through the host-buffer entry point (pinned host psi/hpsi)
+    hin = psi[:E2E_BANDS].cpu().pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    rp_e = rp[:E2E_BANDS].contiguous()
+    for _ in range(2):
+        K.hpsi_host(g, veff, dij, rp_e, hin, hout, chunk=32)
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    e2e_steps = max(3, min(args.steps, 10))
+    for _ in range(e2e_steps):
+        K.hpsi_host(g, veff, dij, rp_e, hin, hout, chunk=32)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - e0) / e2e_steps
+    e2e_bytes = algorithmic_bytes(cell, E2E_BANDS, g.entries)
+    e2e_gbs = e2e_bytes / e2e_s / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(cell, NB)
+    if rank == 0:
+        out = {
+            "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi; SCF-time part of the metric not yet measured)",
+            "value": round(value, 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Si512 geometry, random psi, synthetic smooth veff)",
+            "config": {"workload": "Si512 H*psi sweep: 128^3 grid, 1100 bands, 512 Si atoms "
+                                   "x 12 projectors, FP32 psi, stored <p|psi>",
+                       "grid": [GRID] * 3, "bands": NB, "atoms": cell.natom,
+                       "projectors": cell.nprjmx, "inverse_entries": g.entries,
+                       "l2": "inputs (9.2 GB psi) larger than L2; no flush",
+                       "parallelism": f"bands replicated per GPU x{world}"},
+            "band_points_per_s": round(NB * cell.N * world / (ms * 1e-3), 1),
+            "roofline": {"bound": "hbm", "achieved": round(kernel_gbs, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(kernel_gbs / peak, 4),
+                         "traffic": None, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": nbytes},
+            "e2e": {"value": round(e2e_gbs, 2), "unit": "GB/s",
+                    "h2d_bytes_per_step": int(hin.numel() * 4),
+                    "d2h_bytes_per_step": int(hout.numel() * 4),
+                    "bands": E2E_BANDS, "entry_point": "rs_hpsi_host_f32"},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clk.summary(),
+        }
+        if cpu:
+            out["cpu_baseline"] = cpu
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(cell, nb_full, nthreads=None, nbands=CPU_SAMPLE_BANDS):
+    """Times the oracle's threaded FP64 H*psi on a few bands of the same cell;
+    reports the sweep-equivalent GB/s (FP32 algorithmic bytes of the full
+    1100-band sweep over the extrapolated sweep time)."""
+    from oracle import oracle as O
+    nthreads = nthreads or os.cpu_count()
+    if nbands is None:
+        nbands = max(4, min(64, nthreads))
+    geo = dict(natom=cell.natom, nprjmx=cell.nprjmx, num_list=cell.num_list, nprj=cell.nprj,
+               natinf=cell.natinf, lst=cell.lst, v=cell.vnlocp.ravel())
+    from rspacedist_b200 import system as S
+    veff = S.smooth_veff(cell, 1)
+    sysk = O.make_sys(geo, cell.shape, 4, cell.h, veff, cell.dij, cell.sss)
+    psi = np.random.default_rng(0).standard_normal((nbands, cell.N)) * 0.1
+    rp = np.zeros((nbands, cell.natom, cell.nprjmx))
+    O.hpsi_fast(sysk, psi[:1], rp[:1], 1)
+    t0 = time.perf_counter()
+    O.hpsi_fast(sysk, psi, rp, nthreads)
+    dt = time.perf_counter() - t0
+    sweep_s = dt / nbands * nb_full
+    entries = int(sum(int(n) for n in cell.natinf))
+    byts = algorithmic_bytes(cell, nb_full, entries)
+    return {"value": round(byts / sweep_s / 1e9, 3), "unit": "GB/s", "cores": nthreads,
+            "kind": "port",
+            "sample": f"{nbands} of {nb_full} bands of the Si512 sweep (FP64 oracle H*psi, "
+                      f"{dt:.1f} s), extrapolated to the full sweep",
+            "sweep_seconds": round(sweep_s, 2)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cell = make_cell()
+    vals = []
+    for _ in range(min(args.warmup, 1)):
+        cpu_baseline(cell, NB)
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(cell, NB))
+    v = statistics.mean(x["value"] for x in vals)
+    sweep_s = statistics.mean(x["sweep_seconds"] for x in vals)
+    cores = vals[0]["cores"]
+    print(json.dumps({
+        "impl": "reference",
+        "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi; SCF-time part of the metric not yet measured)",
+        "value": round(v, 3), "unit": "GB/s", "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(sweep_s * 1e3, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Si512 geometry)",
+        "config": {"workload": "Si512 H*psi sweep: 128^3 grid, 1100 bands, 512 Si atoms x 12 "
+                               "projectors; CPU oracle (FP64 restatement of kukan's loops)"},
+        "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": cores, "kind": "port",
+                         "sample": vals[0]["sample"]},
+        "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

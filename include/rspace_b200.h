@@ -1,0 +1,134 @@
+/*
+ * rspace_b200.h -- C ABI of the B200 (sm_100a) replacement for RSPACE kukan's
+ * real-space Kohn-Sham hot path.
+ *
+ * Conventions (all entry points):
+ *   - every function returns RS_OK (0) or a negative RS_E* status; the message
+ *     of the last failure on the calling thread is read with rs_last_error();
+ *   - arrays marked (dev) are device pointers, (host) host pointers;
+ *   - grid arrays are x-fastest, column-major like kukan's
+ *     svecre(ncpx,ncpy,ncpz,neigmx); band b of a band array starts at b*N;
+ *   - <p|psi> arrays are rp[(b*natom + a)*nprjmx + j] (rspsep layout);
+ *   - D / S matrices are m[(a*nprjmx + i)*nprjmx + j] == dij(j,i,a);
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy stream);
+ *   - the library computes on one GPU, the current device of the caller.
+ * Reference files are cited relative to RSPACEes.v08.01/kukan/.
+ */
+#ifndef RSPACE_B200_H
+#define RSPACE_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RS_OK 0
+#define RS_EINVAL (-1)   /* bad argument (reference: stopp with a message) */
+#define RS_ECUDA (-2)    /* CUDA runtime error */
+#define RS_ENOMEM (-3)   /* device allocation failed */
+#define RS_ENOCONV (-4)  /* iteration limit reached without convergence */
+#define RS_ENUMERIC (-5) /* negative norm / failed eigensolve (kukan stopp) */
+
+typedef struct rs_geom rs_geom;
+
+/* Copies the message of the last failure on this thread into buf. */
+int rs_last_error(char* buf, int len);
+/* Library version string, e.g. "rspace_b200 0.1 sm_100a". */
+const char* rs_version(void);
+
+/* ---- geometry: sphere lists + projector tables ------------------------- */
+/* Replaces the list-vector part of pseudocalc_01b (pseudocalc8f.F90:955-1033)
+ * for one rank and nperi=3.  rcut[a] = radial(nradct)*psctoff.  Writes natx..
+ * (host, natom each), natinf (host, natom), lst/lstx/lsty/lstz (host,
+ * natom*num_list, lst 0-based point index).  RS_EINVAL if num_list is too
+ * small ("num_list is too small", pseudocalc8f.F90:1025-1028). */
+int rs_sphere_lists(int natom, const double* atx, const double* aty, const double* atz,
+                    const double* rcut, int nxmax, int nymax, int nzmax, double dx,
+                    double dy, double dz, int npxmax, int npymax, int npzmax, int nfdg,
+                    int num_list, int* natx, int* naty, int* natz, int* natinf, int* lst,
+                    int* lstx, int* lsty, int* lstz);
+
+/* Uploads the grid, the sphere lists and vnlocp (host, vnlocp(num_list,
+ * nprjmx,natom) layout) and builds the point-major inverse lists used by the
+ * fused H*psi.  Stands for the geometry arguments kukan threads through
+ * kslaplacian_r / nonlocaloperation_r_0x (nonlocaloperation8f.F90:9-235). */
+int rs_geom_create(rs_geom** g, int nx, int ny, int nz, int nf, double dx, double dy,
+                   double dz, int natom, int nprjmx, int num_list, const int* nprj,
+                   const int* natinf, const int* lst, const double* vnlocp);
+int rs_geom_destroy(rs_geom* g);
+/* number of inverse-list entries (sum of natinf) */
+long rs_geom_entries(const rs_geom* g);
+
+/* ---- H*psi pieces (FP64 = bit-exact with the strict oracle) ------------- */
+/* out(dev) += (-1/2 lap_FD + veff) psi for nb bands: kslaplacian_r
+ * (kslaplacian8f.F90:23-261, nf=4 at 207-261) with the periodic halo of
+ * overlap_finitedifference_r (overlap_finitedifference8f.F90:97-139). */
+int rs_kslaplacian_f64(const rs_geom* g, const double* psi, const double* veff, double* out,
+                       int nb, void* stream);
+int rs_kslaplacian_f32(const rs_geom* g, const float* psi, const float* veff, float* out,
+                       int nb, void* stream);
+
+/* rp(dev) = <p_j,a|psi_b>: nonlocaloperation_r_01 (nonlocaloperation8f.F90:9-53)
+ * over nb bands.  FP64: one sequential fma chain per (atom, projector, band).
+ * FP32 psi: FP64 accumulation, rp in FP64. */
+int rs_nonlocal_dot_f64(const rs_geom* g, const double* psi, int nb, double* rp, void* stream);
+int rs_nonlocal_dot_f32(const rs_geom* g, const float* psi, int nb, double* rp, void* stream);
+
+/* out(dev) += sum_a p_a (mat_a rp_a)/dV over nb bands: nonlocaloperation_r_02
+ * (nonlocaloperation8f.F90:149-235); mat = dij (nhs=1) or sss (nhs=0). */
+int rs_nonlocal_apply_f64(const rs_geom* g, const double* mat, const double* rp, int nb,
+                          double* out, void* stream);
+
+/* Fused H psi = nonlocal(D) + stencil + veff, one pass over psi (the H*psi of
+ * kscg8f.F90:147-183 and rayleighritz_hamiltonian_r, rayleigh-ritz8f.F90:493-575).
+ * hpsi(dev) is overwritten. */
+int rs_hpsi_f64(const rs_geom* g, const double* veff, const double* dij, const double* rp,
+                const double* psi, double* hpsi, int nb, void* stream);
+int rs_hpsi_f32(const rs_geom* g, const float* veff, const double* dij, const double* rp,
+                const float* psi, float* hpsi, int nb, void* stream);
+/* S psi = psi + nonlocal(sss) (orthogonalization8f.F90:187-210, nhs=0). */
+int rs_spsi_f64(const rs_geom* g, const double* sss, const double* rp, const double* psi,
+                double* spsi, int nb, void* stream);
+int rs_spsi_f32(const rs_geom* g, const double* sss, const double* rp, const float* psi,
+                float* spsi, int nb, void* stream);
+
+/* H psi through host buffers (host psi in, host hpsi out), staged through the
+ * device in band chunks with copies overlapping compute: the drop-in for a
+ * Fortran caller holding svecre/hsvre in host memory. */
+int rs_hpsi_host_f32(const rs_geom* g, const float* veff_dev, const double* dij_dev,
+                     const double* rp_dev, const float* psi_host, float* hpsi_host, int nb,
+                     int chunk, void* stream);
+
+/* ksprecondition (ksprecondition8f.F90:8-39): out = psi/2 + sum_6 nbr/12. */
+int rs_precondition_f64(const rs_geom* g, const double* in, double* out, int nb, void* stream);
+int rs_precondition_f32(const rs_geom* g, const float* in, float* out, int nb, void* stream);
+
+/* ---- density / interpolation / Hartree ---------------------------------- */
+/* scf_charge_smt_r (scf_charge8f.F90:290-321): rho(dev) = sum_b occ_b psi_b^2,
+ * bands accumulated in order.  occ(dev). */
+int rs_density_f64(long N, int nb, const double* occ, const double* psi, double* rho,
+                   void* stream);
+int rs_density_f32(long N, int nb, const double* occ, const float* psi, double* rho,
+                   void* stream);
+/* trans_c2d_smtcharge + interpolation, forward branch, nmesh=2
+ * (trans8f.F90:8-47, interpolation8f.F90:8-100): out(dev) has 8*nx*ny*nz. */
+int rs_interp_c2d(int nx, int ny, int nz, int nf, const double* in, double* out,
+                  void* stream);
+/* scf_hartee_laplacian (scf_hartree8f.F90:901-1004): av = -1/2 lap v. */
+int rs_hartree_laplacian(int nx, int ny, int nz, int nfh, double ddx, double ddy, double ddz,
+                         const double* v, double* av, void* stream);
+/* scf_hartree + scf_hartree_cg for nperi=3 (scf_hartree8f.F90:84-89, 626-812):
+ * CG on -1/2 lap V = 2 pi (rho - mean), warm start from vh(dev, in/out).
+ * Work vectors come from a stream-ordered device allocation.  iters/dp
+ * (host) receive the iteration count and final residual. */
+int rs_hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double zmax,
+                  double epsvh, int ncgmin, int ncgmax, int ncgres, const double* rho,
+                  double* vh, int* iters, double* dp, void* stream);
+
+/* ---- fixed-tree reductions (shared order with the oracle) --------------- */
+/* out(dev, 1 double) = sum_i a_i b_i in the documented block tree. */
+int rs_dot_f64(long n, const double* a, const double* b, double* out, void* stream);
+int rs_dot_f32(long n, const float* a, const float* b, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,317 @@
+// density.cu -- density build, coarse->dense interpolation, fixed-tree dot
+// products and the Hartree CG Poisson solve.
+#include <math.h>
+
+#include <vector>
+
+#include "reduce.cuh"
+#include "rs_common.cuh"
+#include "stencil.cuh"
+
+namespace rs {
+
+// ------------------------------------------------------------ tree dot
+template <class T>
+__global__ void k_tree_partial(long n, const T* __restrict__ a, const T* __restrict__ b,
+                               double* __restrict__ part) {
+  __shared__ double ws[8];
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < kTreePerLane; ++k) {
+    const long i = base + (long)k * kTreeLanes;
+    if (i < n) acc = fma((double)a[i], (double)b[i], acc);
+  }
+  const double s = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// folds nblk chunk sums; scale multiplies the result (scale==1 leaves it exact)
+__global__ void k_tree_final(long nblk, const double* __restrict__ part, double* __restrict__ out) {
+  __shared__ double ws[8];
+  double acc = 0.0;
+  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + part[k];
+  const double s = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) *out = s;
+}
+
+template <class T>
+int tree_dot(long n, const T* a, const T* b, double* out, double* part, cudaStream_t st) {
+  const long nblk = tree_chunks(n);
+  if (nblk == 0) {
+    RS_CUDA(cudaMemsetAsync(out, 0, sizeof(double), st));
+    return RS_OK;
+  }
+  k_tree_partial<T><<<(unsigned)nblk, kTreeLanes, 0, st>>>(n, a, b, part);
+  k_tree_final<<<1, kTreeLanes, 0, st>>>(nblk, part, out);
+  RS_LAUNCH_CHECK("tree_dot");
+  return RS_OK;
+}
+template int tree_dot<double>(long, const double*, const double*, double*, double*, cudaStream_t);
+template int tree_dot<float>(long, const float*, const float*, double*, double*, cudaStream_t);
+
+// ------------------------------------------------------------ density
+// scf_charge_smt_r (scf_charge8f.F90:309-319): rho = rho + (f*psi)*psi over
+// bands in order, one thread per point.
+template <class T>
+__global__ void k_density(long N, int nb, const double* __restrict__ occ,
+                          const T* __restrict__ psi, double* __restrict__ rho) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  double r = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    const double x = (double)__ldg(psi + (long)b * N + p);
+    r = fma(__ldg(occ + b) * x, x, r);
+  }
+  rho[p] = r;
+}
+
+// ------------------------------------------------------------ interpolation
+struct InterpW {
+  double w[2][16];
+};
+
+// One separable pass of interpolation8f.F90:56-95 (forward, nmesh=2): the
+// output axis `axis` is doubled; dense index jd takes coarse base
+// (jd+1)/2 - 1 and weight row (jd+1) mod 2.
+__global__ void k_interp_pass(int nxo, int nyo, int nzo, int nxi, int nyi, int nzi, int axis,
+                              int nf, InterpW W, const double* __restrict__ in,
+                              double* __restrict__ out) {
+  const long No = (long)nxo * nyo * nzo;
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= No) return;
+  const int jx = (int)(q % nxo), jy = (int)((q / nxo) % nyo), jz = (int)(q / ((long)nxo * nyo));
+  const int jd = axis == 0 ? jx : (axis == 1 ? jy : jz);
+  const int k = (jd + 1) % 2, l0 = (jd + 1) / 2 - 1;
+  const int n = axis == 0 ? nxi : (axis == 1 ? nyi : nzi);
+  double acc = 0.0;
+  for (int i = -nf + 1; i <= nf; ++i) {
+    const int c = (int)wrapi(l0 + i, n);
+    long src;
+    if (axis == 0) src = ((long)jz * nyi + jy) * nxi + c;
+    else if (axis == 1) src = ((long)jz * nyi + c) * nxi + jx;
+    else src = ((long)c * nyi + jy) * nxi + jx;
+    acc = fma(W.w[k][i + nf - 1], in[src], acc);
+  }
+  out[q] = acc;
+}
+
+static InterpW interp_weights(int nf) {
+  InterpW W;
+  for (int k = 0; k < 2; ++k) {
+    const double r = ((double)k + 0.5) * 0.5;
+    for (int j = -nf + 1; j <= nf; ++j) {
+      double w = 1.0;
+      for (int i = -nf + 1; i <= nf; ++i)
+        if (i != j) w = w * (r - (double)i) / ((double)j - (double)i);
+      W.w[k][j + nf - 1] = w;
+    }
+  }
+  return W;
+}
+
+// ------------------------------------------------------------ Hartree CG
+// Scalar steps of scf_hartree_cg kept on the device (one thread).
+struct CgScalars {
+  double r1r, pap, r2r, alph, beta, dp, bve;
+};
+
+__global__ void k_cg_alpha(CgScalars* s) { s->alph = s->r1r / s->pap; }
+
+__global__ void k_cg_beta(CgScalars* s, int loop, int ncgres, double ddx, double ddy,
+                          double ddz, double vol) {
+  double beta = s->r2r / s->r1r;
+  if (loop % ncgres == 0) beta = 0.0;
+  s->beta = beta;
+  s->dp = sqrt(s->r2r * ddx * ddy * ddz / vol);
+}
+
+__global__ void k_cg_bvec(long N, const double* __restrict__ rho, double two_pi, double ddx,
+                          double ddy, double ddz, double* __restrict__ b, double* __restrict__ q,
+                          double* __restrict__ one) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double bi = two_pi * rho[i];
+  b[i] = bi;
+  q[i] = bi * ddx * ddy * ddz;
+  one[i] = 1.0;
+}
+
+// b = b - bve/(8 xmax ymax zmax)  (scf_hartree8f.F90:667-691)
+__global__ void k_cg_neutral(long N, double* __restrict__ b, const double* __restrict__ bve,
+                             double vol) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  b[i] = b[i] - (*bve) / vol;
+}
+
+// avhs = Av, r = b - Av, p = r  (scf_hartee_cg_01 and the copies around it)
+__global__ void k_cg_init(long N, const double* __restrict__ b, const double* __restrict__ av,
+                          double* __restrict__ avhs, double* __restrict__ r,
+                          double* __restrict__ p) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  avhs[i] = av[i];
+  const double ri = b[i] - av[i];
+  r[i] = ri;
+  p[i] = ri;
+}
+
+// scf_hartee_cg_03 then the residual of scf_hartee_cg_04
+__global__ void k_cg_update(long N, const CgScalars* __restrict__ s, double* __restrict__ vh,
+                            const double* __restrict__ p, const double* __restrict__ ap,
+                            double* __restrict__ avhs, const double* __restrict__ b,
+                            double* __restrict__ r) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double alph = s->alph;
+  vh[i] = fma(alph, p[i], vh[i]);
+  const double a = fma(alph, ap[i], avhs[i]);
+  avhs[i] = a;
+  r[i] = b[i] - a;
+}
+
+// scf_hartee_cg_05: p = r + beta p
+__global__ void k_cg_dir(long N, const CgScalars* __restrict__ s, const double* __restrict__ r,
+                         double* __restrict__ p) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  p[i] = fma(s->beta, p[i], r[i]);
+}
+
+int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double zmax,
+               double epsvh, int ncgmin, int ncgmax, int ncgres, const double* rho, double* vh,
+               double* work, int* iters, double* dp_out, cudaStream_t st) {
+  const long N = (long)nx * ny * nz;
+  const long nblk = tree_chunks(N);
+  double* b = work;
+  double* r = b + N;
+  double* p = r + N;
+  double* ap = p + N;
+  double* avhs = ap + N;
+  double* part = avhs + N;
+  CgScalars* sc = (CgScalars*)(part + nblk + 1);
+  // q and one reuse r and p before the iteration starts
+  const double ddx = 2.0 * xmax / nx, ddy = 2.0 * ymax / ny, ddz = 2.0 * zmax / nz;
+  const double pi = acos(-1.0);
+  const HartreeCoefs hc = hartree_coefs(nfh, ddx, ddy, ddz);
+  const unsigned gN = div_up(N, 256);
+  int rc;
+  k_cg_bvec<<<gN, 256, 0, st>>>(N, rho, 2.0 * pi, ddx, ddy, ddz, b, r, p);
+  if ((rc = tree_dot<double>(N, r, p, &sc->bve, part, st))) return rc;
+  const double vol = 8.0 * xmax * ymax * zmax;
+  k_cg_neutral<<<gN, 256, 0, st>>>(N, b, &sc->bve, vol);
+  RS_LAUNCH_CHECK("k_cg_neutral");
+  if ((rc = launch_hartree_lap(nx, ny, nz, nfh, hc, vh, ap, st))) return rc;
+  k_cg_init<<<gN, 256, 0, st>>>(N, b, ap, avhs, r, p);
+  int loop = 0;
+  double dp = 0.0;
+  CgScalars hs;
+  for (;;) {
+    ++loop;
+    if ((rc = launch_hartree_lap(nx, ny, nz, nfh, hc, p, ap, st))) return rc;
+    if ((rc = tree_dot<double>(N, r, r, &sc->r1r, part, st))) return rc;
+    if ((rc = tree_dot<double>(N, p, ap, &sc->pap, part, st))) return rc;
+    k_cg_alpha<<<1, 1, 0, st>>>(sc);
+    k_cg_update<<<gN, 256, 0, st>>>(N, sc, vh, p, ap, avhs, b, r);
+    if ((rc = tree_dot<double>(N, r, r, &sc->r2r, part, st))) return rc;
+    k_cg_beta<<<1, 1, 0, st>>>(sc, loop, ncgres, ddx, ddy, ddz, vol);
+    k_cg_dir<<<gN, 256, 0, st>>>(N, sc, r, p);
+    RS_LAUNCH_CHECK("hartree_cg iteration");
+    RS_CUDA(cudaMemcpyAsync(&hs, sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+    RS_CUDA(cudaStreamSynchronize(st));
+    dp = hs.dp;
+    if (loop < ncgmin) continue;
+    if (loop >= ncgmax) break;
+    if (dp > epsvh) continue;
+    break;
+  }
+  if (iters) *iters = loop;
+  if (dp_out) *dp_out = dp;
+  return RS_OK;
+}
+
+}  // namespace rs
+
+extern "C" int rs_dot_f64(long n, const double* a, const double* b, double* out, void* stream) {
+  cudaStream_t st = rs::as_stream(stream);
+  const long nblk = rs::tree_chunks(n);
+  double* part = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&part, sizeof(double) * (nblk + 1), st));
+  int rc = rs::tree_dot<double>(n, a, b, out, part, st);
+  cudaFreeAsync(part, st);
+  return rc;
+}
+
+extern "C" int rs_dot_f32(long n, const float* a, const float* b, double* out, void* stream) {
+  cudaStream_t st = rs::as_stream(stream);
+  const long nblk = rs::tree_chunks(n);
+  double* part = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&part, sizeof(double) * (nblk + 1), st));
+  int rc = rs::tree_dot<float>(n, a, b, out, part, st);
+  cudaFreeAsync(part, st);
+  return rc;
+}
+
+extern "C" int rs_density_f64(long N, int nb, const double* occ, const double* psi, double* rho,
+                              void* stream) {
+  if (N <= 0 || nb < 0) return rs::fail(RS_EINVAL, "rs_density_f64: bad sizes");
+  rs::k_density<double><<<rs::div_up(N, 256), 256, 0, rs::as_stream(stream)>>>(N, nb, occ, psi,
+                                                                               rho);
+  RS_LAUNCH_CHECK("k_density");
+  return RS_OK;
+}
+
+extern "C" int rs_density_f32(long N, int nb, const double* occ, const float* psi, double* rho,
+                              void* stream) {
+  if (N <= 0 || nb < 0) return rs::fail(RS_EINVAL, "rs_density_f32: bad sizes");
+  rs::k_density<float><<<rs::div_up(N, 256), 256, 0, rs::as_stream(stream)>>>(N, nb, occ, psi,
+                                                                              rho);
+  RS_LAUNCH_CHECK("k_density");
+  return RS_OK;
+}
+
+extern "C" int rs_interp_c2d(int nx, int ny, int nz, int nf, const double* in, double* out,
+                             void* stream) {
+  if (nf < 1 || nf > 8 || nx < 2 * nf || ny < 2 * nf || nz < 2 * nf)
+    return rs::fail(RS_EINVAL, "rs_interp_c2d: bad grid or nf");
+  cudaStream_t st = rs::as_stream(stream);
+  const rs::InterpW W = rs::interp_weights(nf);
+  double *t1 = nullptr, *t2 = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&t1, sizeof(double) * 2L * nx * ny * nz, st));
+  RS_CUDA(cudaMallocAsync((void**)&t2, sizeof(double) * 4L * nx * ny * nz, st));
+  const long n1 = 2L * nx * ny * nz, n2 = 4L * nx * ny * nz, n3 = 8L * nx * ny * nz;
+  rs::k_interp_pass<<<rs::div_up(n1, 256), 256, 0, st>>>(2 * nx, ny, nz, nx, ny, nz, 0, nf, W,
+                                                         in, t1);
+  rs::k_interp_pass<<<rs::div_up(n2, 256), 256, 0, st>>>(2 * nx, 2 * ny, nz, 2 * nx, ny, nz, 1,
+                                                         nf, W, t1, t2);
+  rs::k_interp_pass<<<rs::div_up(n3, 256), 256, 0, st>>>(2 * nx, 2 * ny, 2 * nz, 2 * nx, 2 * ny,
+                                                         nz, 2, nf, W, t2, out);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(t1, st);
+  cudaFreeAsync(t2, st);
+  if (e != cudaSuccess) return rs::cuda_status(e, "k_interp_pass");
+  return RS_OK;
+}
+
+extern "C" int rs_hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax,
+                             double zmax, double epsvh, int ncgmin, int ncgmax, int ncgres,
+                             const double* rho, double* vh, int* iters, double* dp,
+                             void* stream) {
+  if (nfh < 1 || nfh > 6 || nx <= 2 * nfh || ny <= 2 * nfh || nz <= 2 * nfh)
+    return rs::fail(RS_EINVAL, "rs_hartree_cg: bad grid or nfh");
+  if (ncgres <= 0 || ncgmax <= 0) return rs::fail(RS_EINVAL, "rs_hartree_cg: bad iteration limits");
+  cudaStream_t st = rs::as_stream(stream);
+  const long N = (long)nx * ny * nz;
+  const long nblk = rs::tree_chunks(N);
+  const size_t bytes = sizeof(double) * (5 * N + nblk + 1) + 2 * sizeof(double) * 8;
+  double* work = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&work, bytes, st));
+  int rc = rs::hartree_cg(nx, ny, nz, nfh, xmax, ymax, zmax, epsvh, ncgmin, ncgmax, ncgres, rho,
+                          vh, work, iters, dp, st);
+  cudaFreeAsync(work, st);
+  if (rc == RS_OK && iters && *iters >= ncgmax && dp && *dp > epsvh) {
+    rs::set_error("rs_hartree_cg: ncgmax reached");
+  }
+  return rc;
+}

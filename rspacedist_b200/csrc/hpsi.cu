@@ -1,0 +1,82 @@
+// hpsi.cu -- mixed-precision (FP32 psi) H*psi entry points and the
+// host-buffer variant that streams band chunks through the device.
+#include "rs_common.cuh"
+#include "stencil.cuh"
+
+namespace rs {
+template <class T, int MODE>
+int launch_gather(const rs_geom* g, const double* mat, const double* rp, const T* psi,
+                  const T* veff, T* out, int nb, cudaStream_t st);
+int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
+                         const double* rp, const float* psi, float* hpsi, int nb,
+                         cudaStream_t st);
+}  // namespace rs
+
+extern "C" int rs_hpsi_f32(const rs_geom* g, const float* veff, const double* dij,
+                           const double* rp, const float* psi, float* hpsi, int nb,
+                           void* stream) {
+  if (!g) return rs::fail(RS_EINVAL, "rs_hpsi_f32: null geometry");
+  return rs::launch_hpsi_f32_fast(g, veff, dij, rp, psi, hpsi, nb, rs::as_stream(stream));
+}
+
+// Host buffers in and out.  Band chunks alternate between two device
+// buffers so that the upload of chunk k+1 and the download of chunk k-1
+// overlap the H*psi of chunk k (copy engines vs SMs).  Host arrays should be
+// pinned for the copies to run asynchronously.
+extern "C" int rs_hpsi_host_f32(const rs_geom* g, const float* veff_dev, const double* dij_dev,
+                                const double* rp_dev, const float* psi_host, float* hpsi_host,
+                                int nb, int chunk, void* stream) {
+  if (!g) return rs::fail(RS_EINVAL, "rs_hpsi_host_f32: null geometry");
+  if (nb <= 0) return RS_OK;
+  if (chunk <= 0) chunk = 64;
+  if (chunk > nb) chunk = nb;
+  cudaStream_t st = rs::as_stream(stream);
+  const long N = g->N;
+  const size_t cb = sizeof(float) * (size_t)N * chunk;
+  float* buf = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&buf, 4 * cb, st));
+  float* din[2] = {buf, buf + (size_t)N * chunk};
+  float* dout[2] = {buf + 2 * (size_t)N * chunk, buf + 3 * (size_t)N * chunk};
+  cudaStream_t cs[2];
+  cudaEvent_t ev_ready[2], ev_done[2], ev_out[2], ev_start;
+  cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming);
+  cudaEventRecord(ev_start, st);
+  for (int i = 0; i < 2; ++i) {
+    cudaStreamCreateWithFlags(&cs[i], cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&ev_ready[i], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev_done[i], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev_out[i], cudaEventDisableTiming);
+    cudaStreamWaitEvent(cs[i], ev_start, 0);
+  }
+  int rc = RS_OK;
+  int k = 0;
+  for (int b0 = 0; b0 < nb && rc == RS_OK; b0 += chunk, ++k) {
+    const int s = k & 1;
+    const int n = (b0 + chunk <= nb) ? chunk : nb - b0;
+    // the buffers of slot s are free once chunk k-2 has been downloaded
+    cudaMemcpyAsync(din[s], psi_host + (size_t)b0 * N, sizeof(float) * (size_t)N * n,
+                    cudaMemcpyHostToDevice, cs[s]);
+    // rp of this chunk starts at band b0
+    rc = rs::launch_hpsi_f32_fast(g, veff_dev, dij_dev,
+                                  rp_dev + (size_t)b0 * g->natom * g->nprjmx, din[s], dout[s],
+                                  n, cs[s]);
+    cudaMemcpyAsync(hpsi_host + (size_t)b0 * N, dout[s], sizeof(float) * (size_t)N * n,
+                    cudaMemcpyDeviceToHost, cs[s]);
+  }
+  for (int i = 0; i < 2; ++i) {
+    cudaEventRecord(ev_done[i], cs[i]);
+    cudaStreamWaitEvent(st, ev_done[i], 0);
+  }
+  cudaFreeAsync(buf, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  for (int i = 0; i < 2; ++i) {
+    cudaStreamDestroy(cs[i]);
+    cudaEventDestroy(ev_ready[i]);
+    cudaEventDestroy(ev_done[i]);
+    cudaEventDestroy(ev_out[i]);
+  }
+  cudaEventDestroy(ev_start);
+  if (rc != RS_OK) return rc;
+  if (e != cudaSuccess) return rs::cuda_status(e, "rs_hpsi_host_f32");
+  return RS_OK;
+}

@@ -1,0 +1,77 @@
+// rs_common.cuh -- shared definitions of the B200 kernels behind the
+// rspace_b200 C-ABI: status handling, the device-resident geometry (grid,
+// sphere lists, projector tables, inverse lists) and small device helpers.
+//
+// Every FP64 kernel states its floating-point evaluation order explicitly:
+// the library is compiled with --fmad=false and each fused multiply-add is an
+// explicit fma(), so results reproduce the strict CPU restatement of kukan's
+// loops bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/rspace_b200.h"
+
+namespace rs {
+
+// thread-local message for rs_last_error()
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_status(cudaError_t e, const char* what);
+
+#define RS_CUDA(call)                                          \
+  do {                                                         \
+    cudaError_t e__ = (call);                                  \
+    if (e__ != cudaSuccess) return rs::cuda_status(e__, #call); \
+  } while (0)
+
+#define RS_LAUNCH_CHECK(what)                                      \
+  do {                                                             \
+    cudaError_t e__ = cudaGetLastError();                          \
+    if (e__ != cudaSuccess) return rs::cuda_status(e__, what);     \
+  } while (0)
+
+}  // namespace rs
+
+// Device-resident geometry: everything H*psi needs that does not change
+// during an SCF iteration.  Layouts follow kukan's arrays (x fastest).
+struct rs_geom {
+  int nx, ny, nz, nf;
+  double dx, dy, dz;
+  long N;
+  int natom, nprjmx, num_list;
+  int max_prj;
+  // atom-major sphere data (nonlocaloperation_*_01 side)
+  int* d_nprj;      // [natom]
+  int* d_natinf;    // [natom]
+  int* d_lst;       // [natom*num_list] 0-based point index
+  double* d_vT64;   // [(a*num_list+ii)*nprjmx + j]
+  float* d_vT32;
+  // point-major inverse lists (nonlocaloperation_*_02 scatter as a gather):
+  // entries of point p are [inv_off[p], inv_off[p+1]) sorted by (atom, ii)
+  long n_inv;
+  int* d_inv_off;   // [N+1]
+  int* d_inv_atom;  // [n_inv]
+  double* d_inv_v64;  // [n_inv*nprjmx]
+  float* d_inv_v32;
+  int max_inv;      // longest inverse list
+  // Laplacian coefficients, computed as acfd(m)/dx/dx*(-0.5d0)
+  double cx[9], cy[9], cz[9];
+};
+
+namespace rs {
+
+__host__ __device__ inline long wrapi(long i, long n) {
+  i %= n;
+  return i < 0 ? i + n : i;
+}
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline unsigned div_up(long a, long b) { return (unsigned)((a + b - 1) / b); }
+
+void fd_coefs(int nf, double a[9]);
+
+}  // namespace rs

@@ -1,0 +1,216 @@
+// stencil.cu -- periodic FD stencils: the kinetic+local operator of
+// kslaplacian_r, the ksprecondition smoother, the Hartree Laplacian and the
+// first-derivative stencil of force_r_02/03/04.
+//
+// Periodic boundaries are handled by index wrapping inside the kernels; this
+// replaces overlap_finitedifference_r's halo copy for a single rank with
+// nperi=3 (overlap_finitedifference8f.F90:97-139, 685-710).
+#include "rs_common.cuh"
+#include "stencil.cuh"
+
+namespace rs {
+
+// One thread per grid point, bands along blockIdx.y.  Accumulation order per
+// point: x pass (including the diagonal (cx0+cy0+cz0+veff)*psi), then y, then
+// z, each term one fma -- kslaplacian8f.F90:207-261 evaluated left to right.
+template <class T>
+__global__ void k_kslaplacian(StencilArgs<T> s, const T* __restrict__ psi,
+                              const T* __restrict__ veff, T* __restrict__ out, int nb) {
+  const long N = (long)s.nx * s.ny * s.nz;
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (p >= N || b >= nb) return;
+  const int ix = (int)(p % s.nx), iy = (int)((p / s.nx) % s.ny), iz = (int)(p / ((long)s.nx * s.ny));
+  const T* v = psi + (long)b * N;
+  T acc = out[(long)b * N + p];
+  acc = stencil_point<T>(s, v, ix, iy, iz, veff[p], acc);
+  out[(long)b * N + p] = acc;
+}
+
+// ksprecondition (ksprecondition8f.F90:8-39).
+template <class T>
+__global__ void k_precondition(int nx, int ny, int nz, const T* __restrict__ in,
+                               T* __restrict__ out, int nb) {
+  const long N = (long)nx * ny * nz;
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (p >= N || b >= nb) return;
+  const int ix = (int)(p % nx), iy = (int)((p / nx) % ny), iz = (int)(p / ((long)nx * ny));
+  const T* v = in + (long)b * N;
+  const T c = (T)(1.0 / 12.0), h = (T)0.5;
+  const long row = ((long)iz * ny + iy) * nx;
+  T t = c * v[row + wrapi(ix - 1, nx)];
+  t = fma(c, v[((long)iz * ny + wrapi(iy - 1, ny)) * nx + ix], t);
+  t = fma(c, v[(wrapi(iz - 1, nz) * ny + iy) * nx + ix], t);
+  t = fma(h, v[p], t);
+  t = fma(c, v[(wrapi(iz + 1, nz) * ny + iy) * nx + ix], t);
+  t = fma(c, v[((long)iz * ny + wrapi(iy + 1, ny)) * nx + ix], t);
+  t = fma(c, v[row + wrapi(ix + 1, nx)], t);
+  out[(long)b * N + p] = t;
+}
+
+// scf_hartee_laplacian (scf_hartree8f.F90:949-1004): the x pass starts from
+// the first product; diagonal = hadx+hady+hadz with had = acfdh(0)/(d*d)*(-1/2).
+__global__ void k_hartree_lap(int nx, int ny, int nz, int nf, HartreeCoefs c,
+                              const double* __restrict__ v, double* __restrict__ av) {
+  const long N = (long)nx * ny * nz;
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const int ix = (int)(p % nx), iy = (int)((p / nx) % ny), iz = (int)(p / ((long)nx * ny));
+  const long row = ((long)iz * ny + iy) * nx;
+  double acc = c.cx[nf] * v[row + wrapi(ix - nf, nx)];
+  for (int m = nf - 1; m >= 1; --m) acc = fma(c.cx[m], v[row + wrapi(ix - m, nx)], acc);
+  acc = fma(c.diag, v[p], acc);
+  for (int m = 1; m <= nf; ++m) acc = fma(c.cx[m], v[row + wrapi(ix + m, nx)], acc);
+  for (int m = nf; m >= 1; --m) acc = fma(c.cy[m], v[((long)iz * ny + wrapi(iy - m, ny)) * nx + ix], acc);
+  for (int m = 1; m <= nf; ++m) acc = fma(c.cy[m], v[((long)iz * ny + wrapi(iy + m, ny)) * nx + ix], acc);
+  for (int m = nf; m >= 1; --m) acc = fma(c.cz[m], v[(wrapi(iz - m, nz) * ny + iy) * nx + ix], acc);
+  for (int m = 1; m <= nf; ++m) acc = fma(c.cz[m], v[(wrapi(iz + m, nz) * ny + iy) * nx + ix], acc);
+  av[p] = acc;
+}
+
+// force_r_02/03/04 (force8f.F90:468-490 for nf=4):
+// -a_nf v(+nf) ... -a_1 v(+1) + a_1 v(-1) ... + a_nf v(-nf).
+template <class T>
+__global__ void k_gradient(int nx, int ny, int nz, int nf, int axis, GradCoefs g,
+                           const T* __restrict__ psi, T* __restrict__ out, int nb) {
+  const long N = (long)nx * ny * nz;
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (p >= N || b >= nb) return;
+  const int ix = (int)(p % nx), iy = (int)((p / nx) % ny), iz = (int)(p / ((long)nx * ny));
+  const T* v = psi + (long)b * N;
+  auto at = [&](int m) -> T {
+    if (axis == 0) return v[((long)iz * ny + iy) * nx + wrapi(ix + m, nx)];
+    if (axis == 1) return v[((long)iz * ny + wrapi(iy + m, ny)) * nx + ix];
+    return v[(wrapi(iz + m, nz) * ny + iy) * nx + ix];
+  };
+  T acc = -((T)g.a[nf] * at(nf));
+  for (int m = nf - 1; m >= 1; --m) acc = fma(-(T)g.a[m], at(m), acc);
+  for (int m = 1; m <= nf; ++m) acc = fma((T)g.a[m], at(-m), acc);
+  out[(long)b * N + p] = acc;
+}
+
+template <class T>
+StencilArgs<T> make_stencil_args(const rs_geom* g) {
+  StencilArgs<T> s;
+  s.nx = g->nx; s.ny = g->ny; s.nz = g->nz; s.nf = g->nf;
+  for (int m = 0; m < 9; ++m) {
+    s.cx[m] = (T)g->cx[m]; s.cy[m] = (T)g->cy[m]; s.cz[m] = (T)g->cz[m];
+  }
+  s.c0 = (T)(g->cx[0] + g->cy[0] + g->cz[0]);
+  return s;
+}
+template StencilArgs<double> make_stencil_args<double>(const rs_geom*);
+template StencilArgs<float> make_stencil_args<float>(const rs_geom*);
+
+GradCoefs grad_coefs(int nf, double h) {
+  GradCoefs g;
+  for (int m = 0; m < 9; ++m) g.a[m] = 0.0;
+  if (nf == 1) g.a[1] = -0.5 / h;
+  if (nf == 2) { g.a[2] = 1.0 / 12.0 / h; g.a[1] = -8.0 / 12.0 / h; }
+  if (nf == 3) { g.a[3] = -1.0 / 60.0 / h; g.a[2] = 9.0 / 60.0 / h; g.a[1] = -45.0 / 60.0 / h; }
+  if (nf >= 4) {
+    g.a[4] = 3.0 / 840.0 / h; g.a[3] = -32.0 / 840.0 / h;
+    g.a[2] = 168.0 / 840.0 / h; g.a[1] = -672.0 / 840.0 / h;
+  }
+  return g;
+}
+
+HartreeCoefs hartree_coefs(int nfh, double ddx, double ddy, double ddz) {
+  double a[9];
+  fd_coefs(nfh, a);
+  HartreeCoefs c;
+  for (int m = 0; m < 9; ++m) {
+    c.cx[m] = a[m] / ddx / ddx * (-0.5);
+    c.cy[m] = a[m] / ddy / ddy * (-0.5);
+    c.cz[m] = a[m] / ddz / ddz * (-0.5);
+  }
+  const double hadx = a[0] / (ddx * ddx) * (-0.5);
+  const double hady = a[0] / (ddy * ddy) * (-0.5);
+  const double hadz = a[0] / (ddz * ddz) * (-0.5);
+  c.diag = hadx + hady + hadz;
+  return c;
+}
+
+template <class T>
+int launch_kslaplacian(const rs_geom* g, const T* psi, const T* veff, T* out, int nb,
+                       cudaStream_t st) {
+  if (nb <= 0) return RS_OK;
+  if (nb > 65535) return fail(RS_EINVAL, "kslaplacian: nb > 65535");
+  dim3 grid(div_up(g->N, 256), nb);
+  k_kslaplacian<T><<<grid, 256, 0, st>>>(make_stencil_args<T>(g), psi, veff, out, nb);
+  RS_LAUNCH_CHECK("k_kslaplacian");
+  return RS_OK;
+}
+
+template <class T>
+int launch_precondition(const rs_geom* g, const T* in, T* out, int nb, cudaStream_t st) {
+  if (nb <= 0) return RS_OK;
+  dim3 grid(div_up(g->N, 256), nb);
+  k_precondition<T><<<grid, 256, 0, st>>>(g->nx, g->ny, g->nz, in, out, nb);
+  RS_LAUNCH_CHECK("k_precondition");
+  return RS_OK;
+}
+
+int launch_hartree_lap(int nx, int ny, int nz, int nfh, const HartreeCoefs& c, const double* v,
+                       double* av, cudaStream_t st) {
+  const long N = (long)nx * ny * nz;
+  k_hartree_lap<<<div_up(N, 256), 256, 0, st>>>(nx, ny, nz, nfh, c, v, av);
+  RS_LAUNCH_CHECK("k_hartree_lap");
+  return RS_OK;
+}
+
+template <class T>
+int launch_gradient(const rs_geom* g, int axis, const T* psi, T* out, int nb, cudaStream_t st) {
+  if (nb <= 0) return RS_OK;
+  const double h = axis == 0 ? g->dx : (axis == 1 ? g->dy : g->dz);
+  const int nf = g->nf > 4 ? 4 : g->nf;
+  dim3 grid(div_up(g->N, 256), nb);
+  k_gradient<T><<<grid, 256, 0, st>>>(g->nx, g->ny, g->nz, nf, axis, grad_coefs(nf, h), psi,
+                                      out, nb);
+  RS_LAUNCH_CHECK("k_gradient");
+  return RS_OK;
+}
+
+template int launch_kslaplacian<double>(const rs_geom*, const double*, const double*, double*,
+                                        int, cudaStream_t);
+template int launch_kslaplacian<float>(const rs_geom*, const float*, const float*, float*, int,
+                                       cudaStream_t);
+template int launch_precondition<double>(const rs_geom*, const double*, double*, int,
+                                         cudaStream_t);
+template int launch_precondition<float>(const rs_geom*, const float*, float*, int, cudaStream_t);
+template int launch_gradient<double>(const rs_geom*, int, const double*, double*, int,
+                                     cudaStream_t);
+template int launch_gradient<float>(const rs_geom*, int, const float*, float*, int,
+                                    cudaStream_t);
+
+}  // namespace rs
+
+extern "C" int rs_kslaplacian_f64(const rs_geom* g, const double* psi, const double* veff,
+                                  double* out, int nb, void* stream) {
+  if (!g) return rs::fail(RS_EINVAL, "rs_kslaplacian_f64: null geometry");
+  return rs::launch_kslaplacian<double>(g, psi, veff, out, nb, rs::as_stream(stream));
+}
+extern "C" int rs_kslaplacian_f32(const rs_geom* g, const float* psi, const float* veff,
+                                  float* out, int nb, void* stream) {
+  if (!g) return rs::fail(RS_EINVAL, "rs_kslaplacian_f32: null geometry");
+  return rs::launch_kslaplacian<float>(g, psi, veff, out, nb, rs::as_stream(stream));
+}
+extern "C" int rs_precondition_f64(const rs_geom* g, const double* in, double* out, int nb,
+                                   void* stream) {
+  if (!g) return rs::fail(RS_EINVAL, "rs_precondition_f64: null geometry");
+  return rs::launch_precondition<double>(g, in, out, nb, rs::as_stream(stream));
+}
+extern "C" int rs_precondition_f32(const rs_geom* g, const float* in, float* out, int nb,
+                                   void* stream) {
+  if (!g) return rs::fail(RS_EINVAL, "rs_precondition_f32: null geometry");
+  return rs::launch_precondition<float>(g, in, out, nb, rs::as_stream(stream));
+}
+extern "C" int rs_hartree_laplacian(int nx, int ny, int nz, int nfh, double ddx, double ddy,
+                                    double ddz, const double* v, double* av, void* stream) {
+  if (nx <= 2 * nfh || ny <= 2 * nfh || nz <= 2 * nfh || nfh < 1 || nfh > 6)
+    return rs::fail(RS_EINVAL, "rs_hartree_laplacian: bad grid or nfh");
+  return rs::launch_hartree_lap(nx, ny, nz, nfh, rs::hartree_coefs(nfh, ddx, ddy, ddz), v, av,
+                                rs::as_stream(stream));
+}

@@ -1,0 +1,186 @@
+"""Python mirror of kukan's hot-path subroutines, running on the B200 library.
+
+Each function carries the name of the kukan subroutine it replaces and the
+same argument meaning; arrays are torch CUDA tensors in kukan's layouts
+(x-fastest grids, band-major band arrays, rspsep-layout <p|psi>).  The calls
+go through the C ABI (rspacedist_b200.lib); torch provides device memory and
+the current CUDA stream.  Errors raise ``RsError`` with the library's
+message, the counterpart of kukan's ``stopp``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import lib as L
+from .system import Cell
+
+
+def _ptr(t):
+    return C.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _need(t, dtype, n=None, what="array"):
+    if not (t.is_cuda and t.dtype == dtype and t.is_contiguous()):
+        raise L.RsError(f"{what}: expected a contiguous CUDA {dtype} tensor")
+    if n is not None and t.numel() != n:
+        raise L.RsError(f"{what}: expected {n} elements, got {t.numel()}")
+
+
+class Geometry:
+    """Device-resident grid + sphere lists + projector tables (rs_geom)."""
+
+    def __init__(self, cell: Cell, nf: int = 4):
+        L.load()
+        self.cell = cell
+        self.nf = nf
+        h = C.c_void_p()
+        ip = lambda a: np.ascontiguousarray(a, np.int32).ctypes.data_as(C.POINTER(C.c_int))
+        self._keep = [np.ascontiguousarray(cell.nprj, np.int32),
+                      np.ascontiguousarray(cell.natinf, np.int32),
+                      np.ascontiguousarray(cell.lst, np.int32),
+                      np.ascontiguousarray(cell.vnlocp, np.float64)]
+        nprj, natinf, lst, v = self._keep
+        L.call("rs_geom_create", C.byref(h), cell.shape[0], cell.shape[1], cell.shape[2], nf,
+               cell.h[0], cell.h[1], cell.h[2], cell.natom, cell.nprjmx, cell.num_list,
+               nprj.ctypes.data_as(C.POINTER(C.c_int)),
+               natinf.ctypes.data_as(C.POINTER(C.c_int)),
+               lst.ctypes.data_as(C.POINTER(C.c_int)),
+               v.ctypes.data_as(C.POINTER(C.c_double)))
+        self.handle = h
+        self.N = cell.N
+        self.natom = cell.natom
+        self.nprjmx = cell.nprjmx
+
+    @property
+    def entries(self) -> int:
+        return int(L.load().rs_geom_entries(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            L.load().rs_geom_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _nb(g: Geometry, psi):
+    if psi.numel() % g.N:
+        raise L.RsError("band array size is not a multiple of the grid size")
+    return psi.numel() // g.N
+
+
+def kslaplacian(g: Geometry, psi, veff, out):
+    """out += (-1/2 lap + veff) psi  (kslaplacian_r)."""
+    nb = _nb(g, psi)
+    fn = "rs_kslaplacian_f64" if psi.dtype == torch.float64 else "rs_kslaplacian_f32"
+    _need(veff, psi.dtype, g.N, "veff")
+    _need(out, psi.dtype, psi.numel(), "out")
+    L.call(fn, g.handle, _ptr(psi), _ptr(veff), _ptr(out), nb, _stream())
+    return out
+
+
+def nonlocaloperation_01(g: Geometry, psi):
+    """<p|psi> for every band (nonlocaloperation_r_01), FP64 result."""
+    nb = _nb(g, psi)
+    rp = torch.empty((nb, g.natom, g.nprjmx), dtype=torch.float64, device=psi.device)
+    fn = "rs_nonlocal_dot_f64" if psi.dtype == torch.float64 else "rs_nonlocal_dot_f32"
+    L.call(fn, g.handle, _ptr(psi), nb, _ptr(rp), _stream())
+    return rp
+
+
+def nonlocaloperation_02(g: Geometry, mat, rp, out):
+    """out += sum_a p_a (mat_a rp_a)/dV  (nonlocaloperation_r_02), FP64."""
+    nb = _nb(g, out)
+    _need(out, torch.float64, what="out")
+    L.call("rs_nonlocal_apply_f64", g.handle, _ptr(mat), _ptr(rp), nb, _ptr(out), _stream())
+    return out
+
+
+def hpsi(g: Geometry, veff, dij, rp, psi, out=None):
+    """Fused H psi (nonlocal D term + stencil + veff)."""
+    nb = _nb(g, psi)
+    out = torch.empty_like(psi) if out is None else out
+    fn = "rs_hpsi_f64" if psi.dtype == torch.float64 else "rs_hpsi_f32"
+    _need(veff, psi.dtype, g.N, "veff")
+    L.call(fn, g.handle, _ptr(veff), _ptr(dij), _ptr(rp), _ptr(psi), _ptr(out), nb, _stream())
+    return out
+
+
+def spsi(g: Geometry, sss, rp, psi, out=None):
+    """S psi = psi + nonlocal(sss) term (nhs=0)."""
+    nb = _nb(g, psi)
+    out = torch.empty_like(psi) if out is None else out
+    fn = "rs_spsi_f64" if psi.dtype == torch.float64 else "rs_spsi_f32"
+    L.call(fn, g.handle, _ptr(sss), _ptr(rp), _ptr(psi), _ptr(out), nb, _stream())
+    return out
+
+
+def hpsi_host(g: Geometry, veff, dij, rp, psi_host: torch.Tensor, out_host: torch.Tensor,
+              chunk: int = 64):
+    """H psi with host (pinned) psi/hpsi buffers, FP32."""
+    nb = psi_host.numel() // g.N
+    L.call("rs_hpsi_host_f32", g.handle, _ptr(veff), _ptr(dij), _ptr(rp), _ptr(psi_host),
+           _ptr(out_host), nb, chunk, _stream())
+    return out_host
+
+
+def ksprecondition(g: Geometry, x, out=None):
+    nb = _nb(g, x)
+    out = torch.empty_like(x) if out is None else out
+    fn = "rs_precondition_f64" if x.dtype == torch.float64 else "rs_precondition_f32"
+    L.call(fn, g.handle, _ptr(x), _ptr(out), nb, _stream())
+    return out
+
+
+def scf_charge_smt(occ, psi, N: int):
+    """rho = sum_b occ_b psi_b^2 (scf_charge_smt_r), FP64."""
+    nb = psi.numel() // N
+    rho = torch.empty(N, dtype=torch.float64, device=psi.device)
+    fn = "rs_density_f64" if psi.dtype == torch.float64 else "rs_density_f32"
+    L.call(fn, N, nb, _ptr(occ), _ptr(psi), _ptr(rho), _stream())
+    return rho
+
+
+def trans_c2d_smtcharge(shape, nf: int, rho):
+    """Coarse -> dense (nmesh=2) Lagrange interpolation of order 2 nf."""
+    nx, ny, nz = shape
+    out = torch.empty(8 * nx * ny * nz, dtype=torch.float64, device=rho.device)
+    L.call("rs_interp_c2d", nx, ny, nz, nf, _ptr(rho), _ptr(out), _stream())
+    return out
+
+
+def scf_hartee_laplacian(shape, nfh: int, h, v):
+    nx, ny, nz = shape
+    out = torch.empty_like(v)
+    L.call("rs_hartree_laplacian", nx, ny, nz, nfh, h[0], h[1], h[2], _ptr(v), _ptr(out),
+           _stream())
+    return out
+
+
+def scf_hartree(shape, nfh: int, xmax, rho, vh, epsvh=1e-12, ncgmin=1, ncgmax=800,
+                ncgres=801):
+    """CG Poisson solve; vh (in/out) is the warm start.  Returns (iters, dp)."""
+    nx, ny, nz = shape
+    it = C.c_int(0)
+    dp = C.c_double(0)
+    L.call("rs_hartree_cg", nx, ny, nz, nfh, xmax[0], xmax[1], xmax[2], epsvh, ncgmin, ncgmax,
+           ncgres, _ptr(rho), _ptr(vh), C.byref(it), C.byref(dp), _stream())
+    return it.value, dp.value
+
+
+def dot(a, b):
+    out = torch.empty(1, dtype=torch.float64, device=a.device)
+    fn = "rs_dot_f64" if a.dtype == torch.float64 else "rs_dot_f32"
+    L.call(fn, a.numel(), _ptr(a), _ptr(b), _ptr(out), _stream())
+    return out

@@ -1,0 +1,91 @@
+"""ctypes binding of librspace_b200.so (the C ABI of include/rspace_b200.h).
+
+The library is the product: every call here runs sm_100a kernels.  There is
+no CPU fallback -- if the shared object is missing or cannot be loaded the
+import fails with an error that says how to build it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librspace_b200.so")
+
+_i = C.c_int
+_l = C.c_long
+_d = C.c_double
+_p = C.c_void_p
+_ip = C.POINTER(C.c_int)
+_dp = C.POINTER(C.c_double)
+
+# name -> argtypes (restype int unless noted)
+SIGNATURES = {
+    "rs_last_error": [C.c_char_p, _i],
+    "rs_sphere_lists": [_i, _dp, _dp, _dp, _dp, _i, _i, _i, _d, _d, _d, _i, _i, _i, _i, _i,
+                        _ip, _ip, _ip, _ip, _ip, _ip, _ip, _ip],
+    "rs_geom_create": [C.POINTER(_p), _i, _i, _i, _i, _d, _d, _d, _i, _i, _i, _ip, _ip, _ip,
+                       _dp],
+    "rs_geom_destroy": [_p],
+    "rs_kslaplacian_f64": [_p, _p, _p, _p, _i, _p],
+    "rs_kslaplacian_f32": [_p, _p, _p, _p, _i, _p],
+    "rs_nonlocal_dot_f64": [_p, _p, _i, _p, _p],
+    "rs_nonlocal_dot_f32": [_p, _p, _i, _p, _p],
+    "rs_nonlocal_apply_f64": [_p, _p, _p, _i, _p, _p],
+    "rs_hpsi_f64": [_p, _p, _p, _p, _p, _p, _i, _p],
+    "rs_hpsi_f32": [_p, _p, _p, _p, _p, _p, _i, _p],
+    "rs_spsi_f64": [_p, _p, _p, _p, _p, _i, _p],
+    "rs_spsi_f32": [_p, _p, _p, _p, _p, _i, _p],
+    "rs_hpsi_host_f32": [_p, _p, _p, _p, _p, _p, _i, _i, _p],
+    "rs_precondition_f64": [_p, _p, _p, _i, _p],
+    "rs_precondition_f32": [_p, _p, _p, _i, _p],
+    "rs_density_f64": [_l, _i, _p, _p, _p, _p],
+    "rs_density_f32": [_l, _i, _p, _p, _p, _p],
+    "rs_interp_c2d": [_i, _i, _i, _i, _p, _p, _p],
+    "rs_hartree_laplacian": [_i, _i, _i, _i, _d, _d, _d, _p, _p, _p],
+    "rs_hartree_cg": [_i, _i, _i, _i, _d, _d, _d, _d, _i, _i, _i, _p, _p, _ip, _dp, _p],
+    "rs_dot_f64": [_l, _p, _p, _p, _p],
+    "rs_dot_f32": [_l, _p, _p, _p, _p],
+}
+RESTYPES = {"rs_version": C.c_char_p, "rs_geom_entries": _l}
+
+_lib = None
+
+
+class RsError(RuntimeError):
+    pass
+
+
+def load(path: str = LIB_PATH):
+    """Loads the shared object and declares every exported signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RsError(f"{path} is missing: build it with `python -m rspacedist_b200.build`")
+    lib = C.CDLL(path)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = _i
+    for name, rt in RESTYPES.items():
+        getattr(lib, name).restype = rt
+    lib.rs_geom_entries.argtypes = [_p]
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    load().rs_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, what: str = ""):
+    if rc != 0:
+        raise RsError(f"{what}: status {rc}: {last_error()}")
+    return rc
+
+
+def call(name: str, *args):
+    return check(getattr(load(), name)(*args), name)

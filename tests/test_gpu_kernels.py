@@ -1,0 +1,193 @@
+"""GPU parity of the hot-path kernels against the CPU oracle.
+
+FP64 kernels must match the strict oracle bit for bit (same evaluation
+order); FP32 (mixed-precision) kernels must match within the stated relative
+tolerance.  All calls go through the C ABI."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+F32_RTOL = 2e-5   # FP32 psi vs FP64 oracle, relative to the max |value|
+
+
+def T(a, dtype=torch.float64):
+    return torch.tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+def geo_dict(cell):
+    return dict(natom=cell.natom, nprjmx=cell.nprjmx, num_list=cell.num_list, nprj=cell.nprj,
+                natinf=cell.natinf, lst=cell.lst, v=cell.vnlocp.ravel())
+
+
+@pytest.fixture(scope="module")
+def setup(si8, cuda):
+    from rspacedist_b200 import kukan as K, system as S
+    g = K.Geometry(si8)
+    veff = S.smooth_veff(si8, 1)
+    psi = S.random_bands(si8, 5, 2)
+    return si8, g, veff, psi
+
+
+def test_kslaplacian_f64_bit_exact(setup, oracle):
+    from rspacedist_b200 import kukan as K
+    cell, g, veff, psi = setup
+    base = np.random.default_rng(3).standard_normal(psi.shape)
+    ref = oracle.kslaplacian(cell.shape, 4, cell.h, psi, veff, base)
+    out = T(base)
+    K.kslaplacian(g, T(psi), T(veff), out)
+    assert np.array_equal(out.cpu().numpy(), ref)
+
+
+def test_kslaplacian_f32(setup, oracle):
+    from rspacedist_b200 import kukan as K
+    cell, g, veff, psi = setup
+    ref = oracle.kslaplacian(cell.shape, 4, cell.h, psi.astype(np.float32), veff.astype(np.float32))
+    out = torch.zeros(psi.shape, dtype=torch.float32, device="cuda")
+    K.kslaplacian(g, T(psi, torch.float32), T(veff, torch.float32), out)
+    np.testing.assert_allclose(out.cpu().numpy(), ref, atol=F32_RTOL * np.abs(ref).max())
+
+
+def test_nonlocal_dot_f64_bit_exact(setup, oracle):
+    from rspacedist_b200 import kukan as K
+    cell, g, veff, psi = setup
+    ref = oracle.nl_dot(geo_dict(cell), psi, cell.N)
+    rp = K.nonlocaloperation_01(g, T(psi))
+    assert np.array_equal(rp.cpu().numpy(), ref)
+
+
+def test_nonlocal_dot_f32(setup, oracle):
+    from rspacedist_b200 import kukan as K
+    cell, g, veff, psi = setup
+    p32 = psi.astype(np.float32)
+    ref = oracle.nl_dot(geo_dict(cell), p32.astype(np.float64), cell.N)
+    rp = K.nonlocaloperation_01(g, T(p32, torch.float32)).cpu().numpy()
+    np.testing.assert_allclose(rp, ref, atol=1e-6 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("which", ["dij", "sss"])
+def test_nonlocal_apply_f64_bit_exact(setup, oracle, which):
+    from rspacedist_b200 import kukan as K
+    cell, g, veff, psi = setup
+    mat = cell.dij if which == "dij" else cell.sss
+    rp = oracle.nl_dot(geo_dict(cell), psi, cell.N)
+    base = np.random.default_rng(4).standard_normal(psi.shape)
+    ref = oracle.nl_apply(geo_dict(cell), mat, cell.dvol, rp, cell.N, base)
+    out = T(base)
+    K.nonlocaloperation_02(g, T(mat), T(rp), out)
+    assert np.array_equal(out.cpu().numpy(), ref)
+
+
+def test_hpsi_f64_bit_exact(setup, oracle):
+    from rspacedist_b200 import kukan as K
+    cell, g, veff, psi = setup
+    sysk = oracle.make_sys(geo_dict(cell), cell.shape, 4, cell.h, veff, cell.dij, cell.sss)
+    rp = oracle.nl_dot(geo_dict(cell), psi, cell.N)
+    ref = oracle.hpsi(sysk, psi, rp)
+    out = K.hpsi(g, T(veff), T(cell.dij), T(rp), T(psi))
+    assert np.array_equal(out.cpu().numpy(), ref)
+    sref = oracle.spsi(sysk, psi, rp)
+    sout = K.spsi(g, T(cell.sss), T(rp), T(psi))
+    assert np.array_equal(sout.cpu().numpy(), sref)
+
+
+@pytest.mark.parametrize("nb", [1, 5, 13])
+def test_hpsi_f32(setup, oracle, nb):
+    from rspacedist_b200 import kukan as K, system as S
+    cell, g, veff, _ = setup
+    psi = S.random_bands(cell, nb, 7 + nb).astype(np.float32)
+    v32 = veff.astype(np.float32)
+    sysk = oracle.make_sys(geo_dict(cell), cell.shape, 4, cell.h, v32, cell.dij, cell.sss)
+    rp = oracle.nl_dot(geo_dict(cell), psi, cell.N)
+    ref = oracle.hpsi(sysk, psi, rp)
+    out = K.hpsi(g, T(v32, torch.float32), T(cell.dij), T(rp), T(psi, torch.float32))
+    np.testing.assert_allclose(out.cpu().numpy(), ref, atol=F32_RTOL * np.abs(ref).max())
+    sref = oracle.spsi(sysk, psi, rp)
+    sout = K.spsi(g, T(cell.sss), T(rp), T(psi, torch.float32))
+    np.testing.assert_allclose(sout.cpu().numpy(), sref, atol=F32_RTOL * np.abs(sref).max())
+
+
+def test_hpsi_host_matches_device(setup):
+    from rspacedist_b200 import kukan as K, system as S
+    cell, g, veff, _ = setup
+    psi = S.random_bands(cell, 11, 5).astype(np.float32)
+    rp = K.nonlocaloperation_01(g, T(psi, torch.float32))
+    v32 = T(veff, torch.float32)
+    dev = K.hpsi(g, v32, T(cell.dij), rp, T(psi, torch.float32)).cpu()
+    hin = torch.tensor(psi).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    K.hpsi_host(g, v32, T(cell.dij), rp, hin, hout, chunk=4)
+    assert torch.equal(hout, dev)
+
+
+def test_precondition(setup, oracle):
+    from rspacedist_b200 import kukan as K
+    cell, g, veff, psi = setup
+    ref = oracle.precondition(cell.shape, psi)
+    out = K.ksprecondition(g, T(psi))
+    assert np.array_equal(out.cpu().numpy(), ref)
+    o32 = K.ksprecondition(g, T(psi, torch.float32)).cpu().numpy()
+    np.testing.assert_allclose(o32, ref, atol=1e-6 * np.abs(ref).max())
+
+
+def test_density(setup, oracle):
+    from rspacedist_b200 import kukan as K
+    cell, g, veff, psi = setup
+    occ = np.array([2.0, 2.0, 1.5, 0.5, 0.0])
+    ref = oracle.density(occ, psi, cell.N)
+    rho = K.scf_charge_smt(T(occ), T(psi), cell.N)
+    assert np.array_equal(rho.cpu().numpy(), ref)
+    r32 = K.scf_charge_smt(T(occ), T(psi, torch.float32), cell.N).cpu().numpy()
+    ref32 = oracle.density(occ, psi.astype(np.float32).astype(np.float64), cell.N)
+    assert np.array_equal(r32, ref32)
+
+
+def test_interp_c2d_bit_exact(oracle, cuda, built_lib):
+    from rspacedist_b200 import kukan as K
+    shape = (12, 10, 14)
+    x = np.random.default_rng(8).standard_normal(np.prod(shape))
+    ref = oracle.interp_c2d(shape, 4, x)
+    out = K.trans_c2d_smtcharge(shape, 4, T(x))
+    assert np.array_equal(out.cpu().numpy(), ref)
+
+
+def test_hartree_bit_exact(oracle, cuda, built_lib):
+    from rspacedist_b200 import kukan as K
+    shape = (24, 20, 16)
+    h = (0.31, 0.33, 0.29)
+    xmax = tuple(n * hh / 2 for n, hh in zip(shape, h))
+    rng = np.random.default_rng(9)
+    rho = rng.standard_normal(np.prod(shape))
+    v = rng.standard_normal(np.prod(shape))
+    ref = oracle.hartree_laplacian(shape, 4, h, v)
+    out = K.scf_hartee_laplacian(shape, 4, h, T(v))
+    assert np.array_equal(out.cpu().numpy(), ref)
+    vh0 = rng.standard_normal(np.prod(shape)) * 0.01
+    vref, itref, dpref = oracle.hartree_cg(shape, 4, xmax, 1e-12, 1, 800, 801, rho, vh0)
+    vh = T(vh0)
+    it, dp = K.scf_hartree(shape, 4, xmax, T(rho), vh)
+    assert it == itref and dp == dpref
+    assert np.array_equal(vh.cpu().numpy(), vref)
+
+
+@pytest.mark.parametrize("n", [1, 4095, 4096, 4097, 300000])
+def test_tree_dot_bit_exact(oracle, cuda, built_lib, n):
+    from rspacedist_b200 import kukan as K
+    rng = np.random.default_rng(n)
+    a, b = rng.standard_normal(n), rng.standard_normal(n)
+    assert K.dot(T(a), T(b)).item() == oracle.tree_dot(a, b)
+    a32, b32 = a.astype(np.float32), b.astype(np.float32)
+    assert K.dot(T(a32, torch.float32), T(b32, torch.float32)).item() == oracle.tree_dot(a32, b32)
+
+
+def test_c8_norm_conserving_hpsi(c8, oracle, cuda):
+    from rspacedist_b200 import kukan as K, system as S
+    g = K.Geometry(c8)
+    veff = S.smooth_veff(c8, 3)
+    psi = S.random_bands(c8, 3, 4)
+    sysk = oracle.make_sys(geo_dict(c8), c8.shape, 4, c8.h, veff, c8.dij, None)
+    rp = oracle.nl_dot(geo_dict(c8), psi, c8.N)
+    ref = oracle.hpsi(sysk, psi, rp)
+    out = K.hpsi(g, T(veff), T(c8.dij), T(rp), T(psi))
+    assert np.array_equal(out.cpu().numpy(), ref)

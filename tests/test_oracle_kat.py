@@ -1,0 +1,184 @@
+"""Pins the CPU oracle against analytic known answers (the reference ships no
+tests or outputs): exact FD rationals, plane-wave symbols, the FFT-exact
+discrete Poisson solution, interpolation error bounds, dense
+diagonalisation, and the band solvers' converged eigenvalues."""
+import json
+import os
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_fd_coefficients_are_the_exact_rationals(oracle):
+    d = json.load(open(os.path.join(GOLD, "fd_coefs.json")))
+    for nf in range(1, 7):
+        a = oracle.fdcoef(nf)
+        exact = [float(Fraction(x)) for x in d["fd"][str(nf)]]
+        assert np.array_equal(a[: nf + 1], np.array(exact))
+        # and they are the Fornberg central weights of order 2nf
+        fb = [float(Fraction(x)) for x in d["fornberg"][str(nf)]]
+        np.testing.assert_allclose(a[: nf + 1], fb, rtol=1e-15, atol=1e-17)
+
+
+@pytest.mark.parametrize("k", [(0, 0, 0), (1, 0, 0), (3, 2, 1), (5, 4, 6)])
+def test_stencil_plane_wave_symbol(oracle, k):
+    nx, ny, nz = 16, 12, 14
+    h = (0.31, 0.29, 0.33)
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    psi = np.cos(2 * np.pi * (k[0] * x / nx + k[1] * y / ny + k[2] * z / nz)).ravel()
+    a = oracle.fdcoef(4)
+    lam = lambda kk, n, hh: -0.5 / hh ** 2 * (a[0] + 2 * sum(a[m] * np.cos(2 * np.pi * kk * m / n)
+                                                           for m in range(1, 5)))
+    ev = lam(k[0], nx, h[0]) + lam(k[1], ny, h[1]) + lam(k[2], nz, h[2])
+    veff = np.full(nx * ny * nz, 0.25)
+    out = oracle.kslaplacian((nx, ny, nz), 4, h, psi, veff)
+    np.testing.assert_allclose(out, (ev + 0.25) * psi, atol=1e-12 * max(1, abs(ev)))
+
+
+def test_hartree_cg_matches_fft_solution(oracle):
+    g = np.load(os.path.join(GOLD, "poisson_fft.npz"))
+    nx, ny, nz = (int(v) for v in g["shape"])
+    h = g["h"]
+    xmax = (nx * h[0] / 2, ny * h[1] / 2, nz * h[2] / 2)
+    vh, it, dp = oracle.hartree_cg((nx, ny, nz), 4, xmax, 1e-12, 1, 800, 801, g["rho"],
+                                   np.zeros(nx * ny * nz))
+    assert dp <= 1e-12 and it < 800
+    v = vh - vh.mean()
+    np.testing.assert_allclose(v, g["v"], atol=1e-10 * np.abs(g["v"]).max())
+
+
+def test_interpolation_order(oracle):
+    g = np.load(os.path.join(GOLD, "interp_trig.npz"))
+    shape = tuple(int(v) for v in g["shape"])
+    out = oracle.interp_c2d(shape, 4, g["coarse"])
+    err = np.abs(out - g["dense"]).max()
+    assert err < 5e-3
+    # constant and order: weights sum to one
+    one = oracle.interp_c2d(shape, 4, np.ones(np.prod(shape)))
+    np.testing.assert_allclose(one, 1.0, atol=1e-14)
+
+
+def test_jacobi_matches_lapack(oracle):
+    rng = np.random.default_rng(3)
+    a = rng.standard_normal((40, 40))
+    a = a + a.T
+    st, w, z = oracle.jacobi_eig(a)
+    assert st > 0
+    np.testing.assert_allclose(w, np.linalg.eigvalsh(a), atol=1e-12)
+    np.testing.assert_allclose(z.T @ a @ z, np.diag(w), atol=1e-11)
+
+
+def test_eig2(oracle):
+    rng = np.random.default_rng(4)
+    for _ in range(50):
+        a = rng.standard_normal((2, 2))
+        a = a + a.T
+        w, z = oracle.eig2(a)
+        np.testing.assert_allclose(w, np.linalg.eigvalsh(a), atol=1e-14)
+        np.testing.assert_allclose(a @ z, z * w, atol=1e-13)
+
+
+def test_reorder_rank_is_stable_sort(oracle):
+    s = np.array([0.3, -1.0, 0.3, 2.0, -1.0, 0.0])
+    r = oracle.reorder_rank(s)
+    assert list(r) == list(np.argsort(np.argsort(s, kind="stable"), kind="stable"))
+
+
+def test_tree_dot_is_a_dot(oracle):
+    rng = np.random.default_rng(5)
+    for n in (0, 1, 4095, 4096, 4097, 1 << 20):
+        a, b = rng.standard_normal(n), rng.standard_normal(n)
+        assert abs(oracle.tree_dot(a, b) - float(a @ b)) <= 1e-12 * (1 + np.abs(a) @ np.abs(b))
+
+
+def smooth_random(shape, M, seed):
+    nx, ny, nz = shape
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((M, nz, ny, nx))
+    kz, ky, kx = np.meshgrid(np.fft.fftfreq(nz), np.fft.fftfreq(ny), np.fft.fftfreq(nx),
+                             indexing="ij")
+    filt = np.exp(-(kx ** 2 + ky ** 2 + kz ** 2) / 0.02)
+    x = np.real(np.fft.ifftn(np.fft.fftn(x, axes=(1, 2, 3)) * filt, axes=(1, 2, 3)))
+    return x.reshape(M, -1)
+
+
+def _tiny_system(oracle, paw):
+    """A 12^3 cell with one or two synthetic projector atoms: small enough to
+    build H and S densely from unit vectors."""
+    nx = ny = nz = 12
+    h = (0.5, 0.5, 0.5)
+    N = nx * ny * nz
+    st, lists = oracle.sphere_lists(np.array([[0.1, -0.2, 0.3], [-2.0, 1.5, 1.0]]), 1.2,
+                                    (6, 6, 6), h, (3, 3, 3), 1, 6 * 6 * 6)
+    assert st == 0
+    A, P, Lm = 2, 2, 216
+    v = np.zeros((A, P, Lm))
+    rng = np.random.default_rng(11)
+    atoms = np.array([[0.1, -0.2, 0.3], [-2.0, 1.5, 1.0]])
+    for a in range(A):
+        n = lists["natinf"][a]
+        # smooth s- and p_x-like projectors on the list points
+        tx = [atoms[a, k] - (lists["nat" + "xyz"[k]][a] * h[k] - 0.5 * h[k]) for k in range(3)]
+        x = lists["lstx"][a * Lm:a * Lm + n] * h[0] - tx[0]
+        y = lists["lsty"][a * Lm:a * Lm + n] * h[1] - tx[1]
+        z = lists["lstz"][a * Lm:a * Lm + n] * h[2] - tx[2]
+        g = np.exp(-(x * x + y * y + z * z) / 0.9)
+        v[a, 0, :n] = g * 0.125
+        v[a, 1, :n] = g * x * 0.125
+    geo = dict(natom=A, nprjmx=P, num_list=Lm, nprj=np.full(A, P, np.int32),
+               natinf=lists["natinf"], lst=lists["lst"], v=v.ravel())
+    D = np.zeros((A, P, P))
+    Sm = np.zeros((A, P, P))
+    for a in range(A):
+        m = rng.standard_normal((P, P))
+        D[a] = (m + m.T) * 0.5
+        m = rng.standard_normal((P, P)) * 0.2
+        Sm[a] = (m + m.T) * 0.5 + 0.3 * np.eye(P)
+    veff = rng.standard_normal(N) * 0.3
+    sysk = oracle.make_sys(geo, (nx, ny, nz), 4, h, veff, D, Sm if paw else None)
+    return sysk, geo, N, h
+
+
+@pytest.mark.parametrize("paw", [False, True])
+def test_band_solvers_reach_dense_eigenvalues(oracle, paw):
+    sysk, geo, N, h = _tiny_system(oracle, paw)
+    dv = h[0] * h[1] * h[2]
+    eye = np.eye(N)
+    rp = oracle.nl_dot(geo, eye, N)
+    H = oracle.hpsi(sysk, eye, rp).reshape(N, N).T
+    S = oracle.spsi(sysk, eye, rp).reshape(N, N).T if paw else np.eye(N)
+    import scipy.linalg as sl
+    ref = sl.eigh(0.5 * (H + H.T), 0.5 * (S + S.T), eigvals_only=True)[:6]
+    M = 8
+    # smooth start: the preconditioner (1/2 + 1/12 sum of 6 neighbours) is
+    # blind to the (pi,pi,pi) mode, so a white-noise start would keep that
+    # component for ever; kukan starts from smooth atomic orbitals
+    psi = smooth_random((12, 12, 12), M, 1)
+    rp = oracle.nl_dot(geo, psi, N)
+    sp = oracle.spsi(sysk, psi, rp) if paw else None
+    psi, sp, rp = oracle.ortho(sysk, M, psi, sp, rp, 0, 1)
+    start = (psi.copy(), None if sp is None else sp.copy(), rp.copy())
+    # without the smoother: converges to rounding
+    for it in range(60):
+        st, psi, sp, rp, sval = oracle.rayleighritz(sysk, M, psi, sp, rp)
+        st, psi, sp, rp, hh, sval, resid = oracle.kscg(sysk, M, psi, sp, rp, nsdmax=4, nprecon=0)
+    st, psi, sp, rp, sval = oracle.rayleighritz(sysk, M, psi, sp, rp)
+    np.testing.assert_allclose(sval[:6], ref, atol=1e-9)
+    # DIIS keeps the converged subspace
+    conv, psi2, sp2, rp2, h2, sval2, res2 = oracle.ksdiis(sysk, M, psi, sp, rp, nprecon=0)
+    st, psi2, sp2, rp2, sval3 = oracle.rayleighritz(sysk, M, psi2, sp2, rp2)
+    np.testing.assert_allclose(sval3[:6], ref, atol=1e-9)
+    # with kukan's smoother: the (pi,pi,pi) mode it cannot reach bounds the error
+    psi3, sp3, rp3 = start
+    for it in range(40):
+        st, psi3, sp3, rp3, sval = oracle.rayleighritz(sysk, M, psi3, sp3, rp3)
+        st, psi3, sp3, rp3, hh, sval, resid = oracle.kscg(sysk, M, psi3, sp3, rp3, nsdmax=4)
+        conv, psi3, sp3, rp3, hh, sval, resid = oracle.ksdiis(sysk, M, psi3, sp3, rp3)
+    st, psi3, sp3, rp3, sval = oracle.rayleighritz(sysk, M, psi3, sp3, rp3)
+    np.testing.assert_allclose(sval[:6], ref, atol=2e-5)
+    # S-orthonormality of the Ritz vectors
+    spn = oracle.spsi(sysk, psi2, oracle.nl_dot(geo, psi2, N)) if paw else psi2
+    np.testing.assert_allclose(psi2 @ spn.T * dv, np.eye(M), atol=1e-9)
