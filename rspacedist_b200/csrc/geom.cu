@@ -137,7 +137,8 @@ static int upload(T** dst, const T* src, size_t n) {
 extern "C" int rs_geom_destroy(rs_geom* g) {
   if (!g) return RS_OK;
   void* ptrs[] = {g->d_nprj, g->d_natinf, g->d_lst, g->d_vT64, g->d_vT32, g->d_inv_off,
-                  g->d_inv_atom, g->d_inv_v64, g->d_inv_v32};
+                  g->d_inv_atom, g->d_inv_v64, g->d_inv_v32, g->d_cov,
+                  g->d_cov_off, g->d_nz_off, g->d_nz_pt, g->d_nz_v32, g->d_nz_v64};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete g;
@@ -208,6 +209,10 @@ extern "C" int rs_geom_create(rs_geom** out, int nx, int ny, int nz, int nf, dou
   for (long p = 0; p < N; ++p) maxinv = std::max(maxinv, off[p + 1] - off[p]);
   g->max_inv = maxinv;
   g->n_inv = ne;
+  std::vector<int> cov;
+  for (long p = 0; p < N; ++p)
+    if (off[p + 1] > off[p]) cov.push_back((int)p);
+  g->n_cov = (long)cov.size();
   std::vector<int> fillp(off.begin(), off.end() - 1);
   std::vector<int> inv_atom(ne > 0 ? ne : 1);
   std::vector<double> inv_v(ne > 0 ? (size_t)ne * nprjmx : 1, 0.0);
@@ -228,6 +233,28 @@ extern "C" int rs_geom_create(rs_geom** out, int nx, int ny, int nz, int nf, dou
     }
   for (size_t i = 0; i < vT.size(); ++i) vT32[i] = (float)vT[i];
   for (size_t i = 0; i < inv_v.size(); ++i) inv_v32[i] = (float)inv_v[i];
+  std::vector<int> cov_off(cov.size() + 1, 0);
+  for (size_t c = 0; c < cov.size(); ++c) {
+    cov_off[c] = off[cov[c]];
+    cov_off[c + 1] = off[cov[c] + 1];
+  }
+  // atom-major compact lists (skipping all-zero list positions leaves every
+  // fma chain of the gather-dot unchanged: the skipped terms add zero)
+  std::vector<int> nz_off(natom + 1, 0), nz_pt;
+  std::vector<double> nz_v;
+  for (int i = 0; i < natom; ++i) {
+    for (int ii = 0; ii < natinf[i]; ++ii) {
+      if (zero_entry(i, ii)) continue;
+      nz_pt.push_back(lst[(long)i * num_list + ii]);
+      for (int j = 0; j < nprjmx; ++j) nz_v.push_back(vT[((size_t)i * num_list + ii) * nprjmx + j]);
+    }
+    nz_off[i + 1] = (int)nz_pt.size();
+  }
+  if (nz_pt.empty()) {
+    nz_pt.push_back(0);
+    nz_v.assign(nprjmx > 0 ? nprjmx : 1, 0.0);
+  }
+  std::vector<float> nz_v32(nz_v.begin(), nz_v.end());
   if ((st = upload(&g->d_inv_off, off.data(), off.size())) ||
       (natom > 0 && (st = upload(&g->d_nprj, nprj, natom))) ||
       (natom > 0 && (st = upload(&g->d_natinf, natinf, natom))) ||
@@ -236,7 +263,13 @@ extern "C" int rs_geom_create(rs_geom** out, int nx, int ny, int nz, int nf, dou
       (st = upload(&g->d_vT32, vT32.data(), vT32.size())) ||
       (st = upload(&g->d_inv_atom, inv_atom.data(), inv_atom.size())) ||
       (st = upload(&g->d_inv_v64, inv_v.data(), inv_v.size())) ||
-      (st = upload(&g->d_inv_v32, inv_v32.data(), inv_v32.size()))) {
+      (st = upload(&g->d_inv_v32, inv_v32.data(), inv_v32.size())) ||
+      (st = upload(&g->d_cov, cov.data(), cov.size())) ||
+      (st = upload(&g->d_cov_off, cov_off.data(), cov_off.size())) ||
+      (st = upload(&g->d_nz_off, nz_off.data(), nz_off.size())) ||
+      (st = upload(&g->d_nz_pt, nz_pt.data(), nz_pt.size())) ||
+      (st = upload(&g->d_nz_v32, nz_v32.data(), nz_v32.size())) ||
+      (st = upload(&g->d_nz_v64, nz_v.data(), nz_v.size()))) {
     rs_geom_destroy(g);
     return st;
   }

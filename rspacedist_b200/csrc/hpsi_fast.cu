@@ -1,15 +1,333 @@
-// hpsi_fast.cu -- FP32 fused H*psi used by the mixed-precision path.
+// hpsi_fast.cu -- FP32 H*psi for the mixed-precision path, in two kernels:
+//
+// 1. k_stencil_f32_zmarch: (-1/2 lap + veff) psi.  One CTA owns a 64 x 32
+//    tile of an xy plane of one band and marches along z.  Each thread holds
+//    a 4(x) x 2(y) block of points:
+//      * the nine planes z-4..z+4 of its block sit in a register queue, so
+//        the z terms need no shared memory;
+//      * whole planes (own blocks plus a 4-point halo) are copied into an
+//        8-slot shared ring with cp.async, 3 planes ahead of the queue's
+//        newest plane, so HBM latency is hidden without spending registers;
+//        x terms read 2 float4 per row, y terms 8 float4 for both rows, and
+//        one __syncthreads per plane protects slot reuse.
+//    Tiles of one band are adjacent in launch order, so halo rows come from
+//    L2 (loaded by the neighbouring tiles), and psi crosses HBM once.
+// 2. k_nl_rmw_f32: the nonlocal D term on the points inside at least one
+//    projector support (a fraction of the grid).  A thread owns one such
+//    point and a block of 16 bands: it loads the point's projector entries
+//    once and adds sum_e sum_j t[atom_e][b][j] p_e[j] to 16 bands of hpsi.
 #include "rs_common.cuh"
 #include "stencil.cuh"
 
 namespace rs {
+
 template <class T, int MODE>
 int launch_gather(const rs_geom* g, const double* mat, const double* rp, const T* psi,
                   const T* veff, T* out, int nb, cudaStream_t st);
 
+namespace {
+
+constexpr int TX = 64;
+constexpr int TY = 32;
+constexpr int NTX = TX / 4;
+constexpr int NTY = TY / 2;
+constexpr int NTHREADS = NTX * NTY;  // 256
+constexpr int HX = TX + 8;
+constexpr int HY = TY + 8;
+constexpr int NL_BANDS = 16;
+
+struct StArgs {
+  int nx, ny, nz, zchunk, ntx, nty;
+  float cx[5], cy[5], cz[5], c0;
+  const float* psi;
+  float* out;
+  const float* veff;
+};
+
+__device__ __forceinline__ int wrap_once(int i, int n) {
+  return i < 0 ? i + n : (i >= n ? i - n : i);
+}
+__device__ __forceinline__ float4 ld4(const float* p) {
+  return __ldg(reinterpret_cast<const float4*>(p));
+}
+__device__ __forceinline__ float4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+
+__device__ __forceinline__ void fma4(float c, const float4& v, float* acc) {
+  acc[0] = fmaf(c, v.x, acc[0]);
+  acc[1] = fmaf(c, v.y, acc[1]);
+  acc[2] = fmaf(c, v.z, acc[2]);
+  acc[3] = fmaf(c, v.w, acc[3]);
+}
+
+// 16-byte asynchronous global->shared copies (cp.async, L2 only)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+constexpr int RING = 8;    // staged planes (halo'd) in shared memory
+constexpr int AHEAD = 3;   // planes in flight beyond the queue's newest plane
+
+__global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
+  extern __shared__ __align__(16) float smem_raw[];
+  float (*pl)[HY][HX] = reinterpret_cast<float (*)[HY][HX]>(smem_raw);  // [RING][HY][HX]
+  const int tid = threadIdx.x;
+  const int tx = tid % NTX, ty = tid / NTX;
+  const int ntile = a.ntx * a.nty;
+  const int tile = blockIdx.x % ntile;
+  const int zc = blockIdx.x / ntile;
+  const int band = blockIdx.y;
+  const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const long plane = (long)nx * ny;
+  const long N = plane * nz;
+  const float* psi = a.psi + (long)band * N;
+  float* out = a.out + (long)band * N;
+  const int zs = zc * a.zchunk;
+  const int ze = min(zs + a.zchunk, nz);
+  const int gx = x0 + 4 * tx, gy = y0 + 2 * ty;
+  const bool active = gx < nx && gy < ny;  // nx % 4 == 0, ny even
+  const int w = min(TX, nx - x0), hgt = min(TY, ny - y0);
+  const long own0 = (long)gy * nx + gx, own1 = own0 + nx;
+  const int lx = 4 * tx + 4, ly = 2 * ty + 4;
+
+  // the halo float4 this thread stages for every plane (or none)
+  int h_src = -1, h_row = 0, h_col = 0;
+  if (tid < 2 * TY) {
+    const int side = tid / TY, r = tid % TY;
+    if (r < hgt) {
+      const int xs = side == 0 ? wrap_once(x0 - 4, nx) : wrap_once(x0 + w, nx);
+      h_src = (y0 + r) * nx + xs;
+      h_row = r + 4;
+      h_col = side == 0 ? 0 : w + 4;
+    }
+  } else if (tid < 2 * TY + 8 * NTX) {
+    const int j = tid - 2 * TY;
+    const int c = j % NTX, rr = (j / NTX) % 4, side = j / (4 * NTX);
+    if (4 * c < w) {
+      const int ys = side == 0 ? wrap_once(y0 - 4 + rr, ny) : wrap_once(y0 + hgt + rr, ny);
+      h_src = ys * nx + x0 + 4 * c;
+      h_row = side == 0 ? rr : hgt + 4 + rr;
+      h_col = 4 + 4 * c;
+    }
+  }
+  auto plane_ptr = [&](int z) { return psi + (long)wrap_once(z, nz) * plane; };
+  // one commit group per plane: this thread's own rows and its halo piece
+  auto stage = [&](int z) {
+    const float* pp = plane_ptr(z);
+    float(*sl)[HX] = pl[z & (RING - 1)];
+    if (active) {
+      cp_async16(&sl[ly][lx], pp + own0);
+      cp_async16(&sl[ly + 1][lx], pp + own1);
+    }
+    if (h_src >= 0) cp_async16(&sl[h_row][h_col], pp + h_src);
+    cp_commit();
+  };
+
+  float4 q[9][2];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float* pp = plane_ptr(zs - 4 + k);
+    q[k][0] = active ? ld4(pp + own0) : zero4();
+    q[k][1] = active ? ld4(pp + own1) : zero4();
+  }
+#pragma unroll
+  for (int k = 0; k < 4 + AHEAD; ++k) stage(zs + k);
+  cp_wait<AHEAD>();
+  __syncthreads();
+#pragma unroll
+  for (int k = 4; k < 8; ++k) {
+    const float(*sl)[HX] = pl[(zs + k - 4) & (RING - 1)];
+    q[k][0] = *reinterpret_cast<const float4*>(&sl[ly][lx]);
+    q[k][1] = *reinterpret_cast<const float4*>(&sl[ly + 1][lx]);
+  }
+  float4 vreg[2];
+  vreg[0] = active ? ld4(a.veff + (long)zs * plane + own0) : zero4();
+  vreg[1] = active ? ld4(a.veff + (long)zs * plane + own1) : zero4();
+
+  for (int z = zs; z < ze; ++z) {
+    stage(z + 4 + AHEAD);   // reuses the slot of plane z-1 (freed by the last sync)
+    cp_wait<AHEAD>();       // this thread's copies of plane z+4 have landed
+    const float(*cur)[HX] = pl[z & (RING - 1)];
+    {
+      const float(*nw)[HX] = pl[(z + 4) & (RING - 1)];
+      q[8][0] = *reinterpret_cast<const float4*>(&nw[ly][lx]);
+      q[8][1] = *reinterpret_cast<const float4*>(&nw[ly + 1][lx]);
+    }
+    const float4 vcur[2] = {vreg[0], vreg[1]};
+    if (active && z + 1 < ze) {
+      vreg[0] = ld4(a.veff + (long)(z + 1) * plane + own0);
+      vreg[1] = ld4(a.veff + (long)(z + 1) * plane + own1);
+    }
+    if (active) {
+#pragma unroll
+      for (int rr = 0; rr < 2; ++rr) {
+        const float4 L = *reinterpret_cast<const float4*>(&cur[ly + rr][lx - 4]);
+        const float4 R = *reinterpret_cast<const float4*>(&cur[ly + rr][lx + 4]);
+        const float4 C = q[4][rr];
+        const float xv[12] = {L.x, L.y, L.z, L.w, C.x, C.y, C.z, C.w, R.x, R.y, R.z, R.w};
+        const float vv[4] = {vcur[rr].x, vcur[rr].y, vcur[rr].z, vcur[rr].w};
+        float acc[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          float s = a.cx[4] * xv[i];
+          s = fmaf(a.cx[3], xv[i + 1], s);
+          s = fmaf(a.cx[2], xv[i + 2], s);
+          s = fmaf(a.cx[1], xv[i + 3], s);
+          s = fmaf(a.c0 + vv[i], xv[i + 4], s);
+          s = fmaf(a.cx[1], xv[i + 5], s);
+          s = fmaf(a.cx[2], xv[i + 6], s);
+          s = fmaf(a.cx[3], xv[i + 7], s);
+          s = fmaf(a.cx[4], xv[i + 8], s);
+          acc[i] = s;
+        }
+#pragma unroll
+        for (int m = 4; m >= 1; --m) {
+          const int yy = rr - m;
+          const float4 v =
+              yy == 0 ? q[4][0] : *reinterpret_cast<const float4*>(&cur[ly + yy][lx]);
+          fma4(a.cy[m], v, acc);
+        }
+#pragma unroll
+        for (int m = 1; m <= 4; ++m) {
+          const int yy = rr + m;
+          const float4 v =
+              yy == 1 ? q[4][1] : *reinterpret_cast<const float4*>(&cur[ly + yy][lx]);
+          fma4(a.cy[m], v, acc);
+        }
+#pragma unroll
+        for (int m = 4; m >= 1; --m) fma4(a.cz[m], q[4 - m][rr], acc);
+#pragma unroll
+        for (int m = 1; m <= 4; ++m) fma4(a.cz[m], q[4 + m][rr], acc);
+        *reinterpret_cast<float4*>(out + (long)z * plane + (rr ? own1 : own0)) =
+            make_float4(acc[0], acc[1], acc[2], acc[3]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      q[k][0] = q[k + 1][0];
+      q[k][1] = q[k + 1][1];
+    }
+    __syncthreads();
+  }
+  cp_wait<0>();
+}
+
+// t coefficients in atom-major order t[a][b][i] = (sum_j rp[b][a][j] m[a][i][j]) / dV
+// (FP64 sum, stored FP32), so that one atom's coefficients for a block of
+// bands are contiguous.
+__global__ void k_tcoef_f32(int natom, int nprjmx, const int* __restrict__ nprj,
+                            const double* __restrict__ mat, const double* __restrict__ rp,
+                            double dxyzin, int nb, float* __restrict__ t) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long total = (long)nb * natom * nprjmx;
+  if (idx >= total) return;
+  const int i = (int)(idx % nprjmx);
+  const long ba = idx / nprjmx;
+  const int at = (int)(ba % natom);
+  const int b = (int)(ba / natom);
+  const int P = nprj[at];
+  double s = 0.0;
+  if (i < P) {
+    const double* r = rp + ba * nprjmx;
+    const double* m = mat + ((long)at * nprjmx + i) * nprjmx;
+    for (int j = 0; j < P; ++j) s = fma(r[j], m[j], s);
+    s = s * dxyzin;
+  }
+  t[((long)at * nb + b) * nprjmx + i] = (float)s;
+}
+
+// hpsi[b][p] += sum over p's entries e of t[a_e][b] . p_e for NL_BANDS bands.
+// All loads of a thread are independent of each other except through the
+// entry's atom index, so many are in flight at once.
+__global__ void __launch_bounds__(128) k_nl_rmw_f32(
+    const int* __restrict__ cov, const int* __restrict__ cov_off, long ncov,
+    const int* __restrict__ inv_atom, const float* __restrict__ inv_v,
+    const float* __restrict__ tco, int P, long N, int nb, float* __restrict__ out) {
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncov) return;
+  const int b0 = blockIdx.y * NL_BANDS;
+  const int nbb = min(NL_BANDS, nb - b0);
+  const int p = __ldg(cov + c);
+  const int e0 = __ldg(cov_off + c), e1 = __ldg(cov_off + c + 1);
+  float h[NL_BANDS];
+#pragma unroll
+  for (int b = 0; b < NL_BANDS; ++b) h[b] = b < nbb ? out[(long)(b0 + b) * N + p] : 0.f;
+  const int nq = P / 4;
+  for (int e = e0; e < e1; ++e) {
+    const int at = __ldg(inv_atom + e);
+    float4 v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = k < nq ? ld4(inv_v + (long)e * P + 4 * k) : zero4();
+    const float* tb = tco + ((long)at * nb + b0) * P;
+#pragma unroll
+    for (int b = 0; b < NL_BANDS; ++b) {
+      if (b < nbb) {
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (k < nq) {
+            const float4 t = ld4(tb + (long)b * P + 4 * k);
+            s = fmaf(t.x, v[k].x, s);
+            s = fmaf(t.y, v[k].y, s);
+            s = fmaf(t.z, v[k].z, s);
+            s = fmaf(t.w, v[k].w, s);
+          }
+        }
+        h[b] += s;
+      }
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < NL_BANDS; ++b)
+    if (b < nbb) out[(long)(b0 + b) * N + p] = h[b];
+}
+
+}  // namespace
+
 int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
                          const double* rp, const float* psi, float* hpsi, int nb,
                          cudaStream_t st) {
-  return launch_gather<float, 1>(g, dij, rp, psi, veff, hpsi, nb, st);
+  if (nb <= 0) return RS_OK;
+  const bool shape_ok = g->nf == 4 && g->nx % 4 == 0 && g->ny % 2 == 0 && g->nx >= 8 &&
+                        g->ny >= 8 && g->nz >= 8 && nb <= 65535;
+  const bool proj_ok = g->nprjmx % 4 == 0 && g->nprjmx <= 16;
+  if (!shape_ok || !proj_ok) return launch_gather<float, 1>(g, dij, rp, psi, veff, hpsi, nb, st);
+  StArgs a;
+  a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+  a.zchunk = g->nz <= 160 ? g->nz : 64;
+  a.ntx = (g->nx + TX - 1) / TX;
+  a.nty = (g->ny + TY - 1) / TY;
+  for (int m = 0; m < 5; ++m) {
+    a.cx[m] = (float)g->cx[m]; a.cy[m] = (float)g->cy[m]; a.cz[m] = (float)g->cz[m];
+  }
+  a.c0 = (float)(g->cx[0] + g->cy[0] + g->cz[0]);
+  a.psi = psi; a.out = hpsi; a.veff = veff;
+  const int nzc = (g->nz + a.zchunk - 1) / a.zchunk;
+  dim3 grid(a.ntx * a.nty * nzc, nb);
+  const size_t smem = sizeof(float) * RING * HY * HX;
+  RS_CUDA(cudaFuncSetAttribute(k_stencil_f32_zmarch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem));
+  k_stencil_f32_zmarch<<<grid, NTHREADS, smem, st>>>(a);
+  RS_LAUNCH_CHECK("k_stencil_f32_zmarch");
+  if (g->natom == 0 || g->n_cov == 0) return RS_OK;
+  const long nt = (long)nb * g->natom * g->nprjmx;
+  float* t = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&t, nt * sizeof(float), st));
+  k_tcoef_f32<<<div_up(nt, 256), 256, 0, st>>>(g->natom, g->nprjmx, g->d_nprj, dij, rp,
+                                               1.0 / (g->dx * g->dy * g->dz), nb, t);
+  dim3 g2(div_up(g->n_cov, 128), div_up(nb, NL_BANDS));
+  k_nl_rmw_f32<<<g2, 128, 0, st>>>(g->d_cov, g->d_cov_off, g->n_cov, g->d_inv_atom,
+                                    g->d_inv_v32, t, g->nprjmx, g->N, nb, hpsi);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(t, st);
+  if (e != cudaSuccess) return cuda_status(e, "k_nl_rmw_f32");
+  return RS_OK;
 }
+
 }  // namespace rs

@@ -16,13 +16,13 @@
 namespace rs {
 
 // ---------------------------------------------------------------- dot
-// Thread (j, band) of block (atom, band group).  For T=double the chain is
-// the reference's; for T=float the products and the sum are FP64.
-template <class T>
-__global__ void k_nl_dot(int natom, int nprjmx, int num_list, const int* __restrict__ nprj,
-                         const int* __restrict__ natinf, const int* __restrict__ lst,
-                         const T* __restrict__ vT, const T* __restrict__ psi, long N, int nb,
-                         double* __restrict__ rp) {
+// FP64: thread (j, band) of block (atom, band group) runs the reference's
+// sequential fma chain over the atom's nonzero list positions only (a
+// skipped position would add fma(0, x, acc) == acc).
+__global__ void k_nl_dot_f64(int natom, int nprjmx, const int* __restrict__ nprj,
+                             const int* __restrict__ nz_off, const int* __restrict__ nz_pt,
+                             const double* __restrict__ nz_v, const double* __restrict__ psi,
+                             long N, int nb, double* __restrict__ rp) {
   const int a = blockIdx.x;
   const int bpb = blockDim.x / nprjmx;
   const int j = threadIdx.x % nprjmx, bl = threadIdx.x / nprjmx;
@@ -30,14 +30,66 @@ __global__ void k_nl_dot(int natom, int nprjmx, int num_list, const int* __restr
   if (bl >= bpb || b >= nb) return;
   double acc = 0.0;
   if (j < nprj[a]) {
-    const int L = natinf[a];
-    const int* l = lst + (long)a * num_list;
-    const T* v = vT + (long)a * num_list * nprjmx + j;
-    const T* x = psi + (long)b * N;
-    for (int ii = 0; ii < L; ++ii)
-      acc = fma((double)__ldg(v + (long)ii * nprjmx), (double)__ldg(x + __ldg(l + ii)), acc);
+    const int e0 = nz_off[a], e1 = nz_off[a + 1];
+    const double* x = psi + (long)b * N;
+    for (int e = e0; e < e1; ++e)
+      acc = fma(__ldg(nz_v + (long)e * nprjmx + j), __ldg(x + __ldg(nz_pt + e)), acc);
   }
   rp[((long)b * natom + a) * nprjmx + j] = acc;
+}
+
+// FP32 psi: CTA (atom, 32 bands).  Chunks of 64 list positions are staged in
+// shared memory (psi gathered per band along the list, projector values
+// contiguous); thread (band, j-group) accumulates its dots over the chunk in
+// FP32 and adds the chunk sum into an FP64 total.
+constexpr int DOT_BANDS = 32;
+constexpr int DOT_CHUNK = 64;
+constexpr int DOT_MAXP = 16;
+
+__global__ void __launch_bounds__(256) k_nl_dot_f32(
+    int natom, int nprjmx, const int* __restrict__ nprj, const int* __restrict__ nz_off,
+    const int* __restrict__ nz_pt, const float* __restrict__ nz_v, const float* __restrict__ psi,
+    long N, int nb, double* __restrict__ rp) {
+  __shared__ float xs[DOT_CHUNK][DOT_BANDS + 1];
+  __shared__ float vs[DOT_CHUNK][DOT_MAXP];
+  __shared__ int ps[DOT_CHUNK];
+  const int a = blockIdx.x;
+  const int b0 = blockIdx.y * DOT_BANDS;
+  const int t = threadIdx.x;
+  const int bl = t % DOT_BANDS, jg = t / DOT_BANDS;  // 8 j-groups
+  const int P = nprj[a];
+  const int e0 = nz_off[a], e1 = nz_off[a + 1];
+  double tot[2] = {0.0, 0.0};
+  for (int c0 = e0; c0 < e1; c0 += DOT_CHUNK) {
+    const int n = min(DOT_CHUNK, e1 - c0);
+    if (t < n) ps[t] = __ldg(nz_pt + c0 + t);
+    for (int i = t; i < n * nprjmx && i < DOT_CHUNK * DOT_MAXP; i += blockDim.x)
+      vs[i / nprjmx][i % nprjmx] = __ldg(nz_v + (long)c0 * nprjmx + i);
+    __syncthreads();
+    // gather: warp w takes bands w, w+8, ...; lanes run along the list
+    for (int i = t; i < DOT_CHUNK * DOT_BANDS; i += blockDim.x) {
+      const int e = i % DOT_CHUNK, bb = i / DOT_CHUNK;
+      const int b = b0 + bb;
+      xs[e][bb] = (b < nb && e < n) ? __ldg(psi + (long)b * N + ps[e]) : 0.f;
+    }
+    __syncthreads();
+    float s0 = 0.f, s1 = 0.f;
+    const int j0 = jg, j1 = jg + 8;
+    for (int e = 0; e < n; ++e) {
+      const float x = xs[e][bl];
+      s0 = fmaf(vs[e][j0], x, s0);
+      if (j1 < DOT_MAXP) s1 = fmaf(vs[e][j1], x, s1);
+    }
+    tot[0] += (double)s0;
+    tot[1] += (double)s1;
+    __syncthreads();
+  }
+  const int b = b0 + bl;
+  if (b < nb) {
+    double* r = rp + ((long)b * natom + a) * nprjmx;
+    if (jg < nprjmx) r[jg] = jg < P ? tot[0] : 0.0;
+    if (jg + 8 < nprjmx) r[jg + 8] = jg + 8 < P ? tot[1] : 0.0;
+  }
 }
 
 // ---------------------------------------------------------------- t coefficients
@@ -111,13 +163,17 @@ template <class T>
 int launch_nl_dot(const rs_geom* g, const T* psi, int nb, double* rp, cudaStream_t st) {
   if (nb <= 0 || g->natom == 0) return RS_OK;
   const int P = g->nprjmx;
-  const int bpb = P > 128 ? 1 : 128 / P;
-  const int threads = bpb * P;
-  dim3 grid(g->natom, div_up(nb, bpb));
-  const T* vT;
-  if constexpr (sizeof(T) == 8) vT = (const T*)g->d_vT64; else vT = (const T*)g->d_vT32;
-  k_nl_dot<T><<<grid, threads, 0, st>>>(g->natom, P, g->num_list, g->d_nprj, g->d_natinf,
-                                        g->d_lst, vT, psi, g->N, nb, rp);
+  if constexpr (sizeof(T) == 8) {
+    const int bpb = P > 128 ? 1 : 128 / P;
+    dim3 grid(g->natom, div_up(nb, bpb));
+    k_nl_dot_f64<<<grid, bpb * P, 0, st>>>(g->natom, P, g->d_nprj, g->d_nz_off, g->d_nz_pt,
+                                          g->d_nz_v64, (const double*)psi, g->N, nb, rp);
+  } else {
+    if (P > DOT_MAXP) return fail(RS_EINVAL, "nonlocal dot: more than 16 projectors per atom");
+    dim3 grid(g->natom, div_up(nb, DOT_BANDS));
+    k_nl_dot_f32<<<grid, 256, 0, st>>>(g->natom, P, g->d_nprj, g->d_nz_off, g->d_nz_pt,
+                                       g->d_nz_v32, (const float*)psi, g->N, nb, rp);
+  }
   RS_LAUNCH_CHECK("k_nl_dot");
   return RS_OK;
 }

@@ -57,6 +57,16 @@ struct rs_geom {
   double* d_inv_v64;  // [n_inv*nprjmx]
   float* d_inv_v32;
   int max_inv;      // longest inverse list
+  // points with at least one entry (the projector support), ascending
+  long n_cov;
+  int* d_cov;       // [n_cov] point index
+  int* d_cov_off;   // [n_cov+1] entry range of covered point c (== inv_off[cov[c]])
+  // atom-major compact lists: the nonzero entries of each atom's sphere
+  // (list positions whose projector values are not all zero), in list order
+  int* d_nz_off;    // [natom+1]
+  int* d_nz_pt;     // [nnz] grid point
+  float* d_nz_v32;  // [nnz*nprjmx]
+  double* d_nz_v64; // [nnz*nprjmx]
   // Laplacian coefficients, computed as acfd(m)/dx/dx*(-0.5d0)
   double cx[9], cy[9], cz[9];
 };

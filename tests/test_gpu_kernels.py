@@ -191,3 +191,22 @@ def test_c8_norm_conserving_hpsi(c8, oracle, cuda):
     ref = oracle.hpsi(sysk, psi, rp)
     out = K.hpsi(g, T(veff), T(c8.dij), T(rp), T(psi))
     assert np.array_equal(out.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("n", [(24, 24, 24), (40, 36, 28), (128, 40, 16)])
+def test_hpsi_f32_ragged_tiles(oracle, cuda, built_lib, n):
+    """Grids whose x/y sizes are not multiples of the CTA tile (64 x 32)."""
+    from rspacedist_b200 import kukan as K, system as S
+    ds = S.load_dataset("c_ncps")
+    A = np.array(n) * 0.28
+    pos = S.diamond_positions(1, 1.0, 0.0)[:4] * A - A / 2 + 0.37
+    pos = (pos + A / 2) % A - A / 2
+    cell = S.make_cell(A, n, pos, ds)
+    g = K.Geometry(cell)
+    veff = S.smooth_veff(cell, 5).astype(np.float32)
+    psi = S.random_bands(cell, 3, 6).astype(np.float32)
+    sysk = oracle.make_sys(geo_dict(cell), cell.shape, 4, cell.h, veff, cell.dij, None)
+    rp = oracle.nl_dot(geo_dict(cell), psi, cell.N)
+    ref = oracle.hpsi(sysk, psi, rp)
+    out = K.hpsi(g, T(veff, torch.float32), T(cell.dij), T(rp), T(psi, torch.float32))
+    np.testing.assert_allclose(out.cpu().numpy(), ref, atol=F32_RTOL * np.abs(ref).max())
