@@ -123,6 +123,27 @@ int rs_hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, dou
                   double epsvh, int ncgmin, int ncgmax, int ncgres, const double* rho,
                   double* vh, int* iters, double* dp, void* stream);
 
+/* ---- subspace contractions (GS / Rayleigh-Ritz) ------------------------- */
+/* C(dev, FP64, column-major ldc) = alpha * A^T B where A and B hold m and n
+ * bands of K grid points (band i at A + i*lda): the Gram products of
+ * rayleighritz_r (rayleigh-ritz8f.F90:80, dgemm 't','n') and of the GS blocks
+ * (orthogonalization8f.F90:225-228).  FP32 operands run on tcgen05 tensor
+ * cores with the 3xTF32 split and FP32 accumulation over K chunks of 16384,
+ * chunks summed in FP64; sym=1 (A==B, m==n) computes one triangle and
+ * mirrors it.  K, lda, ldb multiples of 4. */
+int rs_gram_f32(int m, int n, long K, const float* A, long lda, const float* B, long ldb,
+                double alpha, double* C, long ldc, int sym, void* stream);
+int rs_gram_f64(int m, int n, long K, const double* A, long lda, const double* B, long ldb,
+                double alpha, double* C, long ldc, void* stream);
+/* Y(dev) = X Z: band j of Y = sum_k Z(k,j) * band k of X, Z FP64 column-major
+ * (kin x nout, ldz) -- the Psi <- Psi Z updates of rayleighritz_r
+ * (rayleigh-ritz8f.F90:96-119).  FP32: tcgen05 3xTF32 with X read
+ * MN-major; npts and ldx multiples of 4.  Y must not alias X. */
+int rs_rotate_f32(long npts, int kin, int nout, const float* X, long ldx, const double* Z,
+                  long ldz, float* Y, long ldy, void* stream);
+int rs_rotate_f64(long npts, int kin, int nout, const double* X, long ldx, const double* Z,
+                  long ldz, double* Y, long ldy, void* stream);
+
 /* ---- fixed-tree reductions (shared order with the oracle) --------------- */
 /* out(dev, 1 double) = sum_i a_i b_i in the documented block tree. */
 int rs_dot_f64(long n, const double* a, const double* b, double* out, void* stream);

@@ -44,6 +44,10 @@ SIGNATURES = {
     "rs_interp_c2d": [_i, _i, _i, _i, _p, _p, _p],
     "rs_hartree_laplacian": [_i, _i, _i, _i, _d, _d, _d, _p, _p, _p],
     "rs_hartree_cg": [_i, _i, _i, _i, _d, _d, _d, _d, _i, _i, _i, _p, _p, _ip, _dp, _p],
+    "rs_gram_f32": [_i, _i, _l, _p, _l, _p, _l, _d, _p, _l, _i, _p],
+    "rs_gram_f64": [_i, _i, _l, _p, _l, _p, _l, _d, _p, _l, _p],
+    "rs_rotate_f32": [_l, _i, _i, _p, _l, _p, _l, _p, _l, _p],
+    "rs_rotate_f64": [_l, _i, _i, _p, _l, _p, _l, _p, _l, _p],
     "rs_dot_f64": [_l, _p, _p, _p, _p],
     "rs_dot_f32": [_l, _p, _p, _p, _p],
 }
