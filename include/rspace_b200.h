@@ -144,6 +144,97 @@ int rs_rotate_f32(long npts, int kin, int nout, const float* X, long ldx, const 
 int rs_rotate_f64(long npts, int kin, int nout, const double* X, long ldx, const double* Z,
                   long ldz, double* Y, long ldy, void* stream);
 
+/* Symmetric eigenproblem on the GPU in FP64 (parallel cyclic Jacobi): the
+ * dsyev('v','l') / pdsyevd of rayleighritz_r (rayleigh-ritz8f.F90:89,
+ * rayleigh-ritz8f_sclpck.F90:268).  A (dev, n x n) is destroyed; w (dev)
+ * ascending eigenvalues; Z (dev, column-major) eigenvectors, each with its
+ * largest-magnitude component positive.  RS_ENUMERIC without convergence
+ * (kukan: 'error in matrix diagonalization'). */
+int rs_syev_f64(int n, double* A, double* w, double* Z, int* sweeps, void* stream);
+/* Cholesky-QR helper: G = L L^T (dev, FP64, overwritten by L) and
+ * W = L^{-T} (dev, column-major upper triangular), so that Psi W is
+ * S-orthonormal with the span and ordering of kukan's Gram-Schmidt.
+ * RS_ENUMERIC when G is not positive definite ('wf has negative norm',
+ * orthogonalization8f.F90:249). */
+int rs_chol_inv_t(int n, double* G, double* W, void* stream);
+
+/* ---- band solvers (scf_diag and what it calls) -------------------------- */
+/* Solver parameters with kukan's namelist names and defaults
+ * (read_input_kukan8f.F90:198-249): northo=1, nsdmax=4, nprecon_cg=1,
+ * nprecon_diis=1, epssd=1e-6, ndiismax=4, eps_eig_diis=1e-14,
+ * alambda_diis=0.5, alambda_min=0.1, alambda_max=1.0, nrrz=1, nchange=1,
+ * ncgscf=200, nretcg=2000. */
+typedef struct rs_solver_prm {
+  int northo, nsdmax, nprecon_cg, nprecon_diis, ndiismax;
+  int nrrz, nchange, ncgscf, nretcg;
+  double epssd, eps_eig_diis, alambda_diis, alambda_min, alambda_max;
+} rs_solver_prm;
+
+/* Band arrays: psi, spsi (S psi; pass sss=NULL and spsi=psi for
+ * norm-conserving S=1), hpsi (M bands each), rp (<p|psi>, M x natom x nprjmx),
+ * all device; sval / resid host arrays of M doubles.  _f64 = plain FP64
+ * path, _f32 = mixed path (FP32 band arrays, FP64 rp, dots and matrices);
+ * veff has the band arrays' precision. */
+
+/* orthogonalization_r_01 with l_inp=0 (orthogonalization8f.F90:93-376): all
+ * bands S-orthonormalised in order by Cholesky-QR (tensor-core Gram and
+ * rotation for _f32); cmpt recomputes <p|psi> and S psi first
+ * (key_ortho_cmpt_innerproduct). */
+int rs_orthogonalize_f64(const rs_geom* g, const double* sss, int M, double* psi, double* spsi,
+                         double* rp, int cmpt, void* stream);
+int rs_orthogonalize_f32(const rs_geom* g, const double* sss, int M, float* psi, float* spsi,
+                         double* rp, int cmpt, void* stream);
+/* orthogonalization_r_01 with l_inp=l+1: band l against bands 0..l-1 and
+ * normalised (the level-1 path used inside kscg_r). */
+int rs_orthogonalize_band_f64(const rs_geom* g, const double* sss, int M, int l, double* psi,
+                              double* spsi, double* rp, int cmpt, void* stream);
+int rs_orthogonalize_band_f32(const rs_geom* g, const double* sss, int M, int l, float* psi,
+                              float* spsi, double* rp, int cmpt, void* stream);
+/* rayleighritz_r (rayleigh-ritz8f.F90:22-125): l_rrb recomputes H psi into
+ * hpsi first (rayleighritz_hamiltonian_r); hpsi is work space on exit. */
+int rs_rayleighritz_f64(const rs_geom* g, const double* veff, const double* dij,
+                        const double* sss, int M, double* psi, double* spsi, double* rp,
+                        double* hpsi, int l_rrb, double* sval, void* stream);
+int rs_rayleighritz_f32(const rs_geom* g, const float* veff, const double* dij,
+                        const double* sss, int M, float* psi, float* spsi, double* rp,
+                        float* hpsi, int l_rrb, double* sval, void* stream);
+/* kscg_r (kscg8f.F90:7-489): band-by-band preconditioned CG with the 2x2
+ * Rayleigh-Ritz update; itmax = max iterations over bands. */
+int rs_kscg_f64(const rs_geom* g, const double* veff, const double* dij, const double* sss,
+                const rs_solver_prm* prm, int M, double* psi, double* spsi, double* rp,
+                double* hpsi, double* sval, double* resid, int* itmax, void* stream);
+int rs_kscg_f32(const rs_geom* g, const float* veff, const double* dij, const double* sss,
+                const rs_solver_prm* prm, int M, float* psi, float* spsi, double* rp,
+                float* hpsi, double* sval, double* resid, int* itmax, void* stream);
+/* ksdiis_r (ksdiis8f.F90:8-712): RMM-DIIS sweeps with one trial step per
+ * band; l_hsv orthogonalises all bands and recomputes H psi afterwards.
+ * resid is read (bands whose 2x2 solve degenerates keep their value). */
+int rs_ksdiis_f64(const rs_geom* g, const double* veff, const double* dij, const double* sss,
+                  const rs_solver_prm* prm, int M, int l_hsv, double* psi, double* spsi,
+                  double* rp, double* hpsi, double* sval, double* resid, int* ksconv,
+                  void* stream);
+int rs_ksdiis_f32(const rs_geom* g, const float* veff, const double* dij, const double* sss,
+                  const rs_solver_prm* prm, int M, int l_hsv, float* psi, float* spsi,
+                  double* rp, float* hpsi, double* sval, double* resid, int* ksconv,
+                  void* stream);
+/* reorderstates (reorderstates8f.F90:8-124): stable ascending order of sval;
+ * psi, spsi, rp, sval, resid permuted. */
+int rs_reorder_f64(const rs_geom* g, const double* sss, int M, double* psi, double* spsi,
+                   double* rp, double* sval, double* resid, void* stream);
+int rs_reorder_f32(const rs_geom* g, const double* sss, int M, float* psi, float* spsi,
+                   double* rp, double* sval, double* resid, void* stream);
+/* scf_diag (scf_diag8f.F90:6-316), real path, one k-point and spin: RR
+ * before (nrrz>0) or after (nrrz<0), CG while iscf<=ncgscf or every nretcg,
+ * DIIS otherwise, reorder every nchange. */
+int rs_scf_diag_f64(const rs_geom* g, const double* veff, const double* dij, const double* sss,
+                    const rs_solver_prm* prm, int iscf, int M, double* psi, double* spsi,
+                    double* rp, double* hpsi, double* sval, double* resid, int* ksconv,
+                    int* ksitmax, void* stream);
+int rs_scf_diag_f32(const rs_geom* g, const float* veff, const double* dij, const double* sss,
+                    const rs_solver_prm* prm, int iscf, int M, float* psi, float* spsi,
+                    double* rp, float* hpsi, double* sval, double* resid, int* ksconv,
+                    int* ksitmax, void* stream);
+
 /* ---- fixed-tree reductions (shared order with the oracle) --------------- */
 /* out(dev, 1 double) = sum_i a_i b_i in the documented block tree. */
 int rs_dot_f64(long n, const double* a, const double* b, double* out, void* stream);

@@ -565,6 +565,10 @@ int orc_jacobi_eig(int n, double* a_in, double* w, double* z) {
           z[k * n + p] = c * zkp - s * zkq;
           z[k * n + q] = s * zkp + c * zkq;
         }
+        /* the annihilated pair is zero by construction; its computed value
+           is rounding noise of size eps*|a_pp| */
+        a[p * n + q] = 0.0;
+        a[q * n + p] = 0.0;
       }
   }
   for (int i = 0; i < n; ++i) w[i] = a[i * n + i];

@@ -1,0 +1,922 @@
+// bands.cu -- band solvers of scf_diag on the GPU: Gram-Schmidt in the S
+// metric, Rayleigh-Ritz, band-by-band preconditioned CG (kscg_r), RMM-DIIS
+// (ksdiis_r), reordering (reorderstates) and the dispatcher (scf_diag).
+//
+// Vectors are T = double (plain FP64 path) or T = float (mixed path: FP32
+// wavefunctions, FP64 dots, coefficients and small matrices).  With T =
+// double every per-band vector operation is the fma the Fortran statement
+// contracts to and every dot product uses the fixed tree of reduce.cuh, so
+// the CG and DIIS band updates reproduce the strict CPU restatement bit for
+// bit; the block orthogonalisation (Cholesky-QR) and Rayleigh-Ritz go through
+// GEMMs and an eigensolver and agree to rounding.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "reduce.cuh"
+#include "rs_common.cuh"
+#include "stencil.cuh"
+
+namespace rs {
+
+// kernels implemented elsewhere
+template <class T>
+int launch_nl_dot(const rs_geom* g, const T* psi, int nb, double* rp, cudaStream_t st);
+template <class T, int MODE>
+int launch_gather(const rs_geom* g, const double* mat, const double* rp, const T* psi,
+                  const T* veff, T* out, int nb, cudaStream_t st);
+int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
+                         const double* rp, const float* psi, float* hpsi, int nb,
+                         cudaStream_t st);
+int gram_f32(int m, int n, long K, const float* A, long lda, const float* B, long ldb,
+             double alpha, double* C, long ldc, int sym, cudaStream_t st);
+int gram_f64(int m, int n, long K, const double* A, long lda, const double* B, long ldb,
+             double alpha, double* C, long ldc, cudaStream_t st);
+int rotate_f32(long npts, int kin, int nout, const float* X, long ldx, const double* Z, long ldz,
+               float* Y, long ldy, cudaStream_t st);
+int rotate_f64(long npts, int kin, int nout, const double* X, long ldx, const double* Z, long ldz,
+               double* Y, long ldy, cudaStream_t st);
+int syev_jacobi(int n, double* A, double* w, double* Z, int max_sweeps, cudaStream_t st,
+                int* sweeps_out);
+int chol_inv_t(int n, double* G, double* W, cudaStream_t st);
+
+namespace {
+
+// ------------------------------------------------------------ vector kernels
+// out[j] = tree_dot(Y_j, x) * dx * dy * dz  (j < cnt), partial pass
+template <class T>
+__global__ void k_bdot_partial(long n, const T* __restrict__ Y, long ldy, const T* __restrict__ x,
+                               long nblk, double* __restrict__ part) {
+  __shared__ double ws[8];
+  const int j = blockIdx.y;
+  const T* y = Y + (long)j * ldy;
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < kTreePerLane; ++k) {
+    const long i = base + (long)k * kTreeLanes;
+    if (i < n) acc = fma((double)y[i], (double)x[i], acc);
+  }
+  const double s = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) part[(long)j * nblk + blockIdx.x] = s;
+}
+
+__global__ void k_bdot_final(long nblk, const double* __restrict__ part, double dx, double dy,
+                             double dz, int scale, double* __restrict__ out) {
+  __shared__ double ws[8];
+  const int j = blockIdx.x;
+  double acc = 0.0;
+  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + part[(long)j * nblk + k];
+  const double s = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) out[j] = scale ? s * dx * dy * dz : s;
+}
+
+// x -= sum_{j<cnt} c[j] y_j, j in order (orthogonalization_r_03 / multr)
+template <class T>
+__global__ void k_subcomb(long n, T* __restrict__ x, const T* __restrict__ Y, long ldy,
+                          const double* __restrict__ c, int cnt) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = (double)x[i];
+  for (int j = 0; j < cnt; ++j) v = fma(-c[j], (double)Y[(long)j * ldy + i], v);
+  x[i] = (T)v;
+}
+// double-precision rp vectors
+__global__ void k_subcomb_d(long n, double* __restrict__ x, const double* __restrict__ Y,
+                            long ldy, const double* __restrict__ c, int cnt) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = x[i];
+  for (int j = 0; j < cnt; ++j) v = fma(-c[j], Y[(long)j * ldy + i], v);
+  x[i] = v;
+}
+
+// x *= 1/sqrt(*nrm) for up to three vectors (the third is the rp vector)
+template <class T>
+__global__ void k_scale3(long n, T* __restrict__ a, T* __restrict__ b, long nrp,
+                         double* __restrict__ r, const double* __restrict__ tmp) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const double t = *tmp;
+  if (i < n) {
+    a[i] = (T)((double)a[i] * t);
+    if (b) b[i] = (T)((double)b[i] * t);
+  }
+  if (i < nrp) r[i] = r[i] * t;
+}
+
+// tmp = 1/sqrt(vecnor); status 1 when vecnor <= 0 (kukan's 'negative norm')
+__global__ void k_invsqrt(const double* __restrict__ vecnor, double* __restrict__ tmp,
+                          int* __restrict__ status) {
+  const double v = *vecnor;
+  if (!(v > 0.0)) {
+    *status = 1;
+    *tmp = 1.0;
+  } else {
+    *tmp = 1.0 / sqrt(v);
+  }
+}
+
+// rvec = -(h - lambda s)   (kscg_r_02)
+template <class T>
+__global__ void k_resid(long n, const T* __restrict__ h, const T* __restrict__ s,
+                        const double* __restrict__ lam, T* __restrict__ r) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  r[i] = (T)(-fma(-*lam, (double)s[i], (double)h[i]));
+}
+
+// c = a + d*b  (ksdiis_r_01), d = sign * (*dp)
+template <class T>
+__global__ void k_axpy(long n, const T* __restrict__ a, const T* __restrict__ b,
+                       const double* __restrict__ dp, double sign, T* __restrict__ c) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double d = sign * *dp;
+  c[i] = (T)fma(d, (double)b[i], (double)a[i]);
+}
+__global__ void k_axpy_d(long n, const double* __restrict__ a, const double* __restrict__ b,
+                         const double* __restrict__ dp, double* __restrict__ c) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  c[i] = fma(*dp, b[i], a[i]);
+}
+
+// kscg_r_03 on the grid vectors and the rp vectors
+template <class T>
+__global__ void k_cg_dir(long n, T* __restrict__ pvec, const T* __restrict__ rv,
+                         T* __restrict__ pv, T* __restrict__ spv, const T* __restrict__ asv,
+                         long nrp, double* __restrict__ rpp, const double* __restrict__ rrp,
+                         const double* __restrict__ sc /* ratio at sc[0] */) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const double ratio = sc[0];
+  if (i < n) {
+    const T p = (T)fma(ratio, (double)pv[i], (double)rv[i]);
+    pv[i] = p;
+    pvec[i] = p;
+    if (spv) spv[i] = (T)fma(ratio, (double)spv[i], (double)asv[i]);
+  }
+  if (i < nrp) rpp[i] = fma(ratio, rpp[i], rrp[i]);
+}
+
+// kscg_r_05 rotation x = alph x + beta y on psi, hpsi, spsi and rp
+template <class T>
+__global__ void k_cg_rot(long n, T* __restrict__ psi, const T* __restrict__ p, T* __restrict__ h,
+                         const T* __restrict__ ap, T* __restrict__ s, const T* __restrict__ as,
+                         long nrp, double* __restrict__ rp, const double* __restrict__ rpl,
+                         const double* __restrict__ sc /* alph, beta at sc[0..1] */) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const double al = sc[0], be = sc[1];
+  if (i < n) {
+    psi[i] = (T)fma(be, (double)p[i], al * (double)psi[i]);
+    h[i] = (T)fma(be, (double)ap[i], al * (double)h[i]);
+    if (s) s[i] = (T)fma(be, (double)as[i], al * (double)s[i]);
+  }
+  if (i < nrp) rp[i] = fma(be, rpl[i], al * rp[i]);
+}
+
+// new = c1 y1 + c0 y0 (ksdiis_r_03 with two vectors); rp form starts from 0
+template <class T>
+__global__ void k_comb2(long n, const T* __restrict__ y0, const T* __restrict__ y1,
+                        const double* __restrict__ c, T* __restrict__ out) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = (T)fma(c[1], (double)y1[i], c[0] * (double)y0[i]);
+}
+__global__ void k_comb2_rp(long n, const double* __restrict__ y0, const double* __restrict__ y1,
+                           const double* __restrict__ c, double* __restrict__ out) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double acc = 0.0;
+  acc = fma(c[0], y0[i], acc);
+  acc = fma(c[1], y1[i], acc);
+  out[i] = acc;
+}
+
+// ------------------------------------------------------------ scalar kernels
+// device scalars of one band step
+struct Sc {
+  double valre, r1rr, r2rr, ratio, vecnor, tmp, pap, sapre, ab[2];
+  double s[4];            // DIIS line-search sums
+  double lam;             // DIIS step
+  double rs[4], rr[4];    // 2x2 matrices, rs[i*2+j]
+  double c[2];            // DIIS combination
+  double coef_dummy;
+  int status;
+};
+
+__global__ void k_cg_ratio(Sc* sc) { sc->ratio = sc->r2rr / sc->r1rr; }
+
+// kscg_r_05: 2x2 Rayleigh-Ritz in span{psi, p}
+__global__ void k_cg_alphabeta(Sc* sc, const double* __restrict__ sval) {
+  const double sv = *sval, pap = sc->pap, sapre = sc->sapre, eps = 1.0e-14;
+  double alph = 1.0, beta = 0.0;
+  const double gamma = (sv + pap) * 0.5 - sqrt((sv - pap) * (sv - pap) * 0.25 + sapre * sapre);
+  if (fabs((sv - gamma) / gamma) > eps) {
+    const double den = sqrt(sapre * sapre + (sv - gamma) * (sv - gamma));
+    alph = sapre / den;
+    beta = -(sv - gamma) / den;
+  }
+  if (alph < eps) {
+    alph = -alph;
+    beta = -beta;
+  }
+  sc->ab[0] = alph;
+  sc->ab[1] = beta;
+}
+
+// DIIS step length (ksdiis8f.F90:285-320)
+__global__ void k_diis_lambda(Sc* sc, const double* __restrict__ sval, double a1, double dx,
+                              double dy, double dz, double lmin, double lmax) {
+  const double sv = *sval;
+  const double aaa = 2.0 * fma(-sv, sc->s[1], sc->s[0]) * dx * dy * dz;
+  const double valre = sc->s[2] / sc->s[3];
+  const double bbb = fma(-aaa, a1, valre - sv) / (a1 * a1);
+  double al = 0.5 * aaa / bbb;
+  if (al > lmax) al = lmax;
+  if (al < lmin) al = lmin;
+  sc->lam = al;
+}
+
+__global__ void k_diis_norm(Sc* sc) { sc->tmp = 1.0 / sqrt(sc->rs[3]); }
+
+__device__ void eig2(const double a[4], double w[2], double z[4]) {
+  const double p = a[0], q = a[3], r = 0.5 * (a[1] + a[2]);
+  const double mean = 0.5 * (p + q), half = 0.5 * (p - q);
+  const double rad = sqrt(half * half + r * r);
+  w[0] = mean - rad;
+  w[1] = mean + rad;
+  if (r == 0.0) {
+    if (p <= q) { z[0] = 1.0; z[2] = 0.0; z[1] = 0.0; z[3] = 1.0; }
+    else        { z[0] = 0.0; z[2] = 1.0; z[1] = 1.0; z[3] = 0.0; }
+    return;
+  }
+  double u0, u1;
+  if (half >= 0.0) { u0 = half + rad; u1 = r; }
+  else             { u0 = r; u1 = rad - half; }
+  const double nu = sqrt(u0 * u0 + u1 * u1);
+  u0 /= nu; u1 /= nu;
+  double v0 = -u1, v1 = u0;
+  if (fabs(u1) > fabs(u0) ? u1 < 0.0 : u0 < 0.0) { u0 = -u0; u1 = -u1; }
+  if (fabs(v1) > fabs(v0) ? v1 < 0.0 : v0 < 0.0) { v0 = -v0; v1 = -v1; }
+  z[0] = v0; z[2] = v1;
+  z[1] = u0; z[3] = u1;
+}
+
+// DIIS 2x2 subspace solve (ksdiis8f.F90:405-548); rs/rr already scaled
+__global__ void k_diis_solve(Sc* sc, double eps_eig, double* __restrict__ resid) {
+  double rs[4], rr[4], rs0[4];
+  for (int k = 0; k < 4; ++k) { rs[k] = sc->rs[k]; rr[k] = sc->rr[k]; rs0[k] = rs[k]; }
+  double w[2], z[4], eig[2], vec[4];
+  eig2(rs, w, z);
+  for (int k = 0; k < 2; ++k) {
+    eig[k] = w[1 - k];
+    vec[0 * 2 + k] = z[0 * 2 + (1 - k)];
+    vec[1 * 2 + k] = z[1 * 2 + (1 - k)];
+  }
+  int nmat = 0, k = 0;
+  while (k < 2) {
+    ++nmat; ++k;
+    if (eig[nmat - 1] < eps_eig) --nmat;
+  }
+  double c[2];
+  if (nmat > 1) {
+    for (int i = 0; i < 2; ++i) {
+      const double sq = sqrt(eig[i]);
+      vec[0 * 2 + i] /= sq;
+      vec[1 * 2 + i] /= sq;
+    }
+    double t[4] = {0, 0, 0, 0}, r2[4] = {0, 0, 0, 0};
+    for (int kk = 0; kk < 2; ++kk)
+      for (int j = 0; j < 2; ++j)
+        for (int i = 0; i < 2; ++i) t[kk * 2 + j] = fma(rr[kk * 2 + i], vec[i * 2 + j], t[kk * 2 + j]);
+    for (int kk = 0; kk < 2; ++kk)
+      for (int j = 0; j < 2; ++j)
+        for (int i = 0; i < 2; ++i) r2[kk * 2 + j] = fma(vec[i * 2 + kk], t[i * 2 + j], r2[kk * 2 + j]);
+    double w2[2], z2[4], v2[4];
+    eig2(r2, w2, z2);
+    for (int kk = 0; kk < 2; ++kk) {
+      v2[0 * 2 + kk] = z2[0 * 2 + (1 - kk)];
+      v2[1 * 2 + kk] = z2[1 * 2 + (1 - kk)];
+    }
+    *resid = w2[0];
+    for (int j = 0; j < 2; ++j) {
+      double acc = 0.0;
+      for (int i = 0; i < 2; ++i) acc = fma(vec[j * 2 + i], v2[i * 2 + 1], acc);
+      c[j] = acc;
+    }
+    double nrm = 0.0;
+    for (int j = 0; j < 2; ++j)
+      for (int i = 0; i < 2; ++i) nrm = fma(c[i] * rs0[i * 2 + j], c[j], nrm);
+    const double sq = sqrt(nrm);
+    c[0] /= sq;
+    c[1] /= sq;
+  } else {
+    c[0] = 0.0;
+    c[1] = 1.0;
+  }
+  sc->c[0] = c[0];
+  sc->c[1] = c[1];
+}
+
+// scale row/column 2 of the DIIS matrices by tmp (rs(2,2) twice)
+__global__ void k_diis_scale_mats(Sc* sc) {
+  const double t = sc->tmp;
+  for (int i = 0; i < 2; ++i) { sc->rs[1 * 2 + i] *= t; sc->rr[1 * 2 + i] *= t; }
+  for (int i = 0; i < 2; ++i) { sc->rs[i * 2 + 1] *= t; sc->rr[i * 2 + 1] *= t; }
+}
+
+__global__ void k_copy_d(double* dst, const double* src) { *dst = *src; }
+
+__global__ void k_gather_bands_d(long n, int M, const int* __restrict__ rank,
+                                 const double* __restrict__ src, double* __restrict__ dst) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * M) return;
+  const int j = (int)(i / n);
+  dst[(long)rank[j] * n + (i % n)] = src[i];
+}
+template <class T>
+__global__ void k_permute_bands(long n, int M, const int* __restrict__ rank,
+                                const T* __restrict__ src, T* __restrict__ dst) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * M) return;
+  const int j = (int)(i / n);
+  dst[(long)rank[j] * n + (i % n)] = src[i];
+}
+
+}  // namespace
+
+// ============================================================ the solver
+template <class T>
+struct BandCtx {
+  const rs_geom* g;
+  const T* veff;
+  const double* dij;
+  const double* sss;  // nullptr: S = 1 (spsi aliases psi)
+  int M;
+  T* psi;
+  T* spsi;
+  double* rp;
+  T* hpsi;
+  cudaStream_t st;
+  long N;
+  int nrp;
+  double dx, dy, dz;
+  // work
+  double* part = nullptr;
+  long nblk = 0;
+  double* coef = nullptr;  // M+1
+  Sc* sc = nullptr;
+  T* w[8] = {};
+  double* wrp[6] = {};
+  int status_err = RS_OK;
+
+  bool sep() const { return sss != nullptr; }
+
+  int init(int nvec, int nrpv) {
+    N = g->N;
+    nrp = g->natom * g->nprjmx;
+    dx = g->dx; dy = g->dy; dz = g->dz;
+    nblk = tree_chunks(N);
+    RS_CUDA(cudaMallocAsync((void**)&part, sizeof(double) * nblk * (M + 2), st));
+    RS_CUDA(cudaMallocAsync((void**)&coef, sizeof(double) * (M + 2), st));
+    RS_CUDA(cudaMallocAsync((void**)&sc, sizeof(Sc), st));
+    RS_CUDA(cudaMemsetAsync(sc, 0, sizeof(Sc), st));
+    for (int k = 0; k < nvec; ++k) {
+      RS_CUDA(cudaMallocAsync((void**)&w[k], sizeof(T) * N, st));
+      RS_CUDA(cudaMemsetAsync(w[k], 0, sizeof(T) * N, st));
+    }
+    for (int k = 0; k < nrpv; ++k) {
+      RS_CUDA(cudaMallocAsync((void**)&wrp[k], sizeof(double) * (nrp > 0 ? nrp : 1), st));
+      RS_CUDA(cudaMemsetAsync(wrp[k], 0, sizeof(double) * (nrp > 0 ? nrp : 1), st));
+    }
+    return RS_OK;
+  }
+  void release() {
+    if (part) cudaFreeAsync(part, st);
+    if (coef) cudaFreeAsync(coef, st);
+    if (sc) cudaFreeAsync(sc, st);
+    for (auto& p : w)
+      if (p) { cudaFreeAsync(p, st); p = nullptr; }
+    for (auto& p : wrp)
+      if (p) { cudaFreeAsync(p, st); p = nullptr; }
+  }
+
+  T* band(T* base, int l) const { return base + (long)l * N; }
+  double* rpb(double* base, int l) const { return base + (long)l * nrp; }
+
+  // out[j] = dot(Y_j, x) (times dV when scale)
+  int bdot(const T* Y, int cnt, const T* x, double* out, int scale = 1) {
+    if (cnt <= 0) return RS_OK;
+    dim3 grid((unsigned)nblk, cnt);
+    k_bdot_partial<T><<<grid, kTreeLanes, 0, st>>>(N, Y, N, x, nblk, part);
+    k_bdot_final<<<cnt, kTreeLanes, 0, st>>>(nblk, part, dx, dy, dz, scale, out);
+    RS_LAUNCH_CHECK("bdot");
+    return RS_OK;
+  }
+  void subcomb(T* x, const T* Y, const double* c, int cnt) {
+    if (cnt > 0) k_subcomb<T><<<div_up(N, 256), 256, 0, st>>>(N, x, Y, N, c, cnt);
+  }
+  void subcomb_rp(double* x, const double* Y, const double* c, int cnt) {
+    if (cnt > 0 && nrp > 0) k_subcomb_d<<<div_up(nrp, 256), 256, 0, st>>>(nrp, x, Y, nrp, c, cnt);
+  }
+  int apply_h(const T* x, const double* r, T* out, int nb) {
+    if constexpr (sizeof(T) == 4)
+      return launch_hpsi_f32_fast(g, (const float*)veff, dij, r, (const float*)x, (float*)out, nb, st);
+    else
+      return launch_gather<double, 1>(g, dij, r, (const double*)x, (const double*)veff,
+                                      (double*)out, nb, st);
+  }
+  int apply_s(const T* x, const double* r, T* out, int nb) {
+    if (!sss) {
+      if (out != x) RS_CUDA(cudaMemcpyAsync(out, x, sizeof(T) * N * nb, cudaMemcpyDeviceToDevice, st));
+      return RS_OK;
+    }
+    return launch_gather<T, 2>(g, sss, r, x, nullptr, out, nb, st);
+  }
+  int nl_dot(const T* x, double* r, int nb) {
+    if (g->natom == 0) return RS_OK;
+    return launch_nl_dot<T>(g, x, nb, r, st);
+  }
+  int precond(const T* in, T* out) { return launch_precondition<T>(g, in, out, 1, st); }
+  unsigned gN() const { return div_up(std::max(N, (long)nrp), 256); }
+
+  // normalise x (and sx, r) by 1/sqrt(dot(x, sx) dV)
+  int normalize(T* x, T* sx, double* r) {
+    int rc;
+    if ((rc = bdot(sx, 1, x, &sc->vecnor))) return rc;
+    k_invsqrt<<<1, 1, 0, st>>>(&sc->vecnor, &sc->tmp, &sc->status);
+    k_scale3<T><<<gN(), 256, 0, st>>>(N, x, sep() ? sx : nullptr, nrp, r, &sc->tmp);
+    RS_LAUNCH_CHECK("normalize");
+    return RS_OK;
+  }
+
+  // orthogonalization_r_01 for the single band l (l_inp = l+1), level-1 GS
+  int ortho_band(int l, bool cmpt) {
+    int rc;
+    T* x = band(psi, l);
+    T* sx = band(spsi, l);
+    double* r = rpb(rp, l);
+    if (cmpt) {
+      if ((rc = nl_dot(x, r, 1))) return rc;
+      if (sep() && (rc = apply_s(x, r, sx, 1))) return rc;
+    }
+    if (l > 0) {
+      // coef[j] = dot(spsi_j, psi_l) dV
+      if ((rc = bdot(spsi, l, x, coef))) return rc;
+      subcomb(x, psi, coef, l);
+      if (sep()) subcomb(sx, spsi, coef, l);
+      subcomb_rp(r, rp, coef, l);
+    }
+    return normalize(x, sx, r);
+  }
+
+  // Cholesky-QR of all bands in the S metric (block GS of
+  // orthogonalization_r_01 with l_inp=0): G = dV Psi^T S Psi = L L^T,
+  // Psi <- Psi L^-T, S Psi and <p|Psi> likewise.
+  int ortho_all(bool cmpt) {
+    int rc;
+    if (cmpt) {
+      if ((rc = nl_dot(psi, rp, M))) return rc;
+      if (sep() && (rc = apply_s(psi, rp, spsi, M))) return rc;
+    }
+    double *G = nullptr, *W = nullptr;
+    RS_CUDA(cudaMallocAsync((void**)&G, sizeof(double) * 2 * (size_t)M * M, st));
+    W = G + (size_t)M * M;
+    const double dv = dx * dy * dz;
+    if constexpr (sizeof(T) == 4)
+      rc = gram_f32(M, M, N, (const float*)psi, N, (const float*)spsi, N, dv, G, M,
+                    spsi == psi, st);
+    else
+      rc = gram_f64(M, M, N, (const double*)psi, N, (const double*)spsi, N, dv, G, M, st);
+    if (!rc) rc = chol_inv_t(M, G, W, st);
+    if (!rc) rc = rotate_all(W);
+    cudaFreeAsync(G, st);
+    return rc;
+  }
+
+  // Psi <- Psi Z, S Psi <- S Psi Z, <p|Psi> <- <p|Psi> Z (Z FP64 M x M)
+  int rotate_all(const double* Z) {
+    int rc = RS_OK;
+    T* tmp = nullptr;
+    RS_CUDA(cudaMallocAsync((void**)&tmp, sizeof(T) * (size_t)N * M, st));
+    T* arrs[2] = {psi, sep() ? spsi : nullptr};
+    for (T* a : arrs) {
+      if (!a || rc) continue;
+      if constexpr (sizeof(T) == 4)
+        rc = rotate_f32(N, M, M, (const float*)a, N, Z, M, (float*)tmp, N, st);
+      else
+        rc = rotate_f64(N, M, M, (const double*)a, N, Z, M, (double*)tmp, N, st);
+      if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(a, tmp, sizeof(T) * (size_t)N * M,
+                                        cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) rc = cuda_status(e, "rotate copy");
+      }
+    }
+    cudaFreeAsync(tmp, st);
+    if (rc || nrp == 0) return rc;
+    double* tr = nullptr;
+    RS_CUDA(cudaMallocAsync((void**)&tr, sizeof(double) * (size_t)nrp * M, st));
+    rc = rotate_f64(nrp, M, M, rp, nrp, Z, M, tr, nrp, st);
+    if (!rc) RS_CUDA(cudaMemcpyAsync(rp, tr, sizeof(double) * (size_t)nrp * M,
+                                     cudaMemcpyDeviceToDevice, st));
+    cudaFreeAsync(tr, st);
+    return rc;
+  }
+
+  int check_status() {
+    int h = 0;
+    RS_CUDA(cudaMemcpyAsync(&h, &sc->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RS_CUDA(cudaStreamSynchronize(st));
+    if (h) return fail(RS_ENUMERIC, "band solver: vector has negative norm");
+    return RS_OK;
+  }
+};
+
+template <class T>
+static int kscg(BandCtx<T>& c, const rs_solver_prm* prm, double* sval_h, double* resid_h,
+                int* itmax) {
+  int rc = c.init(7, 4);
+  if (rc) return rc;
+  const long N = c.N;
+  T *rvec = c.w[0], *pvec = c.w[1], *pv = c.w[2], *rv = c.w[3], *spv = c.w[4], *asv = c.w[5],
+    *av = c.w[6];
+  double *rrp = c.wrp[0], *rpp = c.wrp[1], *rpl = c.wrp[2], *dsval = c.wrp[3];
+  double* dval = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&dval, sizeof(double) * (c.M + 1), c.st));
+  const int nsdmax1 = 10, nsdmax2 = 200;
+  int itm = 0;
+  for (int l = 0; l < c.M && !rc; ++l) {
+    T* psl = c.band(c.psi, l);
+    T* ssl = c.band(c.spsi, l);
+    T* hsl = c.band(c.hpsi, l);
+    double* rpsl = c.rpb(c.rp, l);
+    for (int loop = 0; loop < prm->northo && !rc; ++loop) rc = c.ortho_band(l, prm->northo == 2);
+    if (!rc) rc = c.apply_h(psl, rpsl, hsl, 1);
+    int iiter = 0;
+    bool conv = false;
+    while (!rc && iiter < prm->nsdmax && !conv) {
+      ++iiter;
+      bool reset = (iiter == 1) || (iiter == nsdmax1);
+      if (nsdmax2 > 0) reset = reset || ((iiter - 1) % nsdmax2 == 0);
+      if (reset) {
+        const double one = 1.0;
+        cudaMemcpyAsync(&c.sc->r2rr, &one, sizeof(double), cudaMemcpyHostToDevice, c.st);
+        cudaMemsetAsync(pvec, 0, sizeof(T) * N, c.st);
+        cudaMemsetAsync(rvec, 0, sizeof(T) * N, c.st);
+        cudaMemsetAsync(pv, 0, sizeof(T) * N, c.st);
+        cudaMemsetAsync(spv, 0, sizeof(T) * N, c.st);
+        if (c.nrp) cudaMemsetAsync(rpp, 0, sizeof(double) * c.nrp, c.st);
+      }
+      k_copy_d<<<1, 1, 0, c.st>>>(&c.sc->r1rr, &c.sc->r2rr);
+      if ((rc = c.bdot(psl, 1, hsl, &c.sc->valre))) break;
+      k_copy_d<<<1, 1, 0, c.st>>>(dval + l, &c.sc->valre);
+      k_resid<T><<<div_up(N, 256), 256, 0, c.st>>>(N, hsl, ssl, &c.sc->valre, rvec);
+      if (prm->nprecon_cg) rc = c.precond(rvec, rv);
+      else cudaMemcpyAsync(rv, rvec, sizeof(T) * N, cudaMemcpyDeviceToDevice, c.st);
+      for (int loop = 0; loop < prm->northo && !rc; ++loop) {
+        if ((rc = c.bdot(c.spsi, l + 1, rv, c.coef))) break;
+        c.subcomb(rv, c.psi, c.coef, l + 1);
+      }
+      if (rc) break;
+      if ((rc = c.nl_dot(rv, rrp, 1))) break;
+      if ((rc = c.apply_s(rv, rrp, asv, 1))) break;
+      if ((rc = c.bdot(rv, 1, rvec, &c.sc->r2rr))) break;
+      k_copy_d<<<1, 1, 0, c.st>>>(dsval + 0, &c.sc->r2rr);  // resid of this band
+      k_cg_ratio<<<1, 1, 0, c.st>>>(c.sc);
+      k_cg_dir<T><<<c.gN(), 256, 0, c.st>>>(N, pvec, rv, pv, c.sep() ? spv : nullptr, asv,
+                                             c.nrp, rpp, rrp, &c.sc->ratio);
+      if (c.nrp) cudaMemcpyAsync(rpl, rpp, sizeof(double) * c.nrp, cudaMemcpyDeviceToDevice, c.st);
+      if (c.sep()) cudaMemcpyAsync(asv, spv, sizeof(T) * N, cudaMemcpyDeviceToDevice, c.st);
+      else cudaMemcpyAsync(asv, pvec, sizeof(T) * N, cudaMemcpyDeviceToDevice, c.st);
+      for (int loop = 0; loop < prm->northo && !rc; ++loop) {
+        if ((rc = c.bdot(c.spsi, l + 1, pvec, c.coef))) break;
+        c.subcomb(pvec, c.psi, c.coef, l + 1);
+        if (c.sep()) c.subcomb(asv, c.spsi, c.coef, l + 1);
+        else c.subcomb(asv, c.psi, c.coef, l + 1);
+        c.subcomb_rp(rpl, c.rp, c.coef, l + 1);
+      }
+      if (rc) break;
+      if ((rc = c.bdot(asv, 1, pvec, &c.sc->vecnor))) break;
+      k_invsqrt<<<1, 1, 0, c.st>>>(&c.sc->vecnor, &c.sc->tmp, &c.sc->status);
+      k_scale3<T><<<c.gN(), 256, 0, c.st>>>(N, pvec, asv, c.nrp, rpl, &c.sc->tmp);
+      if ((rc = c.apply_h(pvec, rpl, av, 1))) break;
+      if ((rc = c.bdot(pvec, 1, av, &c.sc->pap))) break;
+      if ((rc = c.bdot(psl, 1, av, &c.sc->sapre))) break;
+      k_cg_alphabeta<<<1, 1, 0, c.st>>>(c.sc, dval + l);
+      k_cg_rot<T><<<c.gN(), 256, 0, c.st>>>(N, psl, pvec, hsl, av, c.sep() ? ssl : nullptr, asv,
+                                             c.nrp, rpsl, rpl, c.sc->ab);
+      double r2 = 0.0;
+      int bad = 0;
+      RS_CUDA(cudaMemcpyAsync(&r2, dsval, sizeof(double), cudaMemcpyDeviceToHost, c.st));
+      RS_CUDA(cudaMemcpyAsync(&bad, &c.sc->status, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+      RS_CUDA(cudaStreamSynchronize(c.st));
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) { rc = cuda_status(e, "kscg"); break; }
+      if (bad) { rc = fail(RS_ENUMERIC, "kscg_r: pvec has negative norm"); break; }
+      resid_h[l] = r2;
+      conv = sqrt(r2) < prm->epssd;
+    }
+    if (iiter > itm) itm = iiter;
+  }
+  if (!rc) {
+    RS_CUDA(cudaMemcpyAsync(sval_h, dval, sizeof(double) * c.M, cudaMemcpyDeviceToHost, c.st));
+    RS_CUDA(cudaStreamSynchronize(c.st));
+  }
+  if (itmax) *itmax = itm;
+  cudaFreeAsync(dval, c.st);
+  c.release();
+  return rc;
+}
+
+template <class T>
+static int ksdiis(BandCtx<T>& c, const rs_solver_prm* prm, int l_hsv, double* sval_h,
+                  double* resid_h, int* ksconv) {
+  int rc = c.init(8, 4);
+  if (rc) return rc;
+  const long N = c.N;
+  const bool sp = c.sep();
+  T* ph[2] = {c.w[0], c.w[1]};
+  T* sph[2] = {sp ? c.w[2] : c.w[0], sp ? c.w[3] : c.w[1]};
+  T* hph[2] = {c.w[4], c.w[5]};
+  T* rvv[2] = {c.w[6], c.w[7]};
+  T *rvre = nullptr, *avre = nullptr, *asvre = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&rvre, sizeof(T) * N * 3, c.st));
+  avre = rvre + N;
+  asvre = avre + N;
+  double *rph[2] = {c.wrp[0], c.wrp[1]}, *rpsep = c.wrp[2];
+  double* dval = nullptr;
+  double* dres = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&dval, sizeof(double) * 2 * (c.M + 1), c.st));
+  dres = dval + c.M + 1;
+  RS_CUDA(cudaMemcpyAsync(dres, resid_h, sizeof(double) * c.M, cudaMemcpyHostToDevice, c.st));
+  const double a1 = prm->alambda_diis;
+  double* da1 = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&da1, sizeof(double), c.st));
+  RS_CUDA(cudaMemcpyAsync(da1, &a1, sizeof(double), cudaMemcpyHostToDevice, c.st));
+  const unsigned gN = div_up(N, 256), gR = div_up(c.nrp > 0 ? c.nrp : 1, 256);
+  for (int jiter = 1; jiter + 1 <= prm->ndiismax && !rc; ++jiter) {
+    for (int l = 0; l < c.M && !rc; ++l) {
+      cudaMemcpyAsync(ph[0], c.band(c.psi, l), sizeof(T) * N, cudaMemcpyDeviceToDevice, c.st);
+      if (sp) cudaMemcpyAsync(sph[0], c.band(c.spsi, l), sizeof(T) * N, cudaMemcpyDeviceToDevice, c.st);
+      if (c.nrp) cudaMemcpyAsync(rph[0], c.rpb(c.rp, l), sizeof(double) * c.nrp, cudaMemcpyDeviceToDevice, c.st);
+      if ((rc = c.apply_h(ph[0], rph[0], hph[0], 1))) break;
+      if ((rc = c.bdot(ph[0], 1, hph[0], dval + l))) break;
+      k_axpy<T><<<gN, 256, 0, c.st>>>(N, hph[0], sph[0], dval + l, -1.0, rvv[0]);
+      if (prm->nprecon_diis) rc = c.precond(rvv[0], rvre);
+      else cudaMemcpyAsync(rvre, rvv[0], sizeof(T) * N, cudaMemcpyDeviceToDevice, c.st);
+      if (rc) break;
+      if ((rc = c.nl_dot(rvre, rpsep, 1))) break;
+      if ((rc = c.apply_h(rvre, rpsep, avre, 1))) break;
+      if ((rc = c.apply_s(rvre, rpsep, asvre, 1))) break;
+      // trial step with alambda_diis
+      if (c.nrp) k_axpy_d<<<gR, 256, 0, c.st>>>(c.nrp, rph[0], rpsep, da1, rph[1]);
+      k_axpy<T><<<gN, 256, 0, c.st>>>(N, ph[0], rvre, da1, 1.0, ph[1]);
+      k_axpy<T><<<gN, 256, 0, c.st>>>(N, hph[0], avre, da1, 1.0, hph[1]);
+      if (sp) k_axpy<T><<<gN, 256, 0, c.st>>>(N, sph[0], asvre, da1, 1.0, sph[1]);
+      if ((rc = c.bdot(rvre, 1, hph[0], &c.sc->s[0], 0))) break;
+      if ((rc = c.bdot(rvre, 1, sph[0], &c.sc->s[1], 0))) break;
+      if ((rc = c.bdot(ph[1], 1, hph[1], &c.sc->s[2], 0))) break;
+      if ((rc = c.bdot(ph[1], 1, sph[1], &c.sc->s[3], 0))) break;
+      k_diis_lambda<<<1, 1, 0, c.st>>>(c.sc, dval + l, a1, c.dx, c.dy, c.dz, prm->alambda_min,
+                                       prm->alambda_max);
+      k_axpy<T><<<gN, 256, 0, c.st>>>(N, ph[0], rvre, &c.sc->lam, 1.0, ph[1]);
+      k_axpy<T><<<gN, 256, 0, c.st>>>(N, hph[0], avre, &c.sc->lam, 1.0, hph[1]);
+      if (sp) k_axpy<T><<<gN, 256, 0, c.st>>>(N, sph[0], asvre, &c.sc->lam, 1.0, sph[1]);
+      if (c.nrp) k_axpy_d<<<gR, 256, 0, c.st>>>(c.nrp, rph[0], rpsep, &c.sc->lam, rph[1]);
+      for (int j = 0; j < 2; ++j)
+        k_axpy<T><<<gN, 256, 0, c.st>>>(N, hph[j], sph[j], dval + l, -1.0, rvv[j]);
+      for (int j = 0; j < 2 && !rc; ++j)
+        for (int i = 0; i <= j && !rc; ++i) {
+          if ((rc = c.bdot(ph[i], 1, sph[j], &c.sc->rs[i * 2 + j]))) break;
+          if ((rc = c.bdot(rvv[i], 1, rvv[j], &c.sc->rr[i * 2 + j]))) break;
+          if (i != j) {
+            k_copy_d<<<1, 1, 0, c.st>>>(&c.sc->rs[j * 2 + i], &c.sc->rs[i * 2 + j]);
+            k_copy_d<<<1, 1, 0, c.st>>>(&c.sc->rr[j * 2 + i], &c.sc->rr[i * 2 + j]);
+          }
+        }
+      if (rc) break;
+      k_diis_norm<<<1, 1, 0, c.st>>>(c.sc);
+      k_scale3<T><<<c.gN(), 256, 0, c.st>>>(N, ph[1], hph[1], c.nrp, rph[1], &c.sc->tmp);
+      if (sp) k_scale3<T><<<gN, 256, 0, c.st>>>(N, sph[1], rvv[1], 0, nullptr, &c.sc->tmp);
+      else k_scale3<T><<<gN, 256, 0, c.st>>>(N, rvv[1], nullptr, 0, nullptr, &c.sc->tmp);
+      k_diis_scale_mats<<<1, 1, 0, c.st>>>(c.sc);
+      k_diis_solve<<<1, 1, 0, c.st>>>(c.sc, prm->eps_eig_diis, dres + l);
+      k_comb2<T><<<gN, 256, 0, c.st>>>(N, ph[0], ph[1], c.sc->c, c.band(c.psi, l));
+      if (sp) k_comb2<T><<<gN, 256, 0, c.st>>>(N, sph[0], sph[1], c.sc->c, c.band(c.spsi, l));
+      k_comb2<T><<<gN, 256, 0, c.st>>>(N, hph[0], hph[1], c.sc->c, c.band(c.hpsi, l));
+      if (c.nrp) k_comb2_rp<<<gR, 256, 0, c.st>>>(c.nrp, rph[0], rph[1], c.sc->c, c.rpb(c.rp, l));
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) rc = cuda_status(e, "ksdiis");
+    }
+  }
+  if (!rc) {
+    RS_CUDA(cudaMemcpyAsync(sval_h, dval, sizeof(double) * c.M, cudaMemcpyDeviceToHost, c.st));
+    RS_CUDA(cudaMemcpyAsync(resid_h, dres, sizeof(double) * c.M, cudaMemcpyDeviceToHost, c.st));
+    RS_CUDA(cudaStreamSynchronize(c.st));
+    int conv = 1;
+    for (int l = 0; l < c.M; ++l) conv = conv && (sqrt(resid_h[l]) <= prm->epssd);
+    if (ksconv) *ksconv = conv;
+  }
+  if (!rc && l_hsv) {
+    for (int i = 0; i < prm->northo && !rc; ++i) rc = c.ortho_all(true);
+    if (!rc) rc = c.apply_h(c.psi, c.rp, c.hpsi, c.M);
+  }
+  cudaFreeAsync(rvre, c.st);
+  cudaFreeAsync(dval, c.st);
+  cudaFreeAsync(da1, c.st);
+  c.release();
+  return rc;
+}
+
+// rayleighritz_r: A = dV Psi^T H Psi (lower triangle), eigen, rotations
+template <class T>
+static int rayleighritz(BandCtx<T>& c, int l_rrb, double* sval_h) {
+  c.N = c.g->N;
+  c.nrp = c.g->natom * c.g->nprjmx;
+  c.dx = c.g->dx; c.dy = c.g->dy; c.dz = c.g->dz;
+  const int M = c.M;
+  int rc = RS_OK;
+  if (l_rrb && (rc = c.apply_h(c.psi, c.rp, c.hpsi, M))) return rc;
+  double *A = nullptr, *w = nullptr, *Z = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&A, sizeof(double) * ((size_t)2 * M * M + M), c.st));
+  Z = A + (size_t)M * M;
+  w = Z + (size_t)M * M;
+  const double dv = c.dx * c.dy * c.dz;
+  if constexpr (sizeof(T) == 4)
+    rc = gram_f32(M, M, c.N, (const float*)c.psi, c.N, (const float*)c.hpsi, c.N, dv, A, M, 0, c.st);
+  else
+    rc = gram_f64(M, M, c.N, (const double*)c.psi, c.N, (const double*)c.hpsi, c.N, dv, A, M, c.st);
+  // dsyev('v','l') reads the lower triangle: mirror it
+  if (!rc) {
+    std::vector<double> h((size_t)M * M);
+    cudaMemcpyAsync(h.data(), A, sizeof(double) * M * M, cudaMemcpyDeviceToHost, c.st);
+    cudaStreamSynchronize(c.st);
+    for (int j = 0; j < M; ++j)
+      for (int i = 0; i < j; ++i) h[(size_t)j * M + i] = h[(size_t)i * M + j];
+    cudaMemcpyAsync(A, h.data(), sizeof(double) * M * M, cudaMemcpyHostToDevice, c.st);
+    rc = syev_jacobi(M, A, w, Z, 60, c.st, nullptr);
+  }
+  if (!rc) rc = c.rotate_all(Z);
+  if (!rc) {
+    RS_CUDA(cudaMemcpyAsync(sval_h, w, sizeof(double) * M, cudaMemcpyDeviceToHost, c.st));
+    RS_CUDA(cudaStreamSynchronize(c.st));
+  }
+  cudaFreeAsync(A, c.st);
+  return rc;
+}
+
+// reorderstates: stable ascending rank, permute psi, spsi, rp, sval, resid
+template <class T>
+static int reorder(BandCtx<T>& c, double* sval_h, double* resid_h) {
+  const int M = c.M;
+  const long N = c.g->N;
+  const int nrp = c.g->natom * c.g->nprjmx;
+  std::vector<int> rank(M, 0);
+  for (int j = 1; j < M; ++j)
+    for (int i = 0; i < j; ++i) {
+      if (sval_h[i] > sval_h[j]) rank[i] += 1;
+      else rank[j] += 1;
+    }
+  std::vector<double> t(M);
+  for (int j = 0; j < M; ++j) t[rank[j]] = sval_h[j];
+  std::copy(t.begin(), t.end(), sval_h);
+  for (int j = 0; j < M; ++j) t[rank[j]] = resid_h[j];
+  std::copy(t.begin(), t.end(), resid_h);
+  int* drank = nullptr;
+  void* tmp = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&drank, sizeof(int) * M, c.st));
+  RS_CUDA(cudaMallocAsync(&tmp, sizeof(T) * (size_t)N * M, c.st));
+  RS_CUDA(cudaMemcpyAsync(drank, rank.data(), sizeof(int) * M, cudaMemcpyHostToDevice, c.st));
+  T* arrs[2] = {c.psi, c.sep() ? c.spsi : nullptr};
+  for (T* a : arrs) {
+    if (!a) continue;
+    k_permute_bands<T><<<div_up(N * M, 256), 256, 0, c.st>>>(N, M, drank, a, (T*)tmp);
+    cudaMemcpyAsync(a, tmp, sizeof(T) * N * M, cudaMemcpyDeviceToDevice, c.st);
+  }
+  if (nrp) {
+    k_gather_bands_d<<<div_up((long)nrp * M, 256), 256, 0, c.st>>>(nrp, M, drank, c.rp, (double*)tmp);
+    cudaMemcpyAsync(c.rp, tmp, sizeof(double) * nrp * M, cudaMemcpyDeviceToDevice, c.st);
+  }
+  cudaFreeAsync(drank, c.st);
+  cudaFreeAsync(tmp, c.st);
+  cudaError_t e = cudaStreamSynchronize(c.st);
+  if (e != cudaSuccess) return cuda_status(e, "reorderstates");
+  return RS_OK;
+}
+
+template <class T>
+static BandCtx<T> make_ctx(const rs_geom* g, const T* veff, const double* dij, const double* sss,
+                           int M, T* psi, T* spsi, double* rp, T* hpsi, void* stream) {
+  BandCtx<T> c;
+  c.g = g; c.veff = veff; c.dij = dij; c.sss = sss; c.M = M;
+  c.psi = psi; c.spsi = sss ? spsi : psi; c.rp = rp; c.hpsi = hpsi;
+  c.st = as_stream(stream);
+  c.N = g->N;
+  c.nrp = g->natom * g->nprjmx;
+  c.dx = g->dx; c.dy = g->dy; c.dz = g->dz;
+  return c;
+}
+
+}  // namespace rs
+
+#define RS_BANDS_CHECK(fn)                                                    \
+  if (!g) return rs::fail(RS_EINVAL, fn ": null geometry");                  \
+  if (M <= 0) return rs::fail(RS_EINVAL, fn ": no bands");                   \
+  if (sss && (!spsi || spsi == psi)) return rs::fail(RS_EINVAL, fn ": S psi must be its own array")
+
+#define RS_BANDS_IMPL(SUF, T)                                                                  \
+  extern "C" int rs_orthogonalize_##SUF(const rs_geom* g, const double* sss, int M, T* psi,     \
+                                        T* spsi, double* rp, int cmpt, void* stream) {          \
+    RS_BANDS_CHECK("rs_orthogonalize_" #SUF);                                                  \
+    auto c = rs::make_ctx<T>(g, nullptr, nullptr, sss, M, psi, spsi, rp, nullptr, stream);      \
+    int rc = c.init(0, 0);                                                                     \
+    if (!rc) rc = c.ortho_all(cmpt != 0);                                                       \
+    c.release();                                                                               \
+    return rc;                                                                                 \
+  }                                                                                            \
+  extern "C" int rs_orthogonalize_band_##SUF(const rs_geom* g, const double* sss, int M, int l, \
+                                             T* psi, T* spsi, double* rp, int cmpt,             \
+                                             void* stream) {                                    \
+    RS_BANDS_CHECK("rs_orthogonalize_band_" #SUF);                                             \
+    if (l < 0 || l >= M) return rs::fail(RS_EINVAL, "rs_orthogonalize_band: band out of range"); \
+    auto c = rs::make_ctx<T>(g, nullptr, nullptr, sss, M, psi, spsi, rp, nullptr, stream);      \
+    int rc = c.init(0, 0);                                                                     \
+    if (!rc) rc = c.ortho_band(l, cmpt != 0);                                                   \
+    if (!rc) rc = c.check_status();                                                            \
+    c.release();                                                                               \
+    return rc;                                                                                 \
+  }                                                                                            \
+  extern "C" int rs_rayleighritz_##SUF(const rs_geom* g, const T* veff, const double* dij,      \
+                                       const double* sss, int M, T* psi, T* spsi, double* rp,   \
+                                       T* hpsi, int l_rrb, double* sval, void* stream) {        \
+    RS_BANDS_CHECK("rs_rayleighritz_" #SUF);                                                   \
+    auto c = rs::make_ctx<T>(g, veff, dij, sss, M, psi, spsi, rp, hpsi, stream);                \
+    return rs::rayleighritz<T>(c, l_rrb, sval);                                                 \
+  }                                                                                            \
+  extern "C" int rs_kscg_##SUF(const rs_geom* g, const T* veff, const double* dij,              \
+                               const double* sss, const rs_solver_prm* prm, int M, T* psi,      \
+                               T* spsi, double* rp, T* hpsi, double* sval, double* resid,       \
+                               int* itmax, void* stream) {                                      \
+    RS_BANDS_CHECK("rs_kscg_" #SUF);                                                           \
+    auto c = rs::make_ctx<T>(g, veff, dij, sss, M, psi, spsi, rp, hpsi, stream);                \
+    return rs::kscg<T>(c, prm, sval, resid, itmax);                                             \
+  }                                                                                            \
+  extern "C" int rs_ksdiis_##SUF(const rs_geom* g, const T* veff, const double* dij,            \
+                                 const double* sss, const rs_solver_prm* prm, int M, int l_hsv, \
+                                 T* psi, T* spsi, double* rp, T* hpsi, double* sval,            \
+                                 double* resid, int* ksconv, void* stream) {                    \
+    RS_BANDS_CHECK("rs_ksdiis_" #SUF);                                                         \
+    auto c = rs::make_ctx<T>(g, veff, dij, sss, M, psi, spsi, rp, hpsi, stream);                \
+    return rs::ksdiis<T>(c, prm, l_hsv, sval, resid, ksconv);                                   \
+  }                                                                                            \
+  extern "C" int rs_reorder_##SUF(const rs_geom* g, const double* sss, int M, T* psi, T* spsi,  \
+                                  double* rp, double* sval, double* resid, void* stream) {      \
+    RS_BANDS_CHECK("rs_reorder_" #SUF);                                                        \
+    auto c = rs::make_ctx<T>(g, nullptr, nullptr, sss, M, psi, spsi, rp, nullptr, stream);      \
+    return rs::reorder<T>(c, sval, resid);                                                      \
+  }                                                                                            \
+  extern "C" int rs_scf_diag_##SUF(const rs_geom* g, const T* veff, const double* dij,          \
+                                   const double* sss, const rs_solver_prm* prm, int iscf,       \
+                                   int M, T* psi, T* spsi, double* rp, T* hpsi, double* sval,   \
+                                   double* resid, int* ksconv, int* ksitmax, void* stream) {    \
+    RS_BANDS_CHECK("rs_scf_diag_" #SUF);                                                       \
+    auto c = rs::make_ctx<T>(g, veff, dij, sss, M, psi, spsi, rp, hpsi, stream);                \
+    const int nrrz = prm->nrrz, nchange = prm->nchange;                                         \
+    bool l_rrb = false, l_rra = false, l_hsv = false, l_reo = false;                            \
+    if (nrrz != 0) {                                                                           \
+      l_rrb = (iscf % abs(nrrz) == 0) && nrrz > 0;                                             \
+      l_rra = (iscf % abs(nrrz) == 0) && nrrz < 0;                                             \
+      l_hsv = l_rra || ((iscf + 1) % nrrz == 0 && nrrz > 0);                                   \
+    }                                                                                          \
+    if (nchange > 0) l_reo = (iscf % nchange == 0) && !l_rra;                                  \
+    int rc = RS_OK;                                                                            \
+    *ksconv = 1;                                                                               \
+    *ksitmax = 0;                                                                              \
+    if (l_rrb) rc = rs::rayleighritz<T>(c, 1, sval);                                           \
+    if (!rc) {                                                                                 \
+      if (iscf <= prm->ncgscf || (prm->nretcg > 0 && iscf % prm->nretcg == 0)) {               \
+        auto c2 = rs::make_ctx<T>(g, veff, dij, sss, M, psi, spsi, rp, hpsi, stream);           \
+        rc = rs::kscg<T>(c2, prm, sval, resid, ksitmax);                                       \
+        for (int l = 0; l < M && !rc; ++l)                                                     \
+          *ksconv = *ksconv && (sqrt(resid[l]) < prm->epssd || *ksitmax < prm->nsdmax);        \
+      } else {                                                                                 \
+        auto c2 = rs::make_ctx<T>(g, veff, dij, sss, M, psi, spsi, rp, hpsi, stream);           \
+        rc = rs::ksdiis<T>(c2, prm, l_hsv ? 1 : 0, sval, resid, ksconv);                       \
+        *ksitmax = 1;                                                                          \
+      }                                                                                        \
+    }                                                                                          \
+    if (!rc && l_rra) {                                                                        \
+      auto c3 = rs::make_ctx<T>(g, veff, dij, sss, M, psi, spsi, rp, hpsi, stream);             \
+      rc = rs::rayleighritz<T>(c3, 1, sval);                                                   \
+    }                                                                                          \
+    if (!rc && l_reo) {                                                                        \
+      auto c4 = rs::make_ctx<T>(g, veff, dij, sss, M, psi, spsi, rp, hpsi, stream);             \
+      rc = rs::reorder<T>(c4, sval, resid);                                                    \
+    }                                                                                          \
+    return rc;                                                                                 \
+  }
+
+RS_BANDS_IMPL(f64, double)
+RS_BANDS_IMPL(f32, float)

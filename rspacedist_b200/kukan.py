@@ -184,3 +184,91 @@ def dot(a, b):
     fn = "rs_dot_f64" if a.dtype == torch.float64 else "rs_dot_f32"
     L.call(fn, a.numel(), _ptr(a), _ptr(b), _ptr(out), _stream())
     return out
+
+
+# ----------------------------------------------------------------- band solvers
+class Bands:
+    """Band state of one k-point/spin: psi, S psi (aliases psi when S = 1),
+    H psi, <p|psi> and the eigenvalue / residual arrays, on one device.
+    dtype float64 is the plain FP64 path, float32 the mixed path."""
+
+    def __init__(self, g: Geometry, psi: torch.Tensor, sss=None):
+        self.g = g
+        self.M = psi.shape[0]
+        self.dtype = psi.dtype
+        self.psi = psi.contiguous()
+        self.sss = sss
+        self.spsi = self.psi.clone() if sss is not None else self.psi
+        self.hpsi = torch.zeros_like(self.psi)
+        self.rp = torch.zeros((self.M, g.natom, g.nprjmx), dtype=torch.float64,
+                              device=psi.device)
+        self.sval = np.zeros(self.M)
+        self.resid = np.zeros(self.M)
+
+    @property
+    def suffix(self):
+        return "f64" if self.dtype == torch.float64 else "f32"
+
+    def _dp(self, a):
+        return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def orthogonalization(b: Bands, cmpt: int = 1):
+    """orthogonalization_r_01, all bands (Cholesky-QR in the S metric)."""
+    L.call("rs_orthogonalize_" + b.suffix, b.g.handle, _ptr(b.sss), b.M, _ptr(b.psi),
+           _ptr(b.spsi), _ptr(b.rp), cmpt, _stream())
+
+
+def orthogonalization_band(b: Bands, l: int, cmpt: int = 0):
+    L.call("rs_orthogonalize_band_" + b.suffix, b.g.handle, _ptr(b.sss), b.M, l, _ptr(b.psi),
+           _ptr(b.spsi), _ptr(b.rp), cmpt, _stream())
+
+
+def rayleighritz(b: Bands, veff, dij, l_rrb: int = 1):
+    L.call("rs_rayleighritz_" + b.suffix, b.g.handle, _ptr(veff), _ptr(dij), _ptr(b.sss), b.M,
+           _ptr(b.psi), _ptr(b.spsi), _ptr(b.rp), _ptr(b.hpsi), l_rrb, b._dp(b.sval), _stream())
+    return b.sval
+
+
+def kscg(b: Bands, veff, dij, prm=None):
+    prm = prm or L.solver_prm()
+    itm = C.c_int(0)
+    L.call("rs_kscg_" + b.suffix, b.g.handle, _ptr(veff), _ptr(dij), _ptr(b.sss), C.byref(prm),
+           b.M, _ptr(b.psi), _ptr(b.spsi), _ptr(b.rp), _ptr(b.hpsi), b._dp(b.sval),
+           b._dp(b.resid), C.byref(itm), _stream())
+    return itm.value
+
+
+def ksdiis(b: Bands, veff, dij, prm=None, l_hsv: int = 1):
+    prm = prm or L.solver_prm()
+    conv = C.c_int(0)
+    L.call("rs_ksdiis_" + b.suffix, b.g.handle, _ptr(veff), _ptr(dij), _ptr(b.sss), C.byref(prm),
+           b.M, l_hsv, _ptr(b.psi), _ptr(b.spsi), _ptr(b.rp), _ptr(b.hpsi), b._dp(b.sval),
+           b._dp(b.resid), C.byref(conv), _stream())
+    return bool(conv.value)
+
+
+def reorderstates(b: Bands):
+    L.call("rs_reorder_" + b.suffix, b.g.handle, _ptr(b.sss), b.M, _ptr(b.psi), _ptr(b.spsi),
+           _ptr(b.rp), b._dp(b.sval), b._dp(b.resid), _stream())
+
+
+def scf_diag(b: Bands, veff, dij, iscf: int, prm=None):
+    """scf_diag for one k-point/spin; returns (ksconv, ksitmax)."""
+    prm = prm or L.solver_prm()
+    conv, itm = C.c_int(0), C.c_int(0)
+    L.call("rs_scf_diag_" + b.suffix, b.g.handle, _ptr(veff), _ptr(dij), _ptr(b.sss),
+           C.byref(prm), iscf, b.M, _ptr(b.psi), _ptr(b.spsi), _ptr(b.rp), _ptr(b.hpsi),
+           b._dp(b.sval), b._dp(b.resid), C.byref(conv), C.byref(itm), _stream())
+    return bool(conv.value), itm.value
+
+
+def syev(a: torch.Tensor):
+    """FP64 symmetric eigen-decomposition on the GPU (ascending)."""
+    n = a.shape[0]
+    A = a.to(torch.float64).contiguous().clone()
+    w = torch.empty(n, dtype=torch.float64, device=a.device)
+    Z = torch.empty((n, n), dtype=torch.float64, device=a.device)
+    sw = C.c_int(0)
+    L.call("rs_syev_f64", n, _ptr(A), _ptr(w), _ptr(Z), C.byref(sw), _stream())
+    return w, Z.T, sw.value   # Z stored column-major: columns are vectors

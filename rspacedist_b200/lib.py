@@ -19,6 +19,24 @@ _p = C.c_void_p
 _ip = C.POINTER(C.c_int)
 _dp = C.POINTER(C.c_double)
 
+class SolverPrm(C.Structure):
+    """rs_solver_prm: kukan namelist parameters of the band solvers."""
+    _fields_ = [("northo", _i), ("nsdmax", _i), ("nprecon_cg", _i), ("nprecon_diis", _i),
+                ("ndiismax", _i), ("nrrz", _i), ("nchange", _i), ("ncgscf", _i),
+                ("nretcg", _i), ("epssd", _d), ("eps_eig_diis", _d), ("alambda_diis", _d),
+                ("alambda_min", _d), ("alambda_max", _d)]
+
+
+def solver_prm(northo=1, nsdmax=4, nprecon_cg=1, nprecon_diis=1, ndiismax=4, nrrz=1,
+               nchange=1, ncgscf=200, nretcg=2000, epssd=1e-6, eps_eig_diis=1e-14,
+               alambda_diis=0.5, alambda_min=0.1, alambda_max=1.0) -> SolverPrm:
+    """kukan's defaults (read_input_kukan8f.F90:198-249)."""
+    return SolverPrm(northo, nsdmax, nprecon_cg, nprecon_diis, ndiismax, nrrz, nchange, ncgscf,
+                     nretcg, epssd, eps_eig_diis, alambda_diis, alambda_min, alambda_max)
+
+
+_sp = C.POINTER(SolverPrm)
+
 # name -> argtypes (restype int unless noted)
 SIGNATURES = {
     "rs_last_error": [C.c_char_p, _i],
@@ -48,6 +66,22 @@ SIGNATURES = {
     "rs_gram_f64": [_i, _i, _l, _p, _l, _p, _l, _d, _p, _l, _p],
     "rs_rotate_f32": [_l, _i, _i, _p, _l, _p, _l, _p, _l, _p],
     "rs_rotate_f64": [_l, _i, _i, _p, _l, _p, _l, _p, _l, _p],
+    "rs_syev_f64": [_i, _p, _p, _p, _ip, _p],
+    "rs_chol_inv_t": [_i, _p, _p, _p],
+    "rs_orthogonalize_f64": [_p, _p, _i, _p, _p, _p, _i, _p],
+    "rs_orthogonalize_f32": [_p, _p, _i, _p, _p, _p, _i, _p],
+    "rs_orthogonalize_band_f64": [_p, _p, _i, _i, _p, _p, _p, _i, _p],
+    "rs_orthogonalize_band_f32": [_p, _p, _i, _i, _p, _p, _p, _i, _p],
+    "rs_rayleighritz_f64": [_p, _p, _p, _p, _i, _p, _p, _p, _p, _i, _dp, _p],
+    "rs_rayleighritz_f32": [_p, _p, _p, _p, _i, _p, _p, _p, _p, _i, _dp, _p],
+    "rs_kscg_f64": [_p, _p, _p, _p, _sp, _i, _p, _p, _p, _p, _dp, _dp, _ip, _p],
+    "rs_kscg_f32": [_p, _p, _p, _p, _sp, _i, _p, _p, _p, _p, _dp, _dp, _ip, _p],
+    "rs_ksdiis_f64": [_p, _p, _p, _p, _sp, _i, _i, _p, _p, _p, _p, _dp, _dp, _ip, _p],
+    "rs_ksdiis_f32": [_p, _p, _p, _p, _sp, _i, _i, _p, _p, _p, _p, _dp, _dp, _ip, _p],
+    "rs_reorder_f64": [_p, _p, _i, _p, _p, _p, _dp, _dp, _p],
+    "rs_reorder_f32": [_p, _p, _i, _p, _p, _p, _dp, _dp, _p],
+    "rs_scf_diag_f64": [_p, _p, _p, _p, _sp, _i, _i, _p, _p, _p, _p, _dp, _dp, _ip, _ip, _p],
+    "rs_scf_diag_f32": [_p, _p, _p, _p, _sp, _i, _i, _p, _p, _p, _p, _dp, _dp, _ip, _ip, _p],
     "rs_dot_f64": [_l, _p, _p, _p, _p],
     "rs_dot_f32": [_l, _p, _p, _p, _p],
 }
