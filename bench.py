@@ -138,10 +138,11 @@ def run_gpu(args):
     dij = torch.tensor(cell.dij, dtype=torch.float64, device=dev)
     gen = torch.Generator(device=dev)
     gen.manual_seed(1234 + rank)
-    psi = torch.randn((NB, cell.N), generator=gen, dtype=torch.float32, device=dev) * 0.1
+    nb = args.bands
+    psi = torch.randn((nb, cell.N), generator=gen, dtype=torch.float32, device=dev) * 0.1
     rp = K.nonlocaloperation_01(g, psi)
     hpsi = torch.empty_like(psi)
-    nbytes = algorithmic_bytes(cell, NB, g.entries)
+    nbytes = algorithmic_bytes(cell, nb, g.entries)
     stream = torch.cuda.current_stream()
 
     def step():
@@ -171,9 +172,10 @@ def run_gpu(args):
     kernel_gbs = nbytes / (ms * 1e-3) / 1e9
 
     # end to end through the host-buffer entry point (pinned host psi/hpsi)
-    hin = psi[:E2E_BANDS].cpu().pin_memory()
+    ne = min(E2E_BANDS, nb)
+    hin = psi[:ne].cpu().pin_memory()
     hout = torch.empty_like(hin).pin_memory()
-    rp_e = rp[:E2E_BANDS].contiguous()
+    rp_e = rp[:ne].contiguous()
     for _ in range(2):
         K.hpsi_host(g, veff, dij, rp_e, hin, hout, chunk=32)
     torch.cuda.synchronize()
@@ -183,12 +185,12 @@ def run_gpu(args):
         K.hpsi_host(g, veff, dij, rp_e, hin, hout, chunk=32)
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - e0) / e2e_steps
-    e2e_bytes = algorithmic_bytes(cell, E2E_BANDS, g.entries)
+    e2e_bytes = algorithmic_bytes(cell, ne, g.entries)
     e2e_gbs = e2e_bytes / e2e_s / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(cell, NB)
+        cpu = cpu_baseline(cell, nb)
     if rank == 0:
         out = {
             "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi; SCF-time part of the metric not yet measured)",
@@ -198,11 +200,11 @@ def run_gpu(args):
             "data": "synthetic (seeded Si512 geometry, random psi, synthetic smooth veff)",
             "config": {"workload": "Si512 H*psi sweep: 128^3 grid, 1100 bands, 512 Si atoms "
                                    "x 12 projectors, FP32 psi, stored <p|psi>",
-                       "grid": [GRID] * 3, "bands": NB, "atoms": cell.natom,
+                       "grid": [GRID] * 3, "bands": nb, "atoms": cell.natom,
                        "projectors": cell.nprjmx, "inverse_entries": g.entries,
                        "l2": "inputs (9.2 GB psi) larger than L2; no flush",
                        "parallelism": f"bands replicated per GPU x{world}"},
-            "band_points_per_s": round(NB * cell.N * world / (ms * 1e-3), 1),
+            "band_points_per_s": round(nb * cell.N * world / (ms * 1e-3), 1),
             "roofline": {"bound": "hbm", "achieved": round(kernel_gbs, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(kernel_gbs / peak, 4),
                          "traffic": None, "peak_source": peak_kind,
@@ -210,7 +212,7 @@ def run_gpu(args):
             "e2e": {"value": round(e2e_gbs, 2), "unit": "GB/s",
                     "h2d_bytes_per_step": int(hin.numel() * 4),
                     "d2h_bytes_per_step": int(hout.numel() * 4),
-                    "bands": E2E_BANDS, "entry_point": "rs_hpsi_host_f32"},
+                    "bands": ne, "entry_point": "rs_hpsi_host_f32"},
             "gpu_launches": 2 * args.steps,
             "clocks": clk.summary(),
         }
@@ -286,6 +288,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--bands", type=int, default=NB,
+                    help="bands per sweep (default 1100; smaller values for profiling only)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
