@@ -235,6 +235,20 @@ int rs_scf_diag_f32(const rs_geom* g, const float* veff, const double* dij, cons
                     double* rp, float* hpsi, double* sval, double* resid, int* ksconv,
                     int* ksitmax, void* stream);
 
+/* rs_hartree_cg for callers that cannot allocate device memory (a host code
+ * that handed all device memory to its own pool, a framework whose caching
+ * allocator owns the GPU, work issued where the driver's allocation lock must
+ * not be taken).  Same arguments, results and iterates as rs_hartree_cg, but
+ * the work vectors live in a fixed array inside the library (about 10.5 MB
+ * per GPU, held until exit), so grids are limited to 262144 points (64^3);
+ * larger grids return RS_EINVAL.  The first call on a device looks up the
+ * array's device address, so make it before any stream capture.  Calls that
+ * overlap on one GPU share the array and race.  This entry point has no
+ * counterpart in the reference. */
+int rs_hartree_cg_noalloc(int nx, int ny, int nz, int nfh, double xmax, double ymax,
+                          double zmax, double epsvh, int ncgmin, int ncgmax, int ncgres,
+                          const double* rho, double* vh, int* iters, double* dp, void* stream);
+
 /* ---- fixed-tree reductions (shared order with the oracle) --------------- */
 /* out(dev, 1 double) = sum_i a_i b_i in the documented block tree. */
 int rs_dot_f64(long n, const double* a, const double* b, double* out, void* stream);
