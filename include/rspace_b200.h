@@ -235,6 +235,20 @@ int rs_scf_diag_f32(const rs_geom* g, const float* veff, const double* dij, cons
                     double* rp, float* hpsi, double* sval, double* resid, int* ksconv,
                     int* ksitmax, void* stream);
 
+/* ---- forces ------------------------------------------------------------- */
+/* force_eig_r (force8f.F90:9-195), one k-point and spin: the nonlocal force
+ * fxyz(dev, [3][natom]: x forces, then y, then z) = -sum_l 2 occ_l sum_ij
+ * <p_i|psi_l> (D - sval_l S)_ij <p_j|d psi_l>, with d the nf-order first
+ * derivative (force_r_02/03/04, force8f.F90:409-490).  dij and sss are per
+ * atom [natom][nprjmx][nprjmx] (dev); sss = NULL for norm-conserving sets.
+ * psi [nb][N], sval and occ (fnele) [nb] are device arrays.  The FP64 form
+ * matches the strict oracle bit for bit; the FP32 form takes FP32 bands and
+ * accumulates in FP64. */
+int rs_force_nl_f64(const rs_geom* g, const double* dij, const double* sss, const double* psi,
+                    const double* sval, const double* occ, int nb, double* fxyz, void* stream);
+int rs_force_nl_f32(const rs_geom* g, const double* dij, const double* sss, const float* psi,
+                    const double* sval, const double* occ, int nb, double* fxyz, void* stream);
+
 /* rs_hartree_cg for callers that cannot allocate device memory (a host code
  * that handed all device memory to its own pool, a framework whose caching
  * allocator owns the GPU, work issued where the driver's allocation lock must

@@ -179,6 +179,20 @@ def scf_hartree(shape, nfh: int, xmax, rho, vh, epsvh=1e-12, ncgmin=1, ncgmax=80
     return it.value, dp.value
 
 
+def force_eig(g: Geometry, dij, sss, psi, sval, occ):
+    """Nonlocal force on every atom (force_eig_r), as a (natom, 3) FP64 tensor.
+    dij/sss are per-atom (natom, P, P) FP64 device tensors (sss None for NC),
+    psi (nb, N) FP64 or FP32, sval/occ (nb,) FP64 device tensors."""
+    nb = _nb(g, psi)
+    f = torch.empty((3, max(g.natom, 1)), dtype=torch.float64, device=psi.device)
+    for t, what in ((sval, "sval"), (occ, "occ")):
+        _need(t, torch.float64, nb, what)
+    fn = "rs_force_nl_f64" if psi.dtype == torch.float64 else "rs_force_nl_f32"
+    L.call(fn, g.handle, _ptr(dij), None if sss is None else _ptr(sss), _ptr(psi), _ptr(sval),
+           _ptr(occ), nb, _ptr(f), _stream())
+    return f[:, : g.natom].T
+
+
 def dot(a, b):
     out = torch.empty(1, dtype=torch.float64, device=a.device)
     fn = "rs_dot_f64" if a.dtype == torch.float64 else "rs_dot_f32"

@@ -83,6 +83,8 @@ SIGNATURES = {
     "rs_scf_diag_f64": [_p, _p, _p, _p, _sp, _i, _i, _p, _p, _p, _p, _dp, _dp, _ip, _ip, _p],
     "rs_scf_diag_f32": [_p, _p, _p, _p, _sp, _i, _i, _p, _p, _p, _p, _dp, _dp, _ip, _ip, _p],
     "rs_hartree_cg_noalloc": [_i, _i, _i, _i, _d, _d, _d, _d, _i, _i, _i, _p, _p, _ip, _dp, _p],
+    "rs_force_nl_f64": [_p, _p, _p, _p, _p, _p, _i, _p, _p],
+    "rs_force_nl_f32": [_p, _p, _p, _p, _p, _p, _i, _p, _p],
     "rs_dot_f64": [_l, _p, _p, _p, _p],
     "rs_dot_f32": [_l, _p, _p, _p, _p],
 }
