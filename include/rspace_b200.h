@@ -235,6 +235,35 @@ int rs_scf_diag_f32(const rs_geom* g, const float* veff, const double* dij, cons
                     double* rp, float* hpsi, double* sval, double* resid, int* ksconv,
                     int* ksitmax, void* stream);
 
+/* ---- SCF potentials and mixing (periodic, one spin) --------------------- */
+/* trans_d2c_vh / trans_d2c_vxc for nperi=3 (trans8f.F90:93-152, 415-454):
+ * out(dev, coarse nx*ny*nz) = transpose of the coarse->dense interpolation
+ * applied to in(dev, dense 2nx*2ny*2nz) / 8, with the periodic halo fold of
+ * overlap_interpolation nflag=2.  Needs n >= 2nf on each axis. */
+int rs_interp_d2c(int nx, int ny, int nz, int nf, const double* in, double* out,
+                  void* stream);
+/* vxpot_lda_pz (vxpot8f.F90:126-155): vx, ex(dev) from rho(dev), n points. */
+int rs_vxc_pz(long n, const double* rho, double* vx, double* ex, void* stream);
+/* scf_potentials' veff (scf_potentials8f.F90:256-267, no bias field):
+ * veff = vx + (vloc + vh); writes the FP64 and/or the FP32 copy (either
+ * pointer may be NULL, not both). */
+int rs_veff_sum(long n, const double* vx, const double* vloc, const double* vh, double* veff,
+                float* veff32, void* stream);
+/* scf_diffcharge + kukan8f.F90:672-673: *diff(host) = sqrt(sum (rho_i -
+ * rho_o)^2 dx dy dz / (8 xmax ymax zmax)); synchronises the stream. */
+int rs_diffcharge(long n, const double* rho_o, const double* rho_i, double dx, double dy,
+                  double dz, double xmax, double ymax, double zmax, double* diff,
+                  void* stream);
+/* scf_chargemixing with modified Broyden (scf_chargemixing8f.F90:59-168,
+ * 214-657), grid density of one spin: a mixer keeps nbrydn (2..63) history
+ * vectors of n points on the device.  Each rs_mixer_step is one call of
+ * scf_chargemixing: rho_i(dev) holds the last input density and receives
+ * the next one; the first step copies rho_o.  Synchronises the stream. */
+typedef struct rs_mixer rs_mixer;
+int rs_mixer_create(rs_mixer** m, long n, int nbrydn, double eta);
+int rs_mixer_step(rs_mixer* m, const double* rho_o, double* rho_i, double dvol, void* stream);
+int rs_mixer_destroy(rs_mixer* m);
+
 /* ---- forces ------------------------------------------------------------- */
 /* force_eig_r (force8f.F90:9-195), one k-point and spin: the nonlocal force
  * fxyz(dev, [3][natom]: x forces, then y, then z) = -sum_l 2 occ_l sum_ij

@@ -23,9 +23,11 @@ _ip = C.POINTER(C.c_int)
 
 
 def build(force: bool = False) -> str:
-    """Compile the oracle with its Makefile (gcc, -ffp-contract=off)."""
-    if force or not os.path.exists(_SO):
-        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    """Compile the oracle with its Makefile (gcc, -ffp-contract=off); make
+    rebuilds only when a source is newer than the library."""
+    if force and os.path.exists(_SO):
+        os.remove(_SO)
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _SO
 
 
@@ -186,6 +188,58 @@ def interp_c2d(shape, nf, x):
     out = np.zeros(8 * nx * ny * nz)
     lib().orc_interp_c2d(nx, ny, nz, nf, _d(_f64(x)), _d(out))
     return out
+
+
+def interp_d2c(shape, nf, x):
+    """Dense (2nx, 2ny, 2nz) -> coarse (nx, ny, nz) transfer (trans_d2c_*)."""
+    nx, ny, nz = shape
+    out = np.zeros(nx * ny * nz)
+    lib().orc_interp_d2c(nx, ny, nz, nf, _d(_f64(x)), _d(out))
+    return out
+
+
+def vxc_pz(rho):
+    rho = _f64(rho)
+    vx, ex = np.zeros(rho.size), np.zeros(rho.size)
+    lib().orc_vxc_pz(C.c_long(rho.size), _d(rho), _d(vx), _d(ex))
+    return vx, ex
+
+
+def veff_sum(vx, vloc, vh):
+    vx = _f64(vx)
+    out = np.zeros(vx.size)
+    lib().orc_veff_sum(C.c_long(vx.size), _d(vx), _d(_f64(vloc)), _d(_f64(vh)), _d(out))
+    return out
+
+
+def diffcharge(rho_o, rho_i, h, xmax):
+    L = lib()
+    L.orc_diffcharge.restype = C.c_double
+    rho_o = _f64(rho_o)
+    return L.orc_diffcharge(C.c_long(rho_o.size), _d(rho_o), _d(_f64(rho_i)),
+                            *(C.c_double(v) for v in h), *(C.c_double(v) for v in xmax))
+
+
+class Broyden:
+    """scf_chargemixing with modified Broyden history (one spin, grid density)."""
+
+    def __init__(self, n, nbrydn=20, eta=0.02):
+        L = lib()
+        L.orc_broyden_create.restype = C.c_void_p
+        self.h = C.c_void_p(L.orc_broyden_create(C.c_long(n), nbrydn, C.c_double(eta)))
+        self.n = n
+
+    def step(self, rho_o, rho_i, dvol):
+        """Returns the next input density (rho_i is not modified)."""
+        r = _f64(rho_i).copy()
+        lib().orc_broyden_step(self.h, _d(_f64(rho_o)), _d(r), C.c_double(dvol))
+        return r
+
+    def __del__(self):
+        try:
+            lib().orc_broyden_free(self.h)
+        except Exception:
+            pass
 
 
 def hartree_laplacian(shape, nfh, h, v):

@@ -326,7 +326,7 @@ void orc_density(long N, int nb, const double* occ, const double* psi, double* r
 /* interpolation, forward branch (interpolation8f.F90:8-100) with nmesh=2 and
  * the periodic halo of overlap_interpolation; Lagrange weights of order 2nf
  * from interpolation8f.F90:36-44. */
-static void interp_weights(int nf, double aw[2][16]) {
+void orc_interp_weights(int nf, double aw[2][16]) {
   for (int k = 0; k < 2; ++k) {
     const double r = ((double)k + 0.5) * 0.5;
     for (int j = -nf + 1; j <= nf; ++j) {
@@ -340,7 +340,7 @@ static void interp_weights(int nf, double aw[2][16]) {
 
 void orc_interp_c2d(int nx, int ny, int nz, int nf, const double* in, double* out) {
   double aw[2][16];
-  interp_weights(nf, aw);
+  orc_interp_weights(nf, aw);
   const int Nx = 2 * nx, Ny = 2 * ny, Nz = 2 * nz;
   double* t1 = (double*)malloc(sizeof(double) * (long)Nx * ny * nz);
   double* t2 = (double*)malloc(sizeof(double) * (long)Nx * Ny * nz);

@@ -55,6 +55,36 @@ void orc_gradient(int nx, int ny, int nz, int nf, double h, int axis,
 /* ---- density / interpolation / Hartree ---- */
 void orc_density(long N, int nb, const double* occ, const double* psi, double* rho);
 void orc_interp_c2d(int nx, int ny, int nz, int nf, const double* in, double* out);
+/* interpolation weights aweight(j, k) for nmesh = 2 (interpolation8f.F90):
+ * aw[k][j + nf - 1], k = dense parity, j = -nf+1..nf */
+void orc_interp_weights(int nf, double aw[2][16]);
+
+/* ---- potentials and mixing (rs_oracle_scf.c) ---- */
+/* trans_d2c_vh / trans_d2c_vxc for nperi=3, one rank: interpolation mode 2
+ * (interpolation8f.F90:98-214) + overlap_interpolation nflag=2
+ * (overlap_interpolation8f.F90:492-892) + division by nmesh^3.  in: dense
+ * (2nx, 2ny, 2nz); out: coarse (nx, ny, nz). */
+void orc_interp_d2c(int nx, int ny, int nz, int nf, const double* in, double* out);
+/* vxpot_lda_pz (vxpot8f.F90:126-155): Perdew-Zunger LDA potential and energy
+ * density per point. */
+void orc_vxc_pz(long n, const double* rho, double* vx, double* ex);
+/* scf_potentials' veff sum (scf_potentials8f.F90:256-267, no bias):
+ * veff = vx + (vloc + vh). */
+void orc_veff_sum(long n, const double* vx, const double* vloc, const double* vh,
+                  double* veff);
+/* scf_diffcharge (scf_diffcharge8f.F90) + kukan8f.F90:673:
+ * sqrt(sum (ri-ro)^2 dx dy dz / (8 xmax ymax zmax)), the sum in the fixed
+ * block tree. */
+double orc_diffcharge(long n, const double* rho_o, const double* rho_i, double dx, double dy,
+                      double dz, double xmax, double ymax, double zmax);
+/* scf_chargemixing_broyden (scf_chargemixing8f.F90:214-657), one spin, grid
+ * density only (norm-conserving atoms): modified Broyden with history nbrydn
+ * and mixing ratio eta.  Dot products use the fixed block tree times dV. */
+typedef struct orc_broyden orc_broyden;
+orc_broyden* orc_broyden_create(long n, int nbrydn, double eta);
+void orc_broyden_free(orc_broyden* b);
+/* one call of scf_chargemixing: rho_i (in: last input density, out: next) */
+void orc_broyden_step(orc_broyden* b, const double* rho_o, double* rho_i, double dvol);
 void orc_hartree_laplacian(int nx, int ny, int nz, int nfh, double ddx, double ddy,
                            double ddz, const double* v, double* av);
 int orc_hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double zmax,

@@ -179,6 +179,69 @@ def scf_hartree(shape, nfh: int, xmax, rho, vh, epsvh=1e-12, ncgmin=1, ncgmax=80
     return it.value, dp.value
 
 
+def trans_d2c(shape, nf: int, v_dense):
+    """Dense -> coarse transfer (trans_d2c_vh / trans_d2c_vxc, periodic)."""
+    nx, ny, nz = shape
+    _need(v_dense, torch.float64, 8 * nx * ny * nz, "v_dense")
+    out = torch.empty(nx * ny * nz, dtype=torch.float64, device=v_dense.device)
+    L.call("rs_interp_d2c", nx, ny, nz, nf, _ptr(v_dense), _ptr(out), _stream())
+    return out
+
+
+def vxpot_lda_pz(rho):
+    """Perdew-Zunger LDA: (vx, ex) per point of rho (FP64 device tensor)."""
+    _need(rho, torch.float64, None, "rho")
+    vx, ex = torch.empty_like(rho), torch.empty_like(rho)
+    L.call("rs_vxc_pz", rho.numel(), _ptr(rho), _ptr(vx), _ptr(ex), _stream())
+    return vx, ex
+
+
+def veff_sum(vx, vloc, vh, veff=None, veff32=None):
+    """veff = vx + (vloc + vh) into an FP64 and/or an FP32 tensor."""
+    n = vx.numel()
+    for t, what in ((vx, "vx"), (vloc, "vloc"), (vh, "vh")):
+        _need(t, torch.float64, n, what)
+    L.call("rs_veff_sum", n, _ptr(vx), _ptr(vloc), _ptr(vh), _ptr(veff), _ptr(veff32),
+           _stream())
+    return veff, veff32
+
+
+def scf_diffcharge(rho_o, rho_i, h, xmax):
+    """SCF charge difference sqrt(sum (rho_i - rho_o)^2 dV / V) (host float)."""
+    out = C.c_double(0.0)
+    L.call("rs_diffcharge", rho_o.numel(), _ptr(rho_o), _ptr(rho_i), h[0], h[1], h[2], xmax[0],
+           xmax[1], xmax[2], C.byref(out), _stream())
+    return out.value
+
+
+class Mixer:
+    """scf_chargemixing with modified Broyden history on the device."""
+
+    def __init__(self, n: int, nbrydn: int = 20, eta: float = 0.02):
+        L.load()
+        self.h = C.c_void_p()
+        L.call("rs_mixer_create", C.byref(self.h), n, nbrydn, eta)
+        self.n = n
+
+    def step(self, rho_o, rho_i, dvol: float):
+        """rho_i (in/out): last input density -> next input density."""
+        _need(rho_o, torch.float64, self.n, "rho_o")
+        _need(rho_i, torch.float64, self.n, "rho_i")
+        L.call("rs_mixer_step", self.h, _ptr(rho_o), _ptr(rho_i), dvol, _stream())
+        return rho_i
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            L.load().rs_mixer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def force_eig(g: Geometry, dij, sss, psi, sval, occ):
     """Nonlocal force on every atom (force_eig_r), as a (natom, 3) FP64 tensor.
     dij/sss are per-atom (natom, P, P) FP64 device tensors (sss None for NC),

@@ -83,6 +83,13 @@ SIGNATURES = {
     "rs_scf_diag_f64": [_p, _p, _p, _p, _sp, _i, _i, _p, _p, _p, _p, _dp, _dp, _ip, _ip, _p],
     "rs_scf_diag_f32": [_p, _p, _p, _p, _sp, _i, _i, _p, _p, _p, _p, _dp, _dp, _ip, _ip, _p],
     "rs_hartree_cg_noalloc": [_i, _i, _i, _i, _d, _d, _d, _d, _i, _i, _i, _p, _p, _ip, _dp, _p],
+    "rs_interp_d2c": [_i, _i, _i, _i, _p, _p, _p],
+    "rs_vxc_pz": [_l, _p, _p, _p, _p],
+    "rs_veff_sum": [_l, _p, _p, _p, _p, _p, _p],
+    "rs_diffcharge": [_l, _p, _p, _d, _d, _d, _d, _d, _d, _dp, _p],
+    "rs_mixer_create": [C.POINTER(_p), _l, _i, _d],
+    "rs_mixer_step": [_p, _p, _p, _d, _p],
+    "rs_mixer_destroy": [_p],
     "rs_force_nl_f64": [_p, _p, _p, _p, _p, _p, _i, _p, _p],
     "rs_force_nl_f32": [_p, _p, _p, _p, _p, _p, _i, _p, _p],
     "rs_dot_f64": [_l, _p, _p, _p, _p],

@@ -1,0 +1,169 @@
+"""The Kohn-Sham SCF loop of kukan (kukan8f.F90:513-680) driven through the
+B200 library, one k-point and spin, periodic cell:
+
+    iscf = 1, 2, ...
+      scf_chargemixing   rho_in  <- Broyden(rho_out, rho_in)      (rs_mixer_step)
+      scf_potentials     rho_dense = c2d(rho_in)                   (rs_interp_c2d)
+                         V_H dense by CG (warm start)              (rs_hartree_cg)
+                         V_xc dense = PZ LDA(rho_dense)            (rs_vxc_pz)
+                         veff = d2c(V_xc) + (vloc + d2c(V_H))     (rs_interp_d2c, rs_veff_sum)
+      scf_diag           RR / CG / DIIS / reorder                  (rs_scf_diag_f64|f32)
+      scf_charge         rho_out = sum_l f_l psi_l^2               (rs_density_*)
+      scf_diffcharge     stop when sqrt(sum (rho_in-rho_out)^2 dV/V) < eps_scf
+
+`dtype=torch.float64` is the plain FP64 path, `torch.float32` the mixed path
+(FP32 bands, FP64 potentials, densities, subspace eigensolve and sums).
+
+Inputs the library does not build (they sit outside the ported hot path):
+the local pseudopotential and the starting charge are model fields given per
+atom (a Gaussian well and a normalised Gaussian of the valence charge), D and
+S stay at their dataset values (no PAW one-centre update), and occupations
+are fixed (2 for the lowest nocc bands).  Every step that kukan performs on
+these inputs runs on the GPU."""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import kukan as K
+from . import lib as L
+from .system import Cell
+
+
+def gaussian_sum(cell: Cell, amp: float, sigma: float) -> np.ndarray:
+    """sum_a amp * exp(-|r - R_a|^2 / (2 sigma^2)) on the coarse grid, with
+    the minimum periodic image (grid point x = (ix + 1/2) dx - xmax)."""
+    nx, ny, nz = cell.shape
+    out = np.zeros((nz, ny, nx))
+    reach = [int(np.ceil(5.0 * sigma / h)) for h in cell.h]
+    n = (nx, ny, nz)
+    for at in cell.atoms:
+        idx = []
+        for ax in range(3):
+            c = int(np.floor((at[ax] + cell.xmax[ax]) / cell.h[ax] - 0.5))
+            i = np.arange(c - reach[ax], c + reach[ax] + 2)
+            x = (i + 0.5) * cell.h[ax] - cell.xmax[ax] - at[ax]
+            L2 = 2.0 * cell.xmax[ax]
+            x = x - L2 * np.round(x / L2)
+            idx.append((np.mod(i, n[ax]), x))
+        (ix, x), (iy, y), (iz, z) = idx
+        r2 = z[:, None, None] ** 2 + y[None, :, None] ** 2 + x[None, None, :] ** 2
+        np.add.at(out, (iz[:, None, None], iy[None, :, None], ix[None, None, :]),
+                  amp * np.exp(-r2 / (2.0 * sigma * sigma)))
+    return out.ravel()
+
+
+def model_local_potential(cell: Cell, depth: float = 1.5, width: float = 1.2) -> np.ndarray:
+    return gaussian_sum(cell, -depth, width)
+
+
+def atomic_density(cell: Cell, zval: float, sigma: float = 1.0) -> np.ndarray:
+    amp = zval / (2.0 * np.pi * sigma * sigma) ** 1.5
+    return gaussian_sum(cell, amp, sigma)
+
+
+def smooth_start_bands(shape, M: int, seed: int) -> np.ndarray:
+    """Seeded random bands low-pass filtered on the grid (a smooth start)."""
+    nx, ny, nz = shape
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((M, nz, ny, nx))
+    kz, ky, kx = np.meshgrid(np.fft.fftfreq(nz), np.fft.fftfreq(ny), np.fft.fftfreq(nx),
+                             indexing="ij")
+    filt = np.exp(-(kx ** 2 + ky ** 2 + kz ** 2) / 0.005)
+    x = np.real(np.fft.ifftn(np.fft.fftn(x, axes=(1, 2, 3)) * filt, axes=(1, 2, 3)))
+    return x.reshape(M, -1)
+
+
+@dataclass
+class ScfResult:
+    converged: bool
+    iterations: int
+    seconds: float
+    diff: list = field(default_factory=list)      # diff_charge per iteration
+    seconds_per_iter: list = field(default_factory=list)
+    sval: np.ndarray | None = None                 # eigenvalues (Ha), ascending
+    eband: float = 0.0                             # sum_l f_l e_l (Ha)
+    hartree_iters: list = field(default_factory=list)
+    phase_seconds: dict = field(default_factory=dict)  # with profile=True only
+
+
+def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float = 1e-6,
+            looplimit: int = 200, prm=None, nbrydn: int = 20, eta: float = 0.02,
+            seed: int = 0, zval: float = 4.0, epsvh: float = 1e-12, vloc=None, rho0=None,
+            psi0=None, log=None, profile: bool = False) -> ScfResult:
+    dev = torch.device("cuda")
+    g = K.Geometry(cell)
+    N, shape = cell.N, cell.shape
+    dshape = tuple(2 * s for s in shape)
+    h, xmax = cell.h, cell.xmax
+    dvol = h[0] * h[1] * h[2]
+    f64 = torch.float64
+    psi = smooth_start_bands(shape, M, seed) if psi0 is None else psi0
+    sss = None if cell.sss is None else torch.tensor(cell.sss, dtype=f64, device=dev)
+    b = K.Bands(g, torch.tensor(psi, dtype=dtype, device=dev), sss)
+    K.orthogonalization(b, 1)
+    occ = torch.zeros(M, dtype=f64, device=dev)
+    occ[:nocc] = 2.0
+    vloc_t = torch.tensor(model_local_potential(cell) if vloc is None else vloc, dtype=f64,
+                          device=dev)
+    rho_o = torch.tensor(atomic_density(cell, zval) if rho0 is None else rho0, dtype=f64,
+                         device=dev)
+    rho_i = torch.zeros(N, dtype=f64, device=dev)
+    vh_d = torch.zeros(8 * N, dtype=f64, device=dev)
+    veff64 = torch.empty(N, dtype=f64, device=dev)
+    veff32 = torch.empty(N, dtype=torch.float32, device=dev) if dtype == torch.float32 else None
+    veff = veff64 if veff32 is None else veff32
+    dij = torch.tensor(cell.dij, dtype=f64, device=dev)
+    prm = prm or L.solver_prm()
+    mixer = K.Mixer(N, nbrydn, eta)
+    res = ScfResult(False, 0, 0.0)
+
+    def mark(name, t):
+        # per-phase wall time (synchronising), only when profiling
+        if not profile:
+            return t
+        torch.cuda.synchronize()
+        now = time.perf_counter()
+        res.phase_seconds[name] = res.phase_seconds.get(name, 0.0) + now - t
+        return now
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for iscf in range(1, looplimit + 1):
+        ti = time.perf_counter()
+        tp = ti
+        mixer.step(rho_o, rho_i, dvol)
+        tp = mark("mixing", tp)
+        rho_d = K.trans_c2d_smtcharge(shape, 4, rho_i)
+        it, _ = K.scf_hartree(dshape, 4, xmax, rho_d, vh_d, epsvh)
+        tp = mark("hartree", tp)
+        vh = K.trans_d2c(shape, 4, vh_d)
+        vx_d, _ = K.vxpot_lda_pz(rho_d)
+        vx = K.trans_d2c(shape, 4, vx_d)
+        K.veff_sum(vx, vloc_t, vh, veff64, veff32)
+        tp = mark("xc+transfer", tp)
+        K.scf_diag(b, veff, dij, iscf, prm)
+        tp = mark("scf_diag", tp)
+        rho_o = K.scf_charge_smt(occ, b.psi, N)
+        diff = K.scf_diffcharge(rho_o, rho_i, h, xmax)
+        tp = mark("charge", tp)
+        res.diff.append(diff)
+        res.hartree_iters.append(it)
+        res.seconds_per_iter.append(time.perf_counter() - ti)
+        res.iterations = iscf
+        if log:
+            log(f"iscf {iscf:3d}  diff_charge {diff:.3e}  hartree_cg {it}  "
+                f"{res.seconds_per_iter[-1]:.3f} s")
+        if diff < eps_scf:
+            res.converged = True
+            break
+    torch.cuda.synchronize()
+    res.seconds = time.perf_counter() - t0
+    res.sval = np.array(b.sval)
+    occ_h = occ.cpu().numpy()
+    res.eband = float(np.sum(occ_h * res.sval))
+    mixer.close()
+    return res

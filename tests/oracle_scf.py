@@ -1,0 +1,58 @@
+"""The SCF loop of rspacedist_b200.scf restated on the CPU oracle (test
+infrastructure): same model inputs, same step order, FP64 throughout.  Per
+iteration: Broyden mixing, c2d, Hartree CG, PZ LDA, d2c, veff sum, then
+Rayleigh-Ritz + CG (iscf <= ncgscf) or Rayleigh-Ritz + DIIS, a stable
+ascending reorder, the density and the charge difference."""
+import numpy as np
+
+
+def geo_dict(cell):
+    return dict(natom=cell.natom, nprjmx=cell.nprjmx, num_list=cell.num_list, nprj=cell.nprj,
+                natinf=cell.natinf, lst=cell.lst, v=cell.vnlocp.ravel())
+
+
+def oracle_scf(O, cell, M, nocc, eps_scf=1e-6, looplimit=100, nbrydn=20, eta=0.02, seed=0,
+               ncgscf=3, zval=4.0, epsvh=1e-12):
+    from rspacedist_b200 import scf as SCF
+    geo = geo_dict(cell)
+    N, shape = cell.N, cell.shape
+    dshape = tuple(2 * s for s in shape)
+    h, xmax = cell.h, cell.xmax
+    dvol = h[0] * h[1] * h[2]
+    vloc = SCF.model_local_potential(cell)
+    rho_o = SCF.atomic_density(cell, zval)
+    psi = SCF.smooth_start_bands(shape, M, seed)
+    sysk = O.make_sys(geo, shape, 4, h, np.zeros(N), cell.dij, cell.sss)
+    rp = O.nl_dot(geo, psi, N)
+    sp = O.spsi(sysk, psi, rp) if cell.sss is not None else None
+    psi, sp, rp = O.ortho(sysk, M, psi, sp, rp, 0, 1)
+    occ = np.zeros(M)
+    occ[:nocc] = 2.0
+    mix = O.Broyden(N, nbrydn, eta)
+    rho_i = np.zeros(N)
+    vh_d = np.zeros(8 * N)
+    diffs = []
+    sval = None
+    for iscf in range(1, looplimit + 1):
+        rho_i = mix.step(rho_o, rho_i, dvol)
+        rho_d = O.interp_c2d(shape, 4, rho_i)
+        vh_d, _, _ = O.hartree_cg(dshape, 4, xmax, epsvh, 1, 800, 801, rho_d, vh_d)
+        vh = O.interp_d2c(shape, 4, vh_d)
+        vx = O.interp_d2c(shape, 4, O.vxc_pz(rho_d)[0])
+        veff = O.veff_sum(vx, vloc, vh)
+        sysk = O.make_sys(geo, shape, 4, h, veff, cell.dij, cell.sss)
+        _, psi, sp, rp, sval = O.rayleighritz(sysk, M, psi, sp, rp)
+        if iscf <= ncgscf:
+            _, psi, sp, rp, _, sval, _ = O.kscg(sysk, M, psi, sp, rp, nsdmax=4)
+        else:
+            _, psi, sp, rp, _, sval, _ = O.ksdiis(sysk, M, psi, sp, rp, l_hsv=1)
+        order = np.argsort(sval, kind="stable")
+        psi, rp, sval = psi[order], rp[order], sval[order]
+        if sp is not None:
+            sp = sp[order]
+        rho_o = O.density(occ, psi, N)
+        diffs.append(O.diffcharge(rho_o, rho_i, h, xmax))
+        if diffs[-1] < eps_scf:
+            break
+    return dict(sval=np.asarray(sval), eband=float(np.sum(occ * sval)), diff=diffs,
+                converged=diffs[-1] < eps_scf, iterations=len(diffs))

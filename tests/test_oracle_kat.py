@@ -237,3 +237,80 @@ def test_force_nl_is_minus_energy_gradient(oracle, kind, n, tol):
             p[a, ax] -= 2 * d
             em = energy(S.make_cell(a0, n, p, ds))
             assert abs(F[a, ax] + (ep - em) / (2 * d)) < tol * np.abs(F).max(), (a, ax)
+
+
+def test_d2c_is_the_scaled_transpose_of_c2d(oracle):
+    """trans_d2c (interpolation mode 2 + periodic fold + 1/nmesh^3) is the exact
+    transpose of the periodic coarse->dense interpolation divided by 8:
+    <c2d(u), w>_dense = 8 <u, d2c(w)>_coarse for any u, w."""
+    rng = np.random.default_rng(5)
+    for shape in ((8, 10, 12), (16, 16, 16)):
+        nx, ny, nz = shape
+        u = rng.standard_normal(nx * ny * nz)
+        w = rng.standard_normal(8 * nx * ny * nz)
+        lhs = oracle.interp_c2d(shape, 4, u) @ w
+        rhs = 8.0 * (u @ oracle.interp_d2c(shape, 4, w))
+        assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+        # a constant field maps to the same constant (weights sum to one)
+        c = oracle.interp_d2c(shape, 4, np.full(8 * nx * ny * nz, 0.7))
+        np.testing.assert_allclose(c, 0.7, rtol=1e-14)
+
+
+def test_pz_lda_known_values_and_derivative(oracle):
+    """Exchange part -0.458165.../rs; v = d(rho eps)/drho (central differences)
+    on both sides of rs = 1; eps continuous at rs = 1 to the fit's accuracy."""
+    pi = np.pi
+    rs = np.array([0.3, 0.7, 0.999, 1.0, 1.5, 3.0, 8.0])
+    rho = 3.0 / (4.0 * pi * rs ** 3)
+    vx, ex = oracle.vxc_pz(rho)
+    cx = 0.75 * (2.25 / pi ** 2) ** (1 / 3)
+    assert abs(cx - 0.4581652932831429) < 1e-15
+    ec = np.where(rs >= 1.0, -0.1423 / (1 + 1.0529 * np.sqrt(rs) + 0.3334 * rs),
+                  -0.048 + 0.0311 * np.log(rs) - 0.0116 * rs + 0.002 * rs * np.log(rs))
+    np.testing.assert_allclose(ex, ec - cx / rs, rtol=1e-14)
+    for r in rho[np.abs(rs - 1.0) > 1e-2]:  # the fit switches branch at rs = 1
+        d = 1e-6 * r
+        ep, em = oracle.vxc_pz([r + d])[1][0], oracle.vxc_pz([r - d])[1][0]
+        fd = ((r + d) * ep - (r - d) * em) / (2 * d)
+        assert abs(fd - oracle.vxc_pz([r])[0][0]) < 1e-8
+    lo, hi = oracle.vxc_pz([3.0 / (4.0 * pi * (1 - 1e-12)), 3.0 / (4.0 * pi)])[1]
+    assert abs(lo - hi) < 1e-4
+    vx0, ex0 = oracle.vxc_pz([0.0, 1e-16])
+    assert not vx0.any() and not ex0.any()
+
+
+def test_diffcharge(oracle):
+    rng = np.random.default_rng(2)
+    a, b = rng.random(5000), rng.random(5000)
+    h, xmax = (0.3, 0.31, 0.29), (3.0, 3.1, 2.9)
+    ref = np.sqrt(np.sum((b - a) ** 2) * h[0] * h[1] * h[2] / (8 * xmax[0] * xmax[1] * xmax[2]))
+    assert abs(oracle.diffcharge(a, b, h, xmax) - ref) < 1e-14 * ref
+
+
+def test_broyden_first_step_is_linear_and_it_solves_a_fixed_point(oracle):
+    """scf_chargemixing: the first call copies rho_out, the second is linear
+    mixing with eta; on rho_out = A rho_in + c (A symmetric, eigenvalues in
+    [-0.9, 0.95]) the Broyden iteration reaches the fixed point far faster
+    than linear mixing."""
+    rng = np.random.default_rng(3)
+    n = 300
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    A = Q @ np.diag(np.linspace(-0.9, 0.95, n)) @ Q.T
+    c = rng.standard_normal(n)
+    fix = np.linalg.solve(np.eye(n) - A, c)
+    mix = oracle.Broyden(n, nbrydn=8, eta=0.3)
+    r0 = rng.standard_normal(n)
+    ri = mix.step(r0, np.zeros(n), 0.01)
+    assert np.array_equal(ri, r0)
+    ro = A @ ri + c
+    r2 = mix.step(ro, ri, 0.01)
+    np.testing.assert_array_equal(r2, ri + (ro - ri) * 0.3)
+    ri = r2
+    for _ in range(100):
+        ro = A @ ri + c
+        ri = mix.step(ro, ri, 0.01)
+    assert np.linalg.norm(ri - fix) < 1e-7 * np.linalg.norm(fix)
+    lin = r0.copy()
+    for _ in range(101):
+        lin = lin + 0.3 * (A @ lin + c - lin)
+    assert np.linalg.norm(lin - fix) > 1e-3 * np.linalg.norm(fix)
