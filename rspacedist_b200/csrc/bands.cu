@@ -127,21 +127,6 @@ __global__ void k_resid(long n, const T* __restrict__ h, const T* __restrict__ s
   r[i] = (T)(-fma(-*lam, (double)s[i], (double)h[i]));
 }
 
-// c = a + d*b  (ksdiis_r_01), d = sign * (*dp)
-template <class T>
-__global__ void k_axpy(long n, const T* __restrict__ a, const T* __restrict__ b,
-                       const double* __restrict__ dp, double sign, T* __restrict__ c) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double d = sign * *dp;
-  c[i] = (T)fma(d, (double)b[i], (double)a[i]);
-}
-__global__ void k_axpy_d(long n, const double* __restrict__ a, const double* __restrict__ b,
-                         const double* __restrict__ dp, double* __restrict__ c) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  c[i] = fma(*dp, b[i], a[i]);
-}
 
 // kscg_r_03 on the grid vectors and the rp vectors
 template <class T>
@@ -176,23 +161,6 @@ __global__ void k_cg_rot(long n, T* __restrict__ psi, const T* __restrict__ p, T
   if (i < nrp) rp[i] = fma(be, rpl[i], al * rp[i]);
 }
 
-// new = c1 y1 + c0 y0 (ksdiis_r_03 with two vectors); rp form starts from 0
-template <class T>
-__global__ void k_comb2(long n, const T* __restrict__ y0, const T* __restrict__ y1,
-                        const double* __restrict__ c, T* __restrict__ out) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  out[i] = (T)fma(c[1], (double)y1[i], c[0] * (double)y0[i]);
-}
-__global__ void k_comb2_rp(long n, const double* __restrict__ y0, const double* __restrict__ y1,
-                           const double* __restrict__ c, double* __restrict__ out) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double acc = 0.0;
-  acc = fma(c[0], y0[i], acc);
-  acc = fma(c[1], y1[i], acc);
-  out[i] = acc;
-}
 
 // ------------------------------------------------------------ scalar kernels
 // device scalars of one band step
@@ -227,8 +195,8 @@ __global__ void k_cg_alphabeta(Sc* sc, const double* __restrict__ sval) {
 }
 
 // DIIS step length (ksdiis8f.F90:285-320)
-__global__ void k_diis_lambda(Sc* sc, const double* __restrict__ sval, double a1, double dx,
-                              double dy, double dz, double lmin, double lmax) {
+__device__ void diis_lambda(Sc* sc, const double* __restrict__ sval, double a1, double dx,
+                            double dy, double dz, double lmin, double lmax) {
   const double sv = *sval;
   const double aaa = 2.0 * fma(-sv, sc->s[1], sc->s[0]) * dx * dy * dz;
   const double valre = sc->s[2] / sc->s[3];
@@ -238,8 +206,6 @@ __global__ void k_diis_lambda(Sc* sc, const double* __restrict__ sval, double a1
   if (al < lmin) al = lmin;
   sc->lam = al;
 }
-
-__global__ void k_diis_norm(Sc* sc) { sc->tmp = 1.0 / sqrt(sc->rs[3]); }
 
 __device__ void eig2(const double a[4], double w[2], double z[4]) {
   const double p = a[0], q = a[3], r = 0.5 * (a[1] + a[2]);
@@ -265,7 +231,7 @@ __device__ void eig2(const double a[4], double w[2], double z[4]) {
 }
 
 // DIIS 2x2 subspace solve (ksdiis8f.F90:405-548); rs/rr already scaled
-__global__ void k_diis_solve(Sc* sc, double eps_eig, double* __restrict__ resid) {
+__device__ void diis_solve(Sc* sc, double eps_eig, double* __restrict__ resid) {
   double rs[4], rr[4], rs0[4];
   for (int k = 0; k < 4; ++k) { rs[k] = sc->rs[k]; rr[k] = sc->rr[k]; rs0[k] = rs[k]; }
   double w[2], z[4], eig[2], vec[4];
@@ -321,13 +287,134 @@ __global__ void k_diis_solve(Sc* sc, double eps_eig, double* __restrict__ resid)
 }
 
 // scale row/column 2 of the DIIS matrices by tmp (rs(2,2) twice)
-__global__ void k_diis_scale_mats(Sc* sc) {
+__device__ void diis_scale_mats(Sc* sc) {
   const double t = sc->tmp;
   for (int i = 0; i < 2; ++i) { sc->rs[1 * 2 + i] *= t; sc->rr[1 * 2 + i] *= t; }
   for (int i = 0; i < 2; ++i) { sc->rs[i * 2 + 1] *= t; sc->rr[i * 2 + 1] *= t; }
 }
 
 __global__ void k_copy_d(double* dst, const double* src) { *dst = *src; }
+
+// ------------------------------------------------------------ band-batched DIIS
+// ksdiis_r updates every band from its own vectors only, so one step of the
+// band loop runs for a block of bands at once: vectors of band j of the
+// block sit at offset j*n, its scalars in sc[j].  Each band sees the same
+// operations and tree orders as in the band-by-band loop.
+static_assert(sizeof(Sc) % sizeof(double) == 0, "Sc fields are addressed as doubles");
+constexpr long kScStride = sizeof(Sc) / sizeof(double);
+
+// out[j*ostride] = tree_dot(A_j, B_j) (times dV when scale)
+template <class T>
+__global__ void k_pdot_partial(long n, const T* __restrict__ A, const T* __restrict__ Bv,
+                               long nblk, double* __restrict__ part) {
+  __shared__ double ws[8];
+  const int j = blockIdx.y;
+  const T* a = A + (long)j * n;
+  const T* b = Bv + (long)j * n;
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < kTreePerLane; ++k) {
+    const long i = base + (long)k * kTreeLanes;
+    if (i < n) acc = fma((double)a[i], (double)b[i], acc);
+  }
+  const double s = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) part[(long)j * nblk + blockIdx.x] = s;
+}
+
+__global__ void k_pdot_final(long nblk, const double* __restrict__ part, double dx, double dy,
+                             double dz, int scale, double* __restrict__ out, long ostride) {
+  __shared__ double ws[8];
+  const int j = blockIdx.x;
+  double acc = 0.0;
+  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + part[(long)j * nblk + k];
+  const double s = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) out[(long)j * ostride] = scale ? s * dx * dy * dz : s;
+}
+
+// c_j = a_j + d_j b_j, d_j = sign * dp[j*dstride]  (ksdiis_r_01)
+template <class T>
+__global__ void k_axpy_b(long n, const T* __restrict__ a, const T* __restrict__ b,
+                         const double* __restrict__ dp, long dstride, double sign,
+                         T* __restrict__ c) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long o = (long)blockIdx.y * n + i;
+  const double d = sign * dp[(long)blockIdx.y * dstride];
+  c[o] = (T)fma(d, (double)b[o], (double)a[o]);
+}
+__global__ void k_axpy_d_b(long n, const double* __restrict__ a, const double* __restrict__ b,
+                           const double* __restrict__ dp, long dstride, double* __restrict__ c) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long o = (long)blockIdx.y * n + i;
+  c[o] = fma(dp[(long)blockIdx.y * dstride], b[o], a[o]);
+}
+
+// k_scale3 per band with t = tmp[j*tstride]
+template <class T>
+__global__ void k_scale3_b(long n, T* __restrict__ a, T* __restrict__ b, long nrp,
+                           double* __restrict__ r, const double* __restrict__ tmp, long tstride) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  const double t = tmp[(long)j * tstride];
+  if (i < n) {
+    const long o = (long)j * n + i;
+    a[o] = (T)((double)a[o] * t);
+    if (b) b[o] = (T)((double)b[o] * t);
+  }
+  if (i < nrp) r[(long)j * nrp + i] = r[(long)j * nrp + i] * t;
+}
+
+// new_j = c1 y1_j + c0 y0_j (ksdiis_r_03 with two vectors; the rp form
+// starts from 0), c = cc + j*cstride
+// (y0 and out may be the same array: each element is read before it is written)
+template <class T>
+__global__ void k_comb2_b(long n, const T* y0, const T* __restrict__ y1,
+                          const double* __restrict__ cc, long cstride, T* out) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* c = cc + (long)blockIdx.y * cstride;
+  const long o = (long)blockIdx.y * n + i;
+  out[o] = (T)fma(c[1], (double)y1[o], c[0] * (double)y0[o]);
+}
+__global__ void k_comb2_rp_b(long n, const double* y0, const double* __restrict__ y1,
+                             const double* __restrict__ cc, long cstride, double* out) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* c = cc + (long)blockIdx.y * cstride;
+  const long o = (long)blockIdx.y * n + i;
+  double acc = 0.0;
+  acc = fma(c[0], y0[o], acc);
+  acc = fma(c[1], y1[o], acc);
+  out[o] = acc;
+}
+
+__global__ void k_diis_lambda_b(int nb, Sc* sc, const double* __restrict__ sval, double a1,
+                                double dx, double dy, double dz, double lmin, double lmax) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < nb) diis_lambda(sc + j, sval + j, a1, dx, dy, dz, lmin, lmax);
+}
+
+// the symmetric entries of the 2x2 matrices, then tmp = 1/sqrt(rs(2,2))
+__global__ void k_diis_norm_b(int nb, Sc* sc) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nb) return;
+  Sc* s = sc + j;
+  s->rs[1 * 2 + 0] = s->rs[0 * 2 + 1];
+  s->rr[1 * 2 + 0] = s->rr[0 * 2 + 1];
+  s->tmp = 1.0 / sqrt(s->rs[3]);
+}
+
+__global__ void k_diis_scale_mats_b(int nb, Sc* sc) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < nb) diis_scale_mats(sc + j);
+}
+
+__global__ void k_diis_solve_b(int nb, Sc* sc, double eps_eig, double* __restrict__ resid) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < nb) diis_solve(sc + j, eps_eig, resid + j);
+}
 
 __global__ void k_gather_bands_d(long n, int M, const int* __restrict__ rank,
                                  const double* __restrict__ src, double* __restrict__ dst) {
@@ -633,99 +720,126 @@ static int kscg(BandCtx<T>& c, const rs_solver_prm* prm, double* sval_h, double*
 template <class T>
 static int ksdiis(BandCtx<T>& c, const rs_solver_prm* prm, int l_hsv, double* sval_h,
                   double* resid_h, int* ksconv) {
-  int rc = c.init(8, 4);
+  int rc = c.init(0, 0);
   if (rc) return rc;
   const long N = c.N;
+  const long nrp = c.nrp;
   const bool sp = c.sep();
-  T* ph[2] = {c.w[0], c.w[1]};
-  T* sph[2] = {sp ? c.w[2] : c.w[0], sp ? c.w[3] : c.w[1]};
-  T* hph[2] = {c.w[4], c.w[5]};
-  T* rvv[2] = {c.w[6], c.w[7]};
-  T *rvre = nullptr, *avre = nullptr, *asvre = nullptr;
-  RS_CUDA(cudaMallocAsync((void**)&rvre, sizeof(T) * N * 3, c.st));
-  avre = rvre + N;
-  asvre = avre + N;
-  double *rph[2] = {c.wrp[0], c.wrp[1]}, *rpsep = c.wrp[2];
-  double* dval = nullptr;
-  double* dres = nullptr;
-  RS_CUDA(cudaMallocAsync((void**)&dval, sizeof(double) * 2 * (c.M + 1), c.st));
-  dres = dval + c.M + 1;
-  RS_CUDA(cudaMemcpyAsync(dres, resid_h, sizeof(double) * c.M, cudaMemcpyHostToDevice, c.st));
+  const int M = c.M;
+  // a block of B bands runs each step of the band loop at once; its work
+  // vectors (phi1, H phi1, two residuals, the preconditioned residual and its
+  // H image, plus S phi1 and the S image with an S metric) stay within ~8 GB
+  const int nvec = sp ? 8 : 6;
+  const long per_band = (long)nvec * N * (long)sizeof(T) + 2 * nrp * (long)sizeof(double);
+  const int B = (int)std::min<long>(std::min<long>(M, 65535),
+                                    std::max<long>(1, (8L << 30) / per_band));
+  T* wv = nullptr;
+  double* wd = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&wv, sizeof(T) * (size_t)nvec * B * N, c.st));
+  const size_t nd = (size_t)2 * B * (nrp > 0 ? nrp : 1) + 2 * (M + 1) + 1;
+  cudaError_t e = cudaMallocAsync((void**)&wd, sizeof(double) * nd, c.st);
+  Sc* scb = nullptr;
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&scb, sizeof(Sc) * B, c.st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(scb, 0, sizeof(Sc) * B, c.st);
+  if (e != cudaSuccess) rc = cuda_status(e, "ksdiis: work arrays");
+  const size_t BN = (size_t)B * N;
+  T* ph1 = wv;
+  T* hph1 = ph1 + BN;
+  T* rvv0 = hph1 + BN;
+  T* rvv1 = rvv0 + BN;
+  T* rvre = rvv1 + BN;
+  T* avre = rvre + BN;
+  T* sph1 = sp ? avre + BN : ph1;
+  T* asvre = sp ? sph1 + BN : nullptr;
+  double* rph1 = wd;
+  double* rpsep = rph1 + (size_t)B * (nrp > 0 ? nrp : 1);
+  double* dval = rpsep + (size_t)B * (nrp > 0 ? nrp : 1);
+  double* dres = dval + M + 1;
+  double* da1 = dres + M + 1;
   const double a1 = prm->alambda_diis;
-  double* da1 = nullptr;
-  RS_CUDA(cudaMallocAsync((void**)&da1, sizeof(double), c.st));
-  RS_CUDA(cudaMemcpyAsync(da1, &a1, sizeof(double), cudaMemcpyHostToDevice, c.st));
-  const unsigned gN = div_up(N, 256), gR = div_up(c.nrp > 0 ? c.nrp : 1, 256);
-  for (int jiter = 1; jiter + 1 <= prm->ndiismax && !rc; ++jiter) {
-    for (int l = 0; l < c.M && !rc; ++l) {
-      cudaMemcpyAsync(ph[0], c.band(c.psi, l), sizeof(T) * N, cudaMemcpyDeviceToDevice, c.st);
-      if (sp) cudaMemcpyAsync(sph[0], c.band(c.spsi, l), sizeof(T) * N, cudaMemcpyDeviceToDevice, c.st);
-      if (c.nrp) cudaMemcpyAsync(rph[0], c.rpb(c.rp, l), sizeof(double) * c.nrp, cudaMemcpyDeviceToDevice, c.st);
-      if ((rc = c.apply_h(ph[0], rph[0], hph[0], 1))) break;
-      if ((rc = c.bdot(ph[0], 1, hph[0], dval + l))) break;
-      k_axpy<T><<<gN, 256, 0, c.st>>>(N, hph[0], sph[0], dval + l, -1.0, rvv[0]);
-      if (prm->nprecon_diis) rc = c.precond(rvv[0], rvre);
-      else cudaMemcpyAsync(rvre, rvv[0], sizeof(T) * N, cudaMemcpyDeviceToDevice, c.st);
+  if (!rc) {
+    cudaMemcpyAsync(dres, resid_h, sizeof(double) * M, cudaMemcpyHostToDevice, c.st);
+    cudaMemcpyAsync(da1, &a1, sizeof(double), cudaMemcpyHostToDevice, c.st);
+  }
+  auto pdot = [&](const T* a, const T* b, int nb, double* out, long ostride, int scale) {
+    dim3 grid((unsigned)c.nblk, nb);
+    k_pdot_partial<T><<<grid, kTreeLanes, 0, c.st>>>(N, a, b, c.nblk, c.part);
+    k_pdot_final<<<nb, kTreeLanes, 0, c.st>>>(c.nblk, c.part, c.dx, c.dy, c.dz, scale, out,
+                                              ostride);
+  };
+  for (int b0 = 0; b0 < M && !rc; b0 += B) {
+    const int nb = std::min(B, M - b0);
+    T* ps = c.band(c.psi, b0);                 // phi0 (psi), overwritten by the combination
+    T* ss = sp ? c.band(c.spsi, b0) : ps;      // S phi0
+    T* hs = c.band(c.hpsi, b0);                // H phi0, computed afresh each sweep
+    double* rps = c.rpb(c.rp, b0);
+    T* sph1v = sp ? sph1 : ph1;
+    const dim3 gv(div_up(N, 256), nb), gr(div_up(nrp > 0 ? nrp : 1, 256), nb);
+    const dim3 g3(div_up(std::max(N, nrp), 256), nb);
+    const unsigned gs = div_up(nb, 128);
+    for (int jiter = 1; jiter + 1 <= prm->ndiismax && !rc; ++jiter) {
+      if ((rc = c.apply_h(ps, rps, hs, nb))) break;
+      pdot(ps, hs, nb, dval + b0, 1, 1);
+      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, hs, ss, dval + b0, 1, -1.0, rvv0);
+      if (prm->nprecon_diis) rc = launch_precondition<T>(c.g, rvv0, rvre, nb, c.st);
+      else rc = cudaMemcpyAsync(rvre, rvv0, sizeof(T) * N * nb, cudaMemcpyDeviceToDevice, c.st)
+                    == cudaSuccess ? RS_OK : RS_ECUDA;
       if (rc) break;
-      if ((rc = c.nl_dot(rvre, rpsep, 1))) break;
-      if ((rc = c.apply_h(rvre, rpsep, avre, 1))) break;
-      if ((rc = c.apply_s(rvre, rpsep, asvre, 1))) break;
+      if ((rc = c.nl_dot(rvre, rpsep, nb))) break;
+      if ((rc = c.apply_h(rvre, rpsep, avre, nb))) break;
+      if (sp && (rc = c.apply_s(rvre, rpsep, asvre, nb))) break;
       // trial step with alambda_diis
-      if (c.nrp) k_axpy_d<<<gR, 256, 0, c.st>>>(c.nrp, rph[0], rpsep, da1, rph[1]);
-      k_axpy<T><<<gN, 256, 0, c.st>>>(N, ph[0], rvre, da1, 1.0, ph[1]);
-      k_axpy<T><<<gN, 256, 0, c.st>>>(N, hph[0], avre, da1, 1.0, hph[1]);
-      if (sp) k_axpy<T><<<gN, 256, 0, c.st>>>(N, sph[0], asvre, da1, 1.0, sph[1]);
-      if ((rc = c.bdot(rvre, 1, hph[0], &c.sc->s[0], 0))) break;
-      if ((rc = c.bdot(rvre, 1, sph[0], &c.sc->s[1], 0))) break;
-      if ((rc = c.bdot(ph[1], 1, hph[1], &c.sc->s[2], 0))) break;
-      if ((rc = c.bdot(ph[1], 1, sph[1], &c.sc->s[3], 0))) break;
-      k_diis_lambda<<<1, 1, 0, c.st>>>(c.sc, dval + l, a1, c.dx, c.dy, c.dz, prm->alambda_min,
-                                       prm->alambda_max);
-      k_axpy<T><<<gN, 256, 0, c.st>>>(N, ph[0], rvre, &c.sc->lam, 1.0, ph[1]);
-      k_axpy<T><<<gN, 256, 0, c.st>>>(N, hph[0], avre, &c.sc->lam, 1.0, hph[1]);
-      if (sp) k_axpy<T><<<gN, 256, 0, c.st>>>(N, sph[0], asvre, &c.sc->lam, 1.0, sph[1]);
-      if (c.nrp) k_axpy_d<<<gR, 256, 0, c.st>>>(c.nrp, rph[0], rpsep, &c.sc->lam, rph[1]);
-      for (int j = 0; j < 2; ++j)
-        k_axpy<T><<<gN, 256, 0, c.st>>>(N, hph[j], sph[j], dval + l, -1.0, rvv[j]);
-      for (int j = 0; j < 2 && !rc; ++j)
-        for (int i = 0; i <= j && !rc; ++i) {
-          if ((rc = c.bdot(ph[i], 1, sph[j], &c.sc->rs[i * 2 + j]))) break;
-          if ((rc = c.bdot(rvv[i], 1, rvv[j], &c.sc->rr[i * 2 + j]))) break;
-          if (i != j) {
-            k_copy_d<<<1, 1, 0, c.st>>>(&c.sc->rs[j * 2 + i], &c.sc->rs[i * 2 + j]);
-            k_copy_d<<<1, 1, 0, c.st>>>(&c.sc->rr[j * 2 + i], &c.sc->rr[i * 2 + j]);
-          }
-        }
-      if (rc) break;
-      k_diis_norm<<<1, 1, 0, c.st>>>(c.sc);
-      k_scale3<T><<<c.gN(), 256, 0, c.st>>>(N, ph[1], hph[1], c.nrp, rph[1], &c.sc->tmp);
-      if (sp) k_scale3<T><<<gN, 256, 0, c.st>>>(N, sph[1], rvv[1], 0, nullptr, &c.sc->tmp);
-      else k_scale3<T><<<gN, 256, 0, c.st>>>(N, rvv[1], nullptr, 0, nullptr, &c.sc->tmp);
-      k_diis_scale_mats<<<1, 1, 0, c.st>>>(c.sc);
-      k_diis_solve<<<1, 1, 0, c.st>>>(c.sc, prm->eps_eig_diis, dres + l);
-      k_comb2<T><<<gN, 256, 0, c.st>>>(N, ph[0], ph[1], c.sc->c, c.band(c.psi, l));
-      if (sp) k_comb2<T><<<gN, 256, 0, c.st>>>(N, sph[0], sph[1], c.sc->c, c.band(c.spsi, l));
-      k_comb2<T><<<gN, 256, 0, c.st>>>(N, hph[0], hph[1], c.sc->c, c.band(c.hpsi, l));
-      if (c.nrp) k_comb2_rp<<<gR, 256, 0, c.st>>>(c.nrp, rph[0], rph[1], c.sc->c, c.rpb(c.rp, l));
-      cudaError_t e = cudaGetLastError();
+      if (nrp) k_axpy_d_b<<<gr, 256, 0, c.st>>>(nrp, rps, rpsep, da1, 0, rph1);
+      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, ps, rvre, da1, 0, 1.0, ph1);
+      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, hs, avre, da1, 0, 1.0, hph1);
+      if (sp) k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, ss, asvre, da1, 0, 1.0, sph1);
+      pdot(rvre, hs, nb, &scb->s[0], kScStride, 0);
+      pdot(rvre, ss, nb, &scb->s[1], kScStride, 0);
+      pdot(ph1, hph1, nb, &scb->s[2], kScStride, 0);
+      pdot(ph1, sph1v, nb, &scb->s[3], kScStride, 0);
+      k_diis_lambda_b<<<gs, 128, 0, c.st>>>(nb, scb, dval + b0, a1, c.dx, c.dy, c.dz,
+                                            prm->alambda_min, prm->alambda_max);
+      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, ps, rvre, &scb->lam, kScStride, 1.0, ph1);
+      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, hs, avre, &scb->lam, kScStride, 1.0, hph1);
+      if (sp) k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, ss, asvre, &scb->lam, kScStride, 1.0, sph1);
+      if (nrp) k_axpy_d_b<<<gr, 256, 0, c.st>>>(nrp, rps, rpsep, &scb->lam, kScStride, rph1);
+      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, hs, ss, dval + b0, 1, -1.0, rvv0);
+      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, hph1, sph1v, dval + b0, 1, -1.0, rvv1);
+      pdot(ps, ss, nb, &scb->rs[0], kScStride, 1);
+      pdot(rvv0, rvv0, nb, &scb->rr[0], kScStride, 1);
+      pdot(ps, sph1v, nb, &scb->rs[1], kScStride, 1);
+      pdot(rvv0, rvv1, nb, &scb->rr[1], kScStride, 1);
+      pdot(ph1, sph1v, nb, &scb->rs[3], kScStride, 1);
+      pdot(rvv1, rvv1, nb, &scb->rr[3], kScStride, 1);
+      k_diis_norm_b<<<gs, 128, 0, c.st>>>(nb, scb);
+      k_scale3_b<T><<<g3, 256, 0, c.st>>>(N, ph1, hph1, nrp, rph1, &scb->tmp, kScStride);
+      if (sp) k_scale3_b<T><<<gv, 256, 0, c.st>>>(N, sph1, rvv1, 0, nullptr, &scb->tmp, kScStride);
+      else k_scale3_b<T><<<gv, 256, 0, c.st>>>(N, rvv1, nullptr, 0, nullptr, &scb->tmp, kScStride);
+      k_diis_scale_mats_b<<<gs, 128, 0, c.st>>>(nb, scb);
+      k_diis_solve_b<<<gs, 128, 0, c.st>>>(nb, scb, prm->eps_eig_diis, dres + b0);
+      k_comb2_b<T><<<gv, 256, 0, c.st>>>(N, ps, ph1, &scb->c[0], kScStride, ps);
+      if (sp) k_comb2_b<T><<<gv, 256, 0, c.st>>>(N, ss, sph1, &scb->c[0], kScStride, ss);
+      k_comb2_b<T><<<gv, 256, 0, c.st>>>(N, hs, hph1, &scb->c[0], kScStride, hs);
+      if (nrp) k_comb2_rp_b<<<gr, 256, 0, c.st>>>(nrp, rps, rph1, &scb->c[0], kScStride, rps);
+      e = cudaGetLastError();
       if (e != cudaSuccess) rc = cuda_status(e, "ksdiis");
     }
   }
   if (!rc) {
-    RS_CUDA(cudaMemcpyAsync(sval_h, dval, sizeof(double) * c.M, cudaMemcpyDeviceToHost, c.st));
-    RS_CUDA(cudaMemcpyAsync(resid_h, dres, sizeof(double) * c.M, cudaMemcpyDeviceToHost, c.st));
+    RS_CUDA(cudaMemcpyAsync(sval_h, dval, sizeof(double) * M, cudaMemcpyDeviceToHost, c.st));
+    RS_CUDA(cudaMemcpyAsync(resid_h, dres, sizeof(double) * M, cudaMemcpyDeviceToHost, c.st));
     RS_CUDA(cudaStreamSynchronize(c.st));
     int conv = 1;
-    for (int l = 0; l < c.M; ++l) conv = conv && (sqrt(resid_h[l]) <= prm->epssd);
+    for (int l = 0; l < M; ++l) conv = conv && (sqrt(resid_h[l]) <= prm->epssd);
     if (ksconv) *ksconv = conv;
   }
   if (!rc && l_hsv) {
     for (int i = 0; i < prm->northo && !rc; ++i) rc = c.ortho_all(true);
     if (!rc) rc = c.apply_h(c.psi, c.rp, c.hpsi, c.M);
   }
-  cudaFreeAsync(rvre, c.st);
-  cudaFreeAsync(dval, c.st);
-  cudaFreeAsync(da1, c.st);
+  if (wv) cudaFreeAsync(wv, c.st);
+  if (wd) cudaFreeAsync(wd, c.st);
+  if (scb) cudaFreeAsync(scb, c.st);
   c.release();
   return rc;
 }

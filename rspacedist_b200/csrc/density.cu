@@ -111,19 +111,141 @@ static InterpW interp_weights(int nf) {
 }
 
 // ------------------------------------------------------------ Hartree CG
-// Scalar steps of scf_hartree_cg kept on the device (one thread).
+// scf_hartree_cg (scf_hartree8f.F90:626-812).  Each iteration is five
+// launches: the stencil with the p.Ap chunk sums of the reduction tree, the
+// tree's final fold with alpha, the x/r update with the r.r chunk sums, the
+// final fold with beta, dp and the stopping test, and the direction update.
+// Every sum keeps the tree order of tree_dot (a point's chunk and lane are
+// those of k_tree_partial), so iterates equal the unfused sequence bit for
+// bit.  r1r of an iteration equals r2r of the one before (r is unchanged in
+// between) and is carried over instead of summed again.  The stopping test
+// runs on the device: once it fires, the kernels of the iterations already
+// queued return at once, and the host checks the flag every kCgBatch
+// iterations instead of after each one.
 struct CgScalars {
   double r1r, pap, r2r, alph, beta, dp, bve;
+  int done, iters;
 };
+static_assert(sizeof(CgScalars) <= 16 * sizeof(double), "CG scalars fit the work array");
 
-__global__ void k_cg_alpha(CgScalars* s) { s->alph = s->r1r / s->pap; }
+constexpr int kCgBatch = 16;
 
-__global__ void k_cg_beta(CgScalars* s, int loop, int ncgres, double ddx, double ddy,
-                          double ddz, double vol) {
-  double beta = s->r2r / s->r1r;
-  if (loop % ncgres == 0) beta = 0.0;
-  s->beta = beta;
-  s->dp = sqrt(s->r2r * ddx * ddy * ddz / vol);
+__device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// -1/2 lap v at point p, in k_hartree_lap's order (x with the diagonal, y, z);
+// 32-bit index arithmetic (the grid has fewer than 2^31 points)
+__device__ __forceinline__ double hlap_at(int nx, int ny, int nz, int nf, const HartreeCoefs& c,
+                                          const double* __restrict__ v, int p) {
+  const int pl = nx * ny;
+  const int iz = p / pl, rem = p - iz * pl;
+  const int iy = rem / nx, ix = rem - iy * nx;
+  const int row = p - ix;
+  const int col = p - iz * pl;  // iy*nx + ix
+  double acc = c.cx[nf] * __ldg(v + row + wrap1(ix - nf, nx));
+  for (int m = nf - 1; m >= 1; --m) acc = fma(c.cx[m], __ldg(v + row + wrap1(ix - m, nx)), acc);
+  acc = fma(c.diag, __ldg(v + p), acc);
+  for (int m = 1; m <= nf; ++m) acc = fma(c.cx[m], __ldg(v + row + wrap1(ix + m, nx)), acc);
+  const int zb = iz * pl + ix;
+  for (int m = nf; m >= 1; --m) acc = fma(c.cy[m], __ldg(v + zb + wrap1(iy - m, ny) * nx), acc);
+  for (int m = 1; m <= nf; ++m) acc = fma(c.cy[m], __ldg(v + zb + wrap1(iy + m, ny) * nx), acc);
+  for (int m = nf; m >= 1; --m) acc = fma(c.cz[m], __ldg(v + wrap1(iz - m, nz) * pl + col), acc);
+  for (int m = 1; m <= nf; ++m) acc = fma(c.cz[m], __ldg(v + wrap1(iz + m, nz) * pl + col), acc);
+  return acc;
+}
+
+// ap = A p and the chunk sums of p.ap
+__global__ void __launch_bounds__(kTreeLanes) k_cg_lap_pap(int nx, int ny, int nz, int nf,
+                                                           HartreeCoefs c,
+                                                           const double* __restrict__ p,
+                                                           double* __restrict__ ap,
+                                                           double* __restrict__ part,
+                                                           const CgScalars* __restrict__ s) {
+  if (s->done) return;
+  __shared__ double ws[8];
+  const long N = (long)nx * ny * nz;
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  double acc = 0.0;
+#pragma unroll 4
+  for (int k = 0; k < kTreePerLane; ++k) {
+    const long i = base + (long)k * kTreeLanes;
+    if (i < N) {
+      const double a = hlap_at(nx, ny, nz, nf, c, p, (int)i);
+      ap[i] = a;
+      acc = fma(p[i], a, acc);
+    }
+  }
+  const double t = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// pap = fold(part); alpha = r1r / pap
+__global__ void k_cg_fold_alpha(long nblk, const double* __restrict__ part, CgScalars* s) {
+  if (s->done) return;
+  __shared__ double ws[8];
+  double acc = 0.0;
+  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + part[k];
+  const double t = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) {
+    s->pap = t;
+    s->alph = s->r1r / t;
+  }
+}
+
+// scf_hartee_cg_03 and the residual of scf_hartee_cg_04, with the r.r chunk sums
+__global__ void __launch_bounds__(kTreeLanes) k_cg_update_rr(long N, CgScalars* s,
+                                                             double* __restrict__ vh,
+                                                             const double* __restrict__ p,
+                                                             const double* __restrict__ ap,
+                                                             double* __restrict__ avhs,
+                                                             const double* __restrict__ b,
+                                                             double* __restrict__ r,
+                                                             double* __restrict__ part) {
+  if (s->done) return;
+  __shared__ double ws[8];
+  const double alph = s->alph;
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  double acc = 0.0;
+#pragma unroll 4
+  for (int k = 0; k < kTreePerLane; ++k) {
+    const long i = base + (long)k * kTreeLanes;
+    if (i < N) {
+      vh[i] = fma(alph, p[i], vh[i]);
+      const double a = fma(alph, ap[i], avhs[i]);
+      avhs[i] = a;
+      const double ri = b[i] - a;
+      r[i] = ri;
+      acc = fma(ri, ri, acc);
+    }
+  }
+  const double t = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// r2r = fold(part); beta, dp and the stopping rule of scf_hartree_cg
+// (restart every ncgres; at least ncgmin, at most ncgmax iterations)
+__global__ void k_cg_fold_beta(long nblk, const double* __restrict__ part, CgScalars* s,
+                               int loop, int ncgres, int ncgmin, int ncgmax, double epsvh,
+                               double ddx, double ddy, double ddz, double vol) {
+  if (s->done) return;
+  __shared__ double ws[8];
+  double acc = 0.0;
+  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + part[k];
+  const double t = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) {
+    s->r2r = t;
+    double beta = t / s->r1r;
+    if (loop % ncgres == 0) beta = 0.0;
+    s->beta = beta;
+    s->dp = sqrt(t * ddx * ddy * ddz / vol);
+    s->r1r = t;
+    s->iters = loop;
+    bool stop = false;
+    if (loop >= ncgmin) {
+      if (loop >= ncgmax) stop = true;
+      else if (!(s->dp > epsvh)) stop = true;
+    }
+    if (stop) s->done = 1;
+  }
 }
 
 __global__ void k_cg_bvec(long N, const double* __restrict__ rho, double two_pi, double ddx,
@@ -157,23 +279,10 @@ __global__ void k_cg_init(long N, const double* __restrict__ b, const double* __
   p[i] = ri;
 }
 
-// scf_hartee_cg_03 then the residual of scf_hartee_cg_04
-__global__ void k_cg_update(long N, const CgScalars* __restrict__ s, double* __restrict__ vh,
-                            const double* __restrict__ p, const double* __restrict__ ap,
-                            double* __restrict__ avhs, const double* __restrict__ b,
-                            double* __restrict__ r) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const double alph = s->alph;
-  vh[i] = fma(alph, p[i], vh[i]);
-  const double a = fma(alph, ap[i], avhs[i]);
-  avhs[i] = a;
-  r[i] = b[i] - a;
-}
-
 // scf_hartee_cg_05: p = r + beta p
 __global__ void k_cg_dir(long N, const CgScalars* __restrict__ s, const double* __restrict__ r,
                          double* __restrict__ p) {
+  if (s->done) return;
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   p[i] = fma(s->beta, p[i], r[i]);
@@ -196,38 +305,34 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
   const double pi = acos(-1.0);
   const HartreeCoefs hc = hartree_coefs(nfh, ddx, ddy, ddz);
   const unsigned gN = div_up(N, 256);
+  const double vol = 8.0 * xmax * ymax * zmax;
   int rc;
+  RS_CUDA(cudaMemsetAsync(sc, 0, sizeof(CgScalars), st));
   k_cg_bvec<<<gN, 256, 0, st>>>(N, rho, 2.0 * pi, ddx, ddy, ddz, b, r, p);
   if ((rc = tree_dot<double>(N, r, p, &sc->bve, part, st))) return rc;
-  const double vol = 8.0 * xmax * ymax * zmax;
   k_cg_neutral<<<gN, 256, 0, st>>>(N, b, &sc->bve, vol);
   RS_LAUNCH_CHECK("k_cg_neutral");
   if ((rc = launch_hartree_lap(nx, ny, nz, nfh, hc, vh, ap, st))) return rc;
   k_cg_init<<<gN, 256, 0, st>>>(N, b, ap, avhs, r, p);
-  int loop = 0;
-  double dp = 0.0;
+  if ((rc = tree_dot<double>(N, r, r, &sc->r1r, part, st))) return rc;
   CgScalars hs;
-  for (;;) {
-    ++loop;
-    if ((rc = launch_hartree_lap(nx, ny, nz, nfh, hc, p, ap, st))) return rc;
-    if ((rc = tree_dot<double>(N, r, r, &sc->r1r, part, st))) return rc;
-    if ((rc = tree_dot<double>(N, p, ap, &sc->pap, part, st))) return rc;
-    k_cg_alpha<<<1, 1, 0, st>>>(sc);
-    k_cg_update<<<gN, 256, 0, st>>>(N, sc, vh, p, ap, avhs, b, r);
-    if ((rc = tree_dot<double>(N, r, r, &sc->r2r, part, st))) return rc;
-    k_cg_beta<<<1, 1, 0, st>>>(sc, loop, ncgres, ddx, ddy, ddz, vol);
-    k_cg_dir<<<gN, 256, 0, st>>>(N, sc, r, p);
+  hs.done = 0;
+  const int lmax = ncgmax > ncgmin ? ncgmax : ncgmin;
+  for (int loop = 1; loop <= lmax && !hs.done; loop += kCgBatch) {
+    for (int l = loop; l < loop + kCgBatch && l <= lmax; ++l) {
+      k_cg_lap_pap<<<(unsigned)nblk, kTreeLanes, 0, st>>>(nx, ny, nz, nfh, hc, p, ap, part, sc);
+      k_cg_fold_alpha<<<1, kTreeLanes, 0, st>>>(nblk, part, sc);
+      k_cg_update_rr<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, vh, p, ap, avhs, b, r, part);
+      k_cg_fold_beta<<<1, kTreeLanes, 0, st>>>(nblk, part, sc, l, ncgres, ncgmin, ncgmax, epsvh,
+                                               ddx, ddy, ddz, vol);
+      k_cg_dir<<<gN, 256, 0, st>>>(N, sc, r, p);
+    }
     RS_LAUNCH_CHECK("hartree_cg iteration");
     RS_CUDA(cudaMemcpyAsync(&hs, sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
     RS_CUDA(cudaStreamSynchronize(st));
-    dp = hs.dp;
-    if (loop < ncgmin) continue;
-    if (loop >= ncgmax) break;
-    if (dp > epsvh) continue;
-    break;
   }
-  if (iters) *iters = loop;
-  if (dp_out) *dp_out = dp;
+  if (iters) *iters = hs.iters;
+  if (dp_out) *dp_out = hs.dp;
   return RS_OK;
 }
 

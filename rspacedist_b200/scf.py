@@ -18,8 +18,11 @@ Inputs the library does not build (they sit outside the ported hot path):
 the local pseudopotential and the starting charge are model fields given per
 atom (a Gaussian well and a normalised Gaussian of the valence charge), D and
 S stay at their dataset values (no PAW one-centre update), and occupations
-are fixed (2 for the lowest nocc bands).  Every step that kukan performs on
-these inputs runs on the GPU."""
+follow kukan's Fermi-Dirac smearing (scf_occupation, kT = 3e-3 Ha) for
+nelec = 2 nocc electrons, or are fixed at 2 for the lowest nocc bands with
+smearing=False (kukan's mpre /= 0).  Every grid step that kukan performs on
+these inputs runs on the GPU; the occupations (a bisection over M
+eigenvalues) are host logic."""
 from __future__ import annotations
 
 import time
@@ -77,6 +80,72 @@ def smooth_start_bands(shape, M: int, seed: int) -> np.ndarray:
     return x.reshape(M, -1)
 
 
+def fermidis(fwght: float, r: float, t: float, rc: float) -> float:
+    """mathfunctions8f.F90:21-36: fwght / (exp((r - rc)/t) + 1), clipped."""
+    acoef = (r - rc) / t
+    if abs(acoef) < 1.0e2:
+        fdis = 1.0 / (np.exp(acoef) + 1.0)
+    else:
+        fdis = 0.0 if acoef > 0.0 else 1.0
+    return fdis * fwght
+
+
+def scf_occupation(sval, tnumele: float, tf: float = 3.0e-3, tfmin: float = -3.0e2,
+                   tfmax: float = 3.0e2):
+    """scf_occupation_fnele (scf_occupation8f.F90:227-388), mpre = 0, one
+    k-point and spin: Fermi-Dirac occupations (weight 2) with the Fermi level
+    found by bisection between tfmin and tfmax (at most 100 halvings, stop
+    when the electron count is within 1e-12).  Returns (fnele, ferm)."""
+    fwght = 2.0
+    sval = np.asarray(sval, dtype=np.float64)
+
+    def count(ferm):
+        f = np.array([fermidis(fwght, e, tf, ferm) for e in sval])
+        s = 0.0
+        for v in f:
+            s = s + v
+        return f, s
+
+    ferm1, ferm3 = tfmax, tfmin
+    _, n1 = count(ferm1)
+    bisec1 = n1 - tnumele
+    _, n3 = count(ferm3)
+    bisec3 = n3 - tnumele
+    lbisec = 0
+    f, ferm = None, ferm1
+    while lbisec < 100:
+        lbisec += 1
+        ferm = (ferm1 + ferm3) * 0.5
+        f, n0 = count(ferm)
+        bisec = n0 - tnumele
+        if abs(bisec) < 1.0e-12:
+            lbisec = 100
+        if bisec1 * bisec > 0.0:
+            ferm1, bisec1 = ferm, bisec
+        if bisec * bisec3 > 0.0:
+            ferm3, bisec3 = ferm, bisec
+    return f, ferm
+
+
+def smooth_start_bands_device(shape, M: int, seed: int, dtype=torch.float64):
+    """The same kind of start as smooth_start_bands, generated on the device
+    (seeded normal bands, the same Gaussian low-pass filter), for large cells."""
+    nx, ny, nz = shape
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    kz, ky, kx = torch.meshgrid(torch.fft.fftfreq(nz, device="cuda"),
+                                torch.fft.fftfreq(ny, device="cuda"),
+                                torch.fft.fftfreq(nx, device="cuda"), indexing="ij")
+    filt = torch.exp(-(kx ** 2 + ky ** 2 + kz ** 2) / 0.005)
+    out = torch.empty((M, nx * ny * nz), dtype=dtype, device="cuda")
+    for b0 in range(0, M, 64):
+        x = torch.randn((min(64, M - b0), nz, ny, nx), generator=gen, device="cuda",
+                        dtype=torch.float64)
+        x = torch.fft.ifftn(torch.fft.fftn(x, dim=(1, 2, 3)) * filt, dim=(1, 2, 3)).real
+        out[b0:b0 + x.shape[0]] = x.reshape(x.shape[0], -1).to(dtype)
+    return out
+
+
 @dataclass
 class ScfResult:
     converged: bool
@@ -86,6 +155,7 @@ class ScfResult:
     seconds_per_iter: list = field(default_factory=list)
     sval: np.ndarray | None = None                 # eigenvalues (Ha), ascending
     eband: float = 0.0                             # sum_l f_l e_l (Ha)
+    fermi: float = 0.0                             # Fermi level (Ha), smearing only
     hartree_iters: list = field(default_factory=list)
     phase_seconds: dict = field(default_factory=dict)  # with profile=True only
 
@@ -93,7 +163,8 @@ class ScfResult:
 def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float = 1e-6,
             looplimit: int = 200, prm=None, nbrydn: int = 20, eta: float = 0.02,
             seed: int = 0, zval: float = 4.0, epsvh: float = 1e-12, vloc=None, rho0=None,
-            psi0=None, log=None, profile: bool = False) -> ScfResult:
+            psi0=None, log=None, profile: bool = False, smearing: bool = True,
+            tf: float = 3.0e-3) -> ScfResult:
     dev = torch.device("cuda")
     g = K.Geometry(cell)
     N, shape = cell.N, cell.shape
@@ -101,9 +172,12 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
     h, xmax = cell.h, cell.xmax
     dvol = h[0] * h[1] * h[2]
     f64 = torch.float64
-    psi = smooth_start_bands(shape, M, seed) if psi0 is None else psi0
+    if psi0 is None:
+        psi = smooth_start_bands_device(shape, M, seed, dtype)
+    else:
+        psi = torch.as_tensor(np.ascontiguousarray(psi0), device=dev).to(dtype)
     sss = None if cell.sss is None else torch.tensor(cell.sss, dtype=f64, device=dev)
-    b = K.Bands(g, torch.tensor(psi, dtype=dtype, device=dev), sss)
+    b = K.Bands(g, psi, sss)
     K.orthogonalization(b, 1)
     occ = torch.zeros(M, dtype=f64, device=dev)
     occ[:nocc] = 2.0
@@ -147,6 +221,9 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
         tp = mark("xc+transfer", tp)
         K.scf_diag(b, veff, dij, iscf, prm)
         tp = mark("scf_diag", tp)
+        if smearing:
+            fn, res.fermi = scf_occupation(b.sval, 2.0 * nocc, tf)
+            occ.copy_(torch.from_numpy(fn))
         rho_o = K.scf_charge_smt(occ, b.psi, N)
         diff = K.scf_diffcharge(rho_o, rho_i, h, xmax)
         tp = mark("charge", tp)

@@ -2,7 +2,8 @@
 infrastructure): same model inputs, same step order, FP64 throughout.  Per
 iteration: Broyden mixing, c2d, Hartree CG, PZ LDA, d2c, veff sum, then
 Rayleigh-Ritz + CG (iscf <= ncgscf) or Rayleigh-Ritz + DIIS, a stable
-ascending reorder, the density and the charge difference."""
+ascending reorder, the Fermi-Dirac occupations (the same host function as the
+GPU driver), the density and the charge difference."""
 import numpy as np
 
 
@@ -12,7 +13,7 @@ def geo_dict(cell):
 
 
 def oracle_scf(O, cell, M, nocc, eps_scf=1e-6, looplimit=100, nbrydn=20, eta=0.02, seed=0,
-               ncgscf=3, zval=4.0, epsvh=1e-12):
+               ncgscf=3, zval=4.0, epsvh=1e-12, smearing=True, tf=3.0e-3):
     from rspacedist_b200 import scf as SCF
     geo = geo_dict(cell)
     N, shape = cell.N, cell.shape
@@ -50,6 +51,8 @@ def oracle_scf(O, cell, M, nocc, eps_scf=1e-6, looplimit=100, nbrydn=20, eta=0.0
         psi, rp, sval = psi[order], rp[order], sval[order]
         if sp is not None:
             sp = sp[order]
+        if smearing:
+            occ = SCF.scf_occupation(sval, 2.0 * nocc, tf)[0]
         rho_o = O.density(occ, psi, N)
         diffs.append(O.diffcharge(rho_o, rho_i, h, xmax))
         if diffs[-1] < eps_scf:

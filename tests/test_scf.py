@@ -24,7 +24,8 @@ def test_scf_matches_oracle(ref, dtype, tol_e, tol_band):
     from rspacedist_b200 import lib, scf
     cell, r = ref
     assert r["converged"]
-    res = scf.run_scf(cell, 20, 16, dtype=dtype, prm=lib.solver_prm(ncgscf=3), looplimit=100)
+    res = scf.run_scf(cell, 20, 16, dtype=dtype, prm=lib.solver_prm(ncgscf=3), looplimit=100,
+                      psi0=scf.smooth_start_bands(cell.shape, 20, 0))
     assert res.converged, res.diff[-5:]
     np.testing.assert_allclose(np.sort(res.sval)[:16], r["sval"][:16], atol=tol_band)
     assert abs(res.eband - r["eband"]) / cell.natom < tol_e
