@@ -187,13 +187,19 @@ def run_gpu(args):
     e2e_s = (time.perf_counter() - e0) / e2e_steps
     e2e_bytes = algorithmic_bytes(cell, ne, g.entries)
     e2e_gbs = e2e_bytes / e2e_s / 1e9
+    h2d_bytes, d2h_bytes = int(hin.numel() * 4), int(hout.numel() * 4)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(cell, nb)
+    scf_out = None
+    if rank == 0 and world == 1 and args.scf_iters > 0:
+        del psi, hpsi, rp, hin, hout, rp_e
+        torch.cuda.empty_cache()
+        scf_out = run_scf_leg(cell, args.scf_iters)
     if rank == 0:
         out = {
-            "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi; SCF-time part of the metric not yet measured)",
+            "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi); SCF time per iteration in 'scf'",
             "value": round(value, 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -210,17 +216,61 @@ def run_gpu(args):
                          "traffic": None, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": nbytes},
             "e2e": {"value": round(e2e_gbs, 2), "unit": "GB/s",
-                    "h2d_bytes_per_step": int(hin.numel() * 4),
-                    "d2h_bytes_per_step": int(hout.numel() * 4),
+                    "h2d_bytes_per_step": h2d_bytes,
+                    "d2h_bytes_per_step": d2h_bytes,
                     "bands": ne, "entry_point": "rs_hpsi_host_f32"},
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": 3 * args.steps,
             "clocks": clk.summary(),
         }
         if cpu:
             out["cpu_baseline"] = cpu
+        if scf_out:
+            out["scf"] = scf_out
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_scf_leg(cell, iters):
+    """The SCF half of the metric on the same Si512 cell: `iters` SCF
+    iterations (Broyden mixing, potentials, scf_diag with RR + DIIS, density,
+    charge difference) on the mixed path (FP32 bands) and on the plain FP64
+    path, from the same start, timed per iteration on the wall clock with the
+    device synchronised.  The local potential and start charge are model
+    fields (a Gaussian well / valence Gaussian per atom); 1024 of 1100 bands
+    are filled by Fermi-Dirac occupation (kT = 3e-3 Ha)."""
+    import torch
+    from rspacedist_b200 import lib, scf
+    prm = lib.solver_prm(ncgscf=0)
+    res = {}
+    for name, dt in (("mixed", torch.float32), ("fp64", torch.float64)):
+        r = scf.run_scf(cell, NB, 1024, dtype=dt, prm=prm, looplimit=iters, eta=0.1,
+                        profile=True)
+        res[name] = r
+        torch.cuda.empty_cache()
+        log(f"[scf] {name}: {[round(s, 3) for s in r.seconds_per_iter]} s per iteration")
+    a, b = res["mixed"], res["fp64"]
+    steady = lambda r: statistics.mean(r.seconds_per_iter[1:] or r.seconds_per_iter)
+    nocc = 1024
+    return {
+        "workload": "Si512 model SCF: 128^3 grid, 1100 bands (1024 filled, Fermi-Dirac kT "
+                    "3e-3 Ha), Si PAW projectors with fixed D and S, Gaussian-well local "
+                    "potential, Broyden mixing (eta 0.1, 20 steps), RR + DIIS each iteration, "
+                    "Hartree CG (epsvh 1e-12, at most 800 iterations) on the 256^3 dense grid",
+        "iterations": iters,
+        "mixed_s_per_iter": round(steady(a), 3),
+        "fp64_s_per_iter": round(steady(b), 3),
+        "speedup_mixed_vs_fp64": round(steady(b) / steady(a), 3),
+        "mixed_phase_s": {k: round(v / iters, 3) for k, v in a.phase_seconds.items()},
+        "fp64_phase_s": {k: round(v / iters, 3) for k, v in b.phase_seconds.items()},
+        "diff_charge_mixed": [float(f"{d:.3e}") for d in a.diff],
+        "diff_charge_fp64": [float(f"{d:.3e}") for d in b.diff],
+        "max_abs_occupied_eig_diff_ha": float(np.abs(np.sort(a.sval)[:nocc]
+                                                     - np.sort(b.sval)[:nocc]).max()),
+        "eband_diff_ha_per_atom": abs(a.eband - b.eband) / cell.natom,
+        "timing": "wall clock per SCF iteration with device synchronisation; the first "
+                  "iteration (pool growth) is left out of the means",
+    }
 
 
 def cpu_baseline(cell, nb_full, nthreads=None, nbands=CPU_SAMPLE_BANDS):
@@ -267,7 +317,7 @@ def run_reference(args):
     cores = vals[0]["cores"]
     print(json.dumps({
         "impl": "reference",
-        "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi; SCF-time part of the metric not yet measured)",
+        "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi); SCF time per iteration in 'scf'",
         "value": round(v, 3), "unit": "GB/s", "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(sweep_s * 1e3, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -290,6 +340,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--bands", type=int, default=NB,
                     help="bands per sweep (default 1100; smaller values for profiling only)")
+    ap.add_argument("--scf-iters", type=int, default=3,
+                    help="SCF iterations timed per path on the Si512 cell (0 skips the leg)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -132,29 +132,37 @@ constexpr int kCgBatch = 16;
 
 __device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
-// -1/2 lap v at point p, in k_hartree_lap's order (x with the diagonal, y, z);
-// 32-bit index arithmetic (the grid has fewer than 2^31 points)
-__device__ __forceinline__ double hlap_at(int nx, int ny, int nz, int nf, const HartreeCoefs& c,
-                                          const double* __restrict__ v, int p) {
+// -1/2 lap v at (ix, iy, iz) = point p, in k_hartree_lap's order (x with the
+// diagonal, y, z), NF fixed at compile time
+template <int NF>
+__device__ __forceinline__ double hlap_at(int nx, int ny, int nz, const HartreeCoefs& c,
+                                          const double* __restrict__ v, int p, int ix, int iy,
+                                          int iz) {
   const int pl = nx * ny;
-  const int iz = p / pl, rem = p - iz * pl;
-  const int iy = rem / nx, ix = rem - iy * nx;
   const int row = p - ix;
   const int col = p - iz * pl;  // iy*nx + ix
-  double acc = c.cx[nf] * __ldg(v + row + wrap1(ix - nf, nx));
-  for (int m = nf - 1; m >= 1; --m) acc = fma(c.cx[m], __ldg(v + row + wrap1(ix - m, nx)), acc);
+  double acc = c.cx[NF] * __ldg(v + row + wrap1(ix - NF, nx));
+#pragma unroll
+  for (int m = NF - 1; m >= 1; --m) acc = fma(c.cx[m], __ldg(v + row + wrap1(ix - m, nx)), acc);
   acc = fma(c.diag, __ldg(v + p), acc);
-  for (int m = 1; m <= nf; ++m) acc = fma(c.cx[m], __ldg(v + row + wrap1(ix + m, nx)), acc);
+#pragma unroll
+  for (int m = 1; m <= NF; ++m) acc = fma(c.cx[m], __ldg(v + row + wrap1(ix + m, nx)), acc);
   const int zb = iz * pl + ix;
-  for (int m = nf; m >= 1; --m) acc = fma(c.cy[m], __ldg(v + zb + wrap1(iy - m, ny) * nx), acc);
-  for (int m = 1; m <= nf; ++m) acc = fma(c.cy[m], __ldg(v + zb + wrap1(iy + m, ny) * nx), acc);
-  for (int m = nf; m >= 1; --m) acc = fma(c.cz[m], __ldg(v + wrap1(iz - m, nz) * pl + col), acc);
-  for (int m = 1; m <= nf; ++m) acc = fma(c.cz[m], __ldg(v + wrap1(iz + m, nz) * pl + col), acc);
+#pragma unroll
+  for (int m = NF; m >= 1; --m) acc = fma(c.cy[m], __ldg(v + zb + wrap1(iy - m, ny) * nx), acc);
+#pragma unroll
+  for (int m = 1; m <= NF; ++m) acc = fma(c.cy[m], __ldg(v + zb + wrap1(iy + m, ny) * nx), acc);
+#pragma unroll
+  for (int m = NF; m >= 1; --m) acc = fma(c.cz[m], __ldg(v + wrap1(iz - m, nz) * pl + col), acc);
+#pragma unroll
+  for (int m = 1; m <= NF; ++m) acc = fma(c.cz[m], __ldg(v + wrap1(iz + m, nz) * pl + col), acc);
   return acc;
 }
 
-// ap = A p and the chunk sums of p.ap
-__global__ void __launch_bounds__(kTreeLanes) k_cg_lap_pap(int nx, int ny, int nz, int nf,
+// ap = A p and the chunk sums of p.ap.  A thread's 16 points are kTreeLanes
+// apart: their coordinates are stepped forward instead of divided out.
+template <int NF>
+__global__ void __launch_bounds__(kTreeLanes) k_cg_lap_pap(int nx, int ny, int nz,
                                                            HartreeCoefs c,
                                                            const double* __restrict__ p,
                                                            double* __restrict__ ap,
@@ -162,16 +170,27 @@ __global__ void __launch_bounds__(kTreeLanes) k_cg_lap_pap(int nx, int ny, int n
                                                            const CgScalars* __restrict__ s) {
   if (s->done) return;
   __shared__ double ws[8];
-  const long N = (long)nx * ny * nz;
-  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  const int N = nx * ny * nz;
+  const int base = blockIdx.x * kTreeChunk + threadIdx.x;
+  int iz = base / (nx * ny);
+  int rem = base - iz * nx * ny;
+  int iy = rem / nx, ix = rem - iy * nx;
   double acc = 0.0;
-#pragma unroll 4
+#pragma unroll 2
   for (int k = 0; k < kTreePerLane; ++k) {
-    const long i = base + (long)k * kTreeLanes;
+    const int i = base + k * kTreeLanes;
     if (i < N) {
-      const double a = hlap_at(nx, ny, nz, nf, c, p, (int)i);
+      const double a = hlap_at<NF>(nx, ny, nz, c, p, i, ix, iy, iz);
       ap[i] = a;
       acc = fma(p[i], a, acc);
+    }
+    ix += kTreeLanes;
+    while (ix >= nx) {
+      ix -= nx;
+      if (++iy == ny) {
+        iy = 0;
+        ++iz;
+      }
     }
   }
   const double t = tree_fold256(acc, ws);
@@ -315,12 +334,23 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
   if ((rc = launch_hartree_lap(nx, ny, nz, nfh, hc, vh, ap, st))) return rc;
   k_cg_init<<<gN, 256, 0, st>>>(N, b, ap, avhs, r, p);
   if ((rc = tree_dot<double>(N, r, r, &sc->r1r, part, st))) return rc;
+  auto lap = [&](const double* x, double* ax) {
+    const unsigned gb = (unsigned)nblk;
+    switch (nfh) {
+      case 1: k_cg_lap_pap<1><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
+      case 2: k_cg_lap_pap<2><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
+      case 3: k_cg_lap_pap<3><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
+      case 4: k_cg_lap_pap<4><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
+      case 5: k_cg_lap_pap<5><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
+      default: k_cg_lap_pap<6><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
+    }
+  };
   CgScalars hs;
   hs.done = 0;
   const int lmax = ncgmax > ncgmin ? ncgmax : ncgmin;
   for (int loop = 1; loop <= lmax && !hs.done; loop += kCgBatch) {
     for (int l = loop; l < loop + kCgBatch && l <= lmax; ++l) {
-      k_cg_lap_pap<<<(unsigned)nblk, kTreeLanes, 0, st>>>(nx, ny, nz, nfh, hc, p, ap, part, sc);
+      lap(p, ap);
       k_cg_fold_alpha<<<1, kTreeLanes, 0, st>>>(nblk, part, sc);
       k_cg_update_rr<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, vh, p, ap, avhs, b, r, part);
       k_cg_fold_beta<<<1, kTreeLanes, 0, st>>>(nblk, part, sc, l, ncgres, ncgmin, ncgmax, epsvh,
@@ -406,6 +436,8 @@ extern "C" int rs_hartree_cg(int nx, int ny, int nz, int nfh, double xmax, doubl
   if (nfh < 1 || nfh > 6 || nx <= 2 * nfh || ny <= 2 * nfh || nz <= 2 * nfh)
     return rs::fail(RS_EINVAL, "rs_hartree_cg: bad grid or nfh");
   if (ncgres <= 0 || ncgmax <= 0) return rs::fail(RS_EINVAL, "rs_hartree_cg: bad iteration limits");
+  if ((long)nx * ny * nz > 2147483647L)
+    return rs::fail(RS_EINVAL, "rs_hartree_cg: the dense grid must have fewer than 2^31 points");
   cudaStream_t st = rs::as_stream(stream);
   const long N = (long)nx * ny * nz;
   const long nblk = rs::tree_chunks(N);

@@ -10,9 +10,14 @@
 #include <vector>
 
 #include "reduce.cuh"
+#include <algorithm>
+
+#include <cooperative_groups.h>
+
 #include "rs_common.cuh"
 
 namespace rs {
+namespace cg = cooperative_groups;
 namespace {
 
 // pairs of round r of the circle method over ne (even) players
@@ -30,10 +35,8 @@ struct Rot {
 };
 
 // rotation angle zeroing a_pq (same formula as the CPU oracle's Jacobi)
-__global__ void k_jac_params(const double* __restrict__ A, int n, int ne, int r,
-                             Rot* __restrict__ rot) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ne / 2) return;
+__device__ __forceinline__ void jac_params(const double* __restrict__ A, int n, int ne, int r,
+                                           int t, Rot* __restrict__ rot) {
   int p, q;
   rr_pair(r, t, ne, &p, &q);
   Rot o{p, q, 1.0, 0.0};
@@ -52,9 +55,8 @@ __global__ void k_jac_params(const double* __restrict__ A, int n, int ne, int r,
 }
 
 // A <- J^T A J on every 2x2 block (P, Q) of the pairing, V <- V J
-__global__ void k_jac_apply(double* __restrict__ A, double* __restrict__ V, int n, int npair,
-                            const Rot* __restrict__ rot) {
-  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void jac_apply(double* __restrict__ A, double* __restrict__ V, int n,
+                                          int npair, const Rot* __restrict__ rot, long idx) {
   const long nblk = (long)npair * npair;
   if (idx < nblk) {
     const Rot P = rot[idx % npair], Q = rot[idx / npair];
@@ -91,6 +93,23 @@ __global__ void k_jac_apply(double* __restrict__ A, double* __restrict__ V, int 
     const double vp = V[(long)Q.p * n + i], vq = V[(long)Q.q * n + i];
     V[(long)Q.p * n + i] = Q.c * vp - Q.s * vq;
     V[(long)Q.q * n + i] = Q.s * vp + Q.c * vq;
+  }
+}
+
+// one cyclic sweep: ne-1 rounds of (rotation parameters, apply), separated by
+// grid-wide barriers of a cooperative launch (all blocks are co-resident)
+__global__ void k_jac_sweep(double* __restrict__ A, double* __restrict__ V, int n, int ne,
+                            Rot* __restrict__ rot) {
+  cg::grid_group grid = cg::this_grid();
+  const int npair = ne / 2;
+  const long nwork = (long)npair * npair + (long)npair * n;
+  const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (int r = 0; r < ne - 1; ++r) {
+    for (long t = tid; t < npair; t += stride) jac_params(A, n, ne, r, (int)t, rot);
+    grid.sync();
+    for (long idx = tid; idx < nwork; idx += stride) jac_apply(A, V, n, npair, rot, idx);
+    grid.sync();
   }
 }
 
@@ -136,59 +155,119 @@ __global__ void k_sort_eig(const double* __restrict__ A, const double* __restric
   for (int k = 0; k < n; ++k) Z[(long)rank * n + k] = sg * v[k];
 }
 
-// ---------------------------------------------------------------- Cholesky
-// In-place lower Cholesky of a symmetric positive definite n x n matrix
-// (column-major; only the lower triangle is referenced), one CTA.
-// info[0] = 0, or j+1 when the pivot of column j is not positive.
-__global__ void k_potrf(double* __restrict__ A, int n, int* __restrict__ info) {
+// ------------------------------------------------ blocked Cholesky, L L^T = A
+// A is column-major (element (i, k) at A[k*n + i]); the lower triangle is
+// overwritten by L.  Block steps of kCholB columns: the diagonal block is
+// factored by one CTA in shared memory, the panel below it by one thread per
+// row, and the trailing lower triangle is updated in 32 x 32 tiles.
+constexpr int kCholB = 64;
+
+__global__ void k_chol_diag(double* __restrict__ A, int n, int kb, int* __restrict__ info) {
+  __shared__ double a[kCholB][kCholB + 1];  // a[col][row]
   __shared__ double piv;
-  __shared__ int bad;
-  if (threadIdx.x == 0) bad = 0;
+  const int b = min(kCholB, n - kb);
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int c = e / b, r = e % b;
+    a[c][r] = A[(long)(kb + c) * n + kb + r];
+  }
   __syncthreads();
-  for (int k = 0; k < n; ++k) {
+  for (int k = 0; k < b; ++k) {
     if (threadIdx.x == 0) {
-      const double d = A[(long)k * n + k];
+      const double d = a[k][k];
       if (!(d > 0.0)) {
-        bad = k + 1;
+        if (info[0] == 0) info[0] = kb + k + 1;
         piv = 1.0;
       } else {
         piv = sqrt(d);
-        A[(long)k * n + k] = piv;
       }
+      a[k][k] = piv;
     }
     __syncthreads();
-    if (bad) break;
-    for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) A[(long)k * n + i] /= piv;
+    for (int i = k + 1 + threadIdx.x; i < b; i += blockDim.x) a[k][i] /= piv;
     __syncthreads();
-    // trailing update A[i][j] -= L[i][k] L[j][k], j in (k, i]
-    const long m = n - k - 1;
-    for (long e = threadIdx.x; e < m * m; e += blockDim.x) {
-      const int jj = (int)(e / m), ii = (int)(e % m);
+    const int m = b - k - 1;
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int jj = e / m, ii = e % m;
       if (ii < jj) continue;
-      const int i = k + 1 + ii, j = k + 1 + jj;
-      A[(long)j * n + i] = fma(-A[(long)k * n + i], A[(long)k * n + j], A[(long)j * n + i]);
+      const int i = k + 1 + ii, jc = k + 1 + jj;
+      a[jc][i] = fma(-a[k][i], a[k][jc], a[jc][i]);
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) info[0] = bad;
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int c = e / b, r = e % b;
+    if (r >= c) A[(long)(kb + c) * n + kb + r] = a[c][r];
+  }
 }
 
-// W = L^{-T} (upper triangular, column-major): column j of L^{-1} solved by
-// forward substitution, stored as row j of W.  One thread per column.
-__global__ void k_trinv_t(const double* __restrict__ L, int n, double* __restrict__ W) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  // x = L^{-1} e_j : x_i = 0 for i < j
-  for (int i = 0; i < n; ++i) {
-    double x = 0.0;
-    if (i >= j) {
-      double s = i == j ? 1.0 : 0.0;
-      for (int k = j; k < i; ++k) s = fma(-L[(long)k * n + i], W[(long)k * n + j], s);
-      x = s / L[(long)i * n + i];
-    }
-    // W(j, i) = x   (W = X^T, column-major W[i*n + j])
-    W[(long)i * n + j] = x;
+// rows i >= kb + b of the block column: L(i, kb:kb+b) = A(i, .) L_kk^{-T}
+__global__ void k_chol_panel(double* __restrict__ A, int n, int kb) {
+  __shared__ double l[kCholB][kCholB + 1];  // l[col][row] of L_kk
+  const int b = min(kCholB, n - kb);
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int c = e / b, r = e % b;
+    l[c][r] = A[(long)(kb + c) * n + kb + r];
   }
+  __syncthreads();
+  const int i = kb + b + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x[kCholB];
+  for (int c = 0; c < b; ++c) {
+    double v = A[(long)(kb + c) * n + i];
+    for (int k = 0; k < c; ++k) v = fma(-x[k], l[k][c], v);
+    x[c] = v / l[c][c];
+  }
+  for (int c = 0; c < b; ++c) A[(long)(kb + c) * n + i] = x[c];
+}
+
+// A(i, j) -= sum_{k in block} L(i, k) L(j, k) for kb + b <= j <= i
+__global__ void k_chol_trail(double* __restrict__ A, int n, int kb) {
+  const int b = min(kCholB, n - kb);
+  const int t0 = kb + b;
+  const int ti = blockIdx.y, tj = blockIdx.x;
+  if (tj > ti) return;
+  __shared__ double li[kCholB][33], lj[kCholB][33];  // [k][row within tile]
+  const int i0 = t0 + ti * 32, j0 = t0 + tj * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int k = ty; k < b; k += blockDim.y) {
+    const int ri = i0 + tx, rj = j0 + tx;
+    li[k][tx] = ri < n ? A[(long)(kb + k) * n + ri] : 0.0;
+    lj[k][tx] = rj < n ? A[(long)(kb + k) * n + rj] : 0.0;
+  }
+  __syncthreads();
+  const int i = i0 + ty, j = j0 + tx;
+  if (i >= n || j >= n || j > i) return;
+  double s = 0.0;
+  for (int k = 0; k < b; ++k) s = fma(li[k][ty], lj[k][tx], s);
+  A[(long)j * n + i] -= s;
+}
+
+// LT (row-major) = L: LT[i*n + k] = L(i, k) for k <= i
+__global__ void k_lower_rows(const double* __restrict__ A, int n, double* __restrict__ LT) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long)n * n) return;
+  const int i = (int)(e / n), k = (int)(e % n);
+  LT[e] = k <= i ? A[(long)k * n + i] : 0.0;
+}
+
+// W (column-major) = L^{-T}: column j of X = L^{-1} by forward substitution,
+// one warp per column, the sum of each step spread over the lanes; the
+// column lives in shared memory (n doubles per warp)
+__global__ void k_trinv_cols(const double* __restrict__ LT, int n, double* __restrict__ W) {
+  extern __shared__ double xs[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int j = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (j >= n) return;
+  double* x = xs + (long)wib * n;
+  for (int i = j; i < n; ++i) {
+    const double* row = LT + (long)i * n;
+    double s = 0.0;
+    for (int k = j + lane; k < i; k += 32) s = fma(row[k], x[k], s);
+    for (int off = 16; off >= 1; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (lane == 0) x[i] = ((i == j ? 1.0 : 0.0) - s) / row[i];
+    __syncwarp();
+  }
+  for (int i = lane; i < n; i += 32) W[(long)i * n + j] = i >= j ? x[i] : 0.0;
 }
 
 }  // namespace
@@ -208,7 +287,15 @@ int syev_jacobi(int n, double* A, double* w, double* Z, int max_sweeps, cudaStre
   RS_CUDA(cudaMallocAsync((void**)&od, sizeof(double) * 2, st));
   k_eye<<<div_up((long)n * n, 256), 256, 0, st>>>(V, n);
   int sweep = 0, rc = RS_OK;
+  // the cooperative grid: as many 256-thread blocks as are co-resident, at
+  // most one per 256 work items
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jac_sweep, 256, 0);
   const long nwork = (long)npair * npair + (long)npair * n;
+  const unsigned coop_grid = (unsigned)std::max(1L, std::min((long)nsm * std::max(per_sm, 1),
+                                                             (nwork + 255) / 256));
   for (; sweep < max_sweeps; ++sweep) {
     double h[2];
     k_offdiag<<<1, 256, 0, st>>>(A, n, od);
@@ -216,12 +303,12 @@ int syev_jacobi(int n, double* A, double* w, double* Z, int max_sweeps, cudaStre
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { rc = cuda_status(e, "syev_jacobi"); break; }
     if (h[0] == 0.0 || h[0] <= 1e-30 * h[1]) break;
-    for (int r = 0; r < ne - 1; ++r) {
-      k_jac_params<<<div_up(npair, 128), 128, 0, st>>>(A, n, ne, r, rot);
-      k_jac_apply<<<div_up(nwork, 256), 256, 0, st>>>(A, V, n, npair, rot);
+    {
+      int nn = n, nne = ne;
+      void* args[] = {&A, &V, &nn, &nne, &rot};
+      e = cudaLaunchCooperativeKernel((void*)k_jac_sweep, coop_grid, 256, args, 0, st);
     }
-    e = cudaGetLastError();
-    if (e != cudaSuccess) { rc = cuda_status(e, "k_jac_apply"); break; }
+    if (e != cudaSuccess) { rc = cuda_status(e, "k_jac_sweep"); break; }
   }
   if (rc == RS_OK && sweep >= max_sweeps) rc = fail(RS_ENUMERIC, "syev: Jacobi did not converge");
   if (rc == RS_OK) {
@@ -241,15 +328,36 @@ int syev_jacobi(int n, double* A, double* w, double* Z, int max_sweeps, cudaStre
 int chol_inv_t(int n, double* G, double* W, cudaStream_t st) {
   if (n <= 0) return RS_OK;
   int* info = nullptr;
+  double* LT = nullptr;
   RS_CUDA(cudaMallocAsync((void**)&info, sizeof(int), st));
-  k_potrf<<<1, 1024, 0, st>>>(G, n, info);
+  RS_CUDA(cudaMemsetAsync(info, 0, sizeof(int), st));
+  for (int kb = 0; kb < n; kb += kCholB) {
+    k_chol_diag<<<1, 256, 0, st>>>(G, n, kb, info);
+    const int rest = n - kb - kCholB;
+    if (rest > 0) {
+      k_chol_panel<<<div_up(rest, 64), 64, 0, st>>>(G, n, kb);
+      const unsigned nt = div_up(rest, 32);
+      k_chol_trail<<<dim3(nt, nt), dim3(32, 32), 0, st>>>(G, n, kb);
+    }
+  }
   int h = 0;
   RS_CUDA(cudaMemcpyAsync(&h, info, sizeof(int), cudaMemcpyDeviceToHost, st));
   RS_CUDA(cudaStreamSynchronize(st));
   cudaFreeAsync(info, st);
   if (h) return fail(RS_ENUMERIC, "Cholesky-QR: overlap matrix not positive definite (negative norm)");
-  k_trinv_t<<<div_up(n, 64), 64, 0, st>>>(G, n, W);
-  RS_LAUNCH_CHECK("k_trinv_t");
+  RS_CUDA(cudaMallocAsync((void**)&LT, sizeof(double) * (size_t)n * n, st));
+  k_lower_rows<<<div_up((long)n * n, 256), 256, 0, st>>>(G, n, LT);
+  const int wpb = (int)std::max(1L, std::min(8L, (96L * 1024) / ((long)n * 8)));
+  const size_t sm = sizeof(double) * (size_t)wpb * n;
+  cudaError_t e = cudaSuccess;
+  if (sm > 48 * 1024)
+    e = cudaFuncSetAttribute(k_trinv_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e == cudaSuccess) {
+    k_trinv_cols<<<div_up(n, wpb), 32 * wpb, sm, st>>>(LT, n, W);
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(LT, st);
+  if (e != cudaSuccess) return cuda_status(e, "k_trinv_cols");
   return RS_OK;
 }
 
