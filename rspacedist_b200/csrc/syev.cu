@@ -98,7 +98,8 @@ __device__ __forceinline__ void jac_apply(double* __restrict__ A, double* __rest
 
 // one cyclic sweep: ne-1 rounds of (rotation parameters, apply), separated by
 // grid-wide barriers of a cooperative launch (all blocks are co-resident)
-__global__ void k_jac_sweep(double* __restrict__ A, double* __restrict__ V, int n, int ne,
+constexpr int kJacThreads = 1024;
+__global__ void __launch_bounds__(kJacThreads) k_jac_sweep(double* __restrict__ A, double* __restrict__ V, int n, int ne,
                             Rot* __restrict__ rot) {
   cg::grid_group grid = cg::this_grid();
   const int npair = ne / 2;
@@ -113,13 +114,36 @@ __global__ void k_jac_sweep(double* __restrict__ A, double* __restrict__ V, int 
   }
 }
 
-__global__ void k_offdiag(const double* __restrict__ A, int n, double* __restrict__ out) {
+// sums of squares of the off-diagonal and of all elements: chunk sums of the
+// reduction tree (one 256-thread block per 4096 elements), then one fold
+__global__ void k_offdiag_part(const double* __restrict__ A, int n, double* __restrict__ part) {
+  __shared__ double ws[8];
+  const long nn = (long)n * n;
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  double off = 0.0, tot = 0.0;
+#pragma unroll
+  for (int k = 0; k < kTreePerLane; ++k) {
+    const long e = base + (long)k * kTreeLanes;
+    if (e < nn) {
+      const double a = A[e];
+      tot = fma(a, a, tot);
+      if (e / n != e % n) off = fma(a, a, off);
+    }
+  }
+  off = tree_fold256(off, ws);
+  tot = tree_fold256(tot, ws);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = off;
+    part[2 * blockIdx.x + 1] = tot;
+  }
+}
+
+__global__ void k_offdiag_fold(long nblk, const double* __restrict__ part, double* __restrict__ out) {
   __shared__ double ws[8];
   double off = 0.0, tot = 0.0;
-  for (long k = threadIdx.x; k < (long)n * n; k += blockDim.x) {
-    const double a = A[k];
-    tot = fma(a, a, tot);
-    if (k / n != k % n) off = fma(a, a, off);
+  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) {
+    off = off + part[2 * k];
+    tot = tot + part[2 * k + 1];
   }
   off = tree_fold256(off, ws);
   tot = tree_fold256(tot, ws);
@@ -284,21 +308,24 @@ int syev_jacobi(int n, double* A, double* w, double* Z, int max_sweeps, cudaStre
   double* od = nullptr;
   RS_CUDA(cudaMallocAsync((void**)&V, sizeof(double) * (size_t)n * n, st));
   RS_CUDA(cudaMallocAsync((void**)&rot, sizeof(Rot) * npair, st));
-  RS_CUDA(cudaMallocAsync((void**)&od, sizeof(double) * 2, st));
+  const long oblk = tree_chunks((long)n * n);
+  RS_CUDA(cudaMallocAsync((void**)&od, sizeof(double) * (2 + 2 * oblk), st));
   k_eye<<<div_up((long)n * n, 256), 256, 0, st>>>(V, n);
   int sweep = 0, rc = RS_OK;
-  // the cooperative grid: as many 256-thread blocks as are co-resident, at
-  // most one per 256 work items
+  // the cooperative grid: one 1024-thread block per SM (fewer blocks make
+  // the grid barrier cheaper), at most one block per 1024 work items
   int dev = 0, nsm = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jac_sweep, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jac_sweep, kJacThreads, 0);
   const long nwork = (long)npair * npair + (long)npair * n;
-  const unsigned coop_grid = (unsigned)std::max(1L, std::min((long)nsm * std::max(per_sm, 1),
-                                                             (nwork + 255) / 256));
+  const unsigned coop_grid = (unsigned)std::max(
+      1L, std::min((long)nsm * std::min(std::max(per_sm, 1), 1),
+                   (nwork + kJacThreads - 1) / kJacThreads));
   for (; sweep < max_sweeps; ++sweep) {
     double h[2];
-    k_offdiag<<<1, 256, 0, st>>>(A, n, od);
+    k_offdiag_part<<<(unsigned)oblk, kTreeLanes, 0, st>>>(A, n, od + 2);
+    k_offdiag_fold<<<1, kTreeLanes, 0, st>>>(oblk, od + 2, od);
     cudaError_t e = cudaMemcpyAsync(h, od, sizeof(h), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { rc = cuda_status(e, "syev_jacobi"); break; }
@@ -306,7 +333,7 @@ int syev_jacobi(int n, double* A, double* w, double* Z, int max_sweeps, cudaStre
     {
       int nn = n, nne = ne;
       void* args[] = {&A, &V, &nn, &nne, &rot};
-      e = cudaLaunchCooperativeKernel((void*)k_jac_sweep, coop_grid, 256, args, 0, st);
+      e = cudaLaunchCooperativeKernel((void*)k_jac_sweep, coop_grid, kJacThreads, args, 0, st);
     }
     if (e != cudaSuccess) { rc = cuda_status(e, "k_jac_sweep"); break; }
   }
