@@ -7,12 +7,14 @@
 // FP32 operands run on the 5th-generation tensor cores (tcgen05.mma,
 // kind::tf32) with the 3xTF32 split: x = hi + lo with hi = tf32(x) and lo = x -
 // hi, and A B ~ hi_A hi_B + hi_A lo_B + lo_A hi_B, accumulated in FP32 in
-// TMEM.  Operands are staged global -> registers -> shared memory (where the
-// split happens) in the 128-byte-swizzled canonical layouts; one thread issues
-// the MMAs and commits them to an mbarrier that frees the stage.  Gram
-// products split K into chunks whose FP32 partial tiles are summed in FP64 in
-// a fixed order.  FP64 operands use tiled FP64 kernels (CUDA cores).
+// TMEM.  The hi/lo pieces are packed once per call into operand blocks in
+// the canonical tcgen05 layouts; a warp-specialised pipeline (bulk-copy
+// producer, MMA issuer, drain warps) streams them through shared memory.
+// Gram products split K into chunks whose partial tiles are summed in FP64
+// in a fixed order.  FP64 operands use tiled FP64 kernels (CUDA cores).
 #include <math.h>
+
+#include <string>
 
 #include "rs_common.cuh"
 #include "tc_ptx.cuh"
@@ -25,56 +27,226 @@ using namespace tc;
 constexpr int GM = 128;        // tile rows (MMA M)
 constexpr int GN = 128;        // Gram tile cols (MMA N)
 constexpr int KB = 32;         // K per stage: one 128-byte swizzle row of fp32
-constexpr int TILE_BYTES = GM * KB * 4;  // 16 KB
 
 __device__ int g_tc_error;     // set when a bounded wait gives up
 
-// byte offset of (row r, 16-byte chunk c) in a K-major SW128 tile of 128-byte rows
-__device__ __forceinline__ uint32_t kmaj_off(int r, int c) {
-  return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4));
+// Operands are packed once per call into 32 KB blocks (hi 16 KB | lo 16 KB,
+// hi = tf32_rna(x), lo = x - hi, both exact in TF32) of 128 rows (MMA M or
+// N) by 32 K values, in the canonical tcgen05 shared-memory layouts, so a
+// pipeline stage is a plain bulk copy:
+//  * K-major (Gram A and B, rotation Z): row r at byte r*128 with its 16-byte
+//    chunk c stored at chunk c ^ (r mod 8) (SW128: 8-row atoms, SBO = 1 KB);
+//  * MN-major (rotation X, points contiguous): see mnmaj_off.
+
+// byte offset of (point p, band k) in the MN-major tile: each k-row holds 32
+// points (128 B) whose 32-byte chunks are XOR-swizzled with (k mod 4);
+// 4-row atoms (512 B) step along k (SBO = 512 B), 32-point blocks of 8
+// atoms (4 KB) step along the points (LBO = 4 KB)
+__device__ __forceinline__ uint32_t mnmaj_off(int p, int k) {
+  return (uint32_t)((p >> 5) * 4096 + (k >> 2) * 512 + (k & 3) * 128 +
+                    ((((p & 31) >> 3) ^ (k & 3)) << 5) + (p & 7) * 4);
+}
+// byte offset of (row r, K index k) in the K-major SW128 tile
+__device__ __forceinline__ uint32_t kmaj_off(int r, int k) {
+  return (uint32_t)(r * 128 + ((((k >> 2) ^ (r & 7))) << 4) + (k & 3) * 4);
 }
 
-__device__ __forceinline__ void split_store(char* hi_base, char* lo_base, uint32_t off,
-                                            float4 v) {
-  float4 h, l;
-  h.x = tf32_rna(v.x); l.x = v.x - h.x;
-  h.y = tf32_rna(v.y); l.y = v.y - h.y;
-  h.z = tf32_rna(v.z); l.z = v.z - h.z;
-  h.w = tf32_rna(v.w); l.w = v.w - h.w;
-  *reinterpret_cast<float4*>(hi_base + off) = h;
-  *reinterpret_cast<float4*>(lo_base + off) = l;
+// ------------------------------------------------------------------ pipeline
+// Both tensor-core kernels run the same warp-specialised pipeline:
+//  * warp 0 (one lane): producer -- keeps STAGES operand stages in flight
+//    (bulk copies into shared memory, completion counted in bytes);
+//  * warp 1 (one lane): issues the 12 MMAs of a stage (4 K-steps x 3 passes)
+//    into one of TM_BUFS TMEM accumulators, DGRP stages per accumulator, and
+//    commits them to the mbarriers that free the stage and hand the
+//    accumulator to the drain warps;
+//  * warps 2..: drain finished accumulators into registers (warp w reads
+//    TMEM lanes 32*(w%4).. and a share of the 128 columns: a half in the
+//    rotation, a quarter in the Gram, whose sums are (hi, lo) pairs) and
+//    write the results.
+// Every wait is bounded; a timeout raises a shared abort flag that winds all
+// roles down, and the host sees g_tc_error.
+constexpr int STAGES = 3;
+constexpr int TM_BUFS = 4;
+constexpr int DGRP = 2;
+constexpr int NDRAIN = 256;                  // rotation: 8 drain warps, 64 columns each
+constexpr int TC_THREADS = 64 + NDRAIN;
+constexpr int GRAM_DRAIN = 512;              // Gram: 16 drain warps, 32 columns each
+constexpr int GRAM_THREADS = 64 + GRAM_DRAIN;
+constexpr int OPB = GM * KB * 4;      // one 128 x 32 FP32 operand tile: 16 KB
+constexpr int STAGE_BYTES = 4 * OPB;  // a hi | a lo | b hi | b lo
+constexpr size_t TC_SMEM = (size_t)STAGES * STAGE_BYTES + 1024;
+
+struct PipeBars {
+  uint64_t full[STAGES], empty[STAGES], tfull[TM_BUFS], tempty[TM_BUFS];
+};
+
+__device__ __forceinline__ void pipe_init(PipeBars& b, int ndrain) {
+  for (int s = 0; s < STAGES; ++s) {
+    mbar_init(&b.full[s], 1);
+    mbar_init(&b.empty[s], 1);
+  }
+  for (int t = 0; t < TM_BUFS; ++t) {
+    mbar_init(&b.tfull[t], 1);
+    mbar_init(&b.tempty[t], ndrain);
+  }
 }
+
+// untiled bulk copy global -> this CTA's shared memory (16-byte aligned, size
+// a multiple of 16), completion counted on *bar
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+      ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// The MMA role for one stage: 3xTF32 over K = 32 into accumulator d.
+// a_mn / b_mn select the MN-major layout for the operand (descriptor type 1,
+// LBO 4 KB, SBO 512 B, K-steps 1 KB apart) instead of K-major SW128.
+template <bool A_MN>
+__device__ __forceinline__ void issue_stage(uint32_t d, uint32_t ahi, uint32_t alo, uint32_t bhi,
+                                            uint32_t blo, uint32_t idesc, bool first) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint64_t dah, dal;
+    if (A_MN) {
+      dah = smem_desc_sw128_b32(ahi + q * 1024, 4096, 512);
+      dal = smem_desc_sw128_b32(alo + q * 1024, 4096, 512);
+    } else {
+      dah = smem_desc_sw128(ahi + q * 32, 16, 1024);
+      dal = smem_desc_sw128(alo + q * 32, 16, 1024);
+    }
+    const uint64_t dbh = smem_desc_sw128(bhi + q * 32, 16, 1024);
+    const uint64_t dbl = smem_desc_sw128(blo + q * 32, 16, 1024);
+    mma_tf32(d, dal, dbh, idesc, (first && q == 0) ? 0u : 1u);
+    mma_tf32(d, dah, dbl, idesc, 1);
+    mma_tf32(d, dah, dbh, idesc, 1);
+  }
+}
+
+// ------------------------------------------------------------------ operand pieces
+// Rows of K values (stride ld) -> 32 KB blocks [row tile][k block] of hi | lo
+// in the K-major layout (row = band), for the K range [k0, k0 + nkb*32) cut
+// at K, zero beyond `rows` and K.  One CTA per block, 256 threads, 4 float4
+// each: 8 threads read one 128-byte row piece.
+__global__ void __launch_bounds__(256) k_tile_rows(const float* __restrict__ x, long ld, int rows,
+                                                   long k0, long K, int nkb,
+                                                   char* __restrict__ out) {
+  const long blk = blockIdx.x;
+  const int rt = (int)(blk / nkb), kb = (int)(blk % nkb);
+  char* hi = out + blk * (2 * OPB);
+  char* lo = hi + OPB;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int f = threadIdx.x + 256 * i;
+    const int r = f >> 3, c4 = f & 7;
+    const int row = rt * GM + r;
+    const long k = k0 + (long)kb * KB + 4 * c4;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (row < rows && k < K) v = __ldg(reinterpret_cast<const float4*>(x + (long)row * ld + k));
+    float4 h, l;
+    h.x = tf32_rna(v.x); l.x = v.x - h.x;
+    h.y = tf32_rna(v.y); l.y = v.y - h.y;
+    h.z = tf32_rna(v.z); l.z = v.z - h.z;
+    h.w = tf32_rna(v.w); l.w = v.w - h.w;
+    const uint32_t off = kmaj_off(r, 4 * c4);
+    *reinterpret_cast<float4*>(hi + off) = h;
+    *reinterpret_cast<float4*>(lo + off) = l;
+  }
+}
+
+// X (kin rows of npts points, stride ldx) -> 32 KB blocks [point tile][k block]
+// of hi | lo in the MN-major layout, zero beyond kin and npts.  One CTA per
+// block, 256 threads, 4 float4 each.
+__global__ void __launch_bounds__(256) k_tile_x(const float* __restrict__ X, long ldx, long npts,
+                                                int kin, int nkb, char* __restrict__ xt) {
+  const long blk = blockIdx.x;
+  const long pt = blk / nkb;
+  const int kb = (int)(blk % nkb);
+  char* hi = xt + blk * (2 * OPB);
+  char* lo = hi + OPB;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int f = threadIdx.x + 256 * i;  // k = f / 32, points 4 (f % 32) ..
+    const int kk = f >> 5, p4 = 4 * (f & 31);
+    const int k = kb * KB + kk;
+    const long p = pt * GM + p4;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (k < kin && p < npts) v = __ldg(reinterpret_cast<const float4*>(X + (long)k * ldx + p));
+    float4 h, l;
+    h.x = tf32_rna(v.x); l.x = v.x - h.x;
+    h.y = tf32_rna(v.y); l.y = v.y - h.y;
+    h.z = tf32_rna(v.z); l.z = v.z - h.z;
+    h.w = tf32_rna(v.w); l.w = v.w - h.w;
+    const uint32_t off = mnmaj_off(p4, kk);
+    *reinterpret_cast<float4*>(hi + off) = h;
+    *reinterpret_cast<float4*>(lo + off) = l;
+  }
+}
+
+// Z (FP64, column-major kin x nout) -> 32 KB blocks [band tile][k block] of
+// hi | lo in the K-major layout (row = output band j), zero beyond kin, nout.
+__global__ void __launch_bounds__(256) k_tile_z(const double* __restrict__ Z, long ldz, int kin,
+                                                int nout, int nkb, char* __restrict__ zt) {
+  const long blk = blockIdx.x;
+  const int jt = (int)(blk / nkb), kb = (int)(blk % nkb);
+  char* hi = zt + blk * (2 * OPB);
+  char* lo = hi + OPB;
+  for (int e = threadIdx.x; e < GM * KB; e += 256) {
+    const int kk = e % KB, jj = e / KB;
+    const int k = kb * KB + kk, j = jt * GM + jj;
+    const float z = (k < kin && j < nout) ? (float)Z[(long)j * ldz + k] : 0.f;
+    const float h = tf32_rna(z);
+    const uint32_t off = kmaj_off(jj, kk);
+    *reinterpret_cast<float*>(hi + off) = h;
+    *reinterpret_cast<float*>(lo + off) = z - h;
+  }
+}
+
 
 // ------------------------------------------------------------------ Gram
 // FP64 partial tiles P[pair][split][j][i] = sum_{k in chunk} A[i][k] B[j][k]
-// for one 128 x 128 tile pair and one K chunk.  The tensor core accumulates
-// at most DG stages (DG*32 terms, 3 MMA passes) in FP32 in one of two TMEM
-// buffers; each finished buffer is drained into FP64 registers while the
-// other one fills, so long sums never build up in FP32.
-constexpr int GRAM_THREADS = 256;
-constexpr int DG = 2;
-
-__device__ __forceinline__ void drain_f64(uint32_t taddr, double* acc) {
-  uint32_t r[32];
-  tmem_ld32(taddr, r);
-  tmem_ld_wait();
+// for one 128 x 128 tile pair and one K chunk.  The product runs over K in
+// pieces: each piece of A and B is first packed into hi | lo blocks
+// (k_tile_rows), so a stage is two 32 KB bulk copies of contiguous memory.
+// The tensor core accumulates DGRP stages (64 K terms, 3 passes) in FP32 in
+// one TMEM accumulator; the drain warps fold each finished accumulator into
+// compensated (hi, lo) FP32 register pairs while the next ones fill, so long
+// sums never build up in plain FP32.  A diagonal pair of a symmetric product
+// loads its block once.
+// Compensated FP32 accumulation: (hi, lo) += x with TwoSum (Knuth), so that
+// hi + lo carries the running sum to about 44 bits without FP64 conversions
+// in the loop (the library is built without contraction, so the six
+// additions run exactly as written).
+__device__ __forceinline__ void two_sum_acc(float& hi, float& lo, float x) {
+  const float s = hi + x;
+  const float bp = s - hi;
+  const float ap = s - bp;
+  lo += (hi - ap) + (x - bp);
+  hi = s;
+}
+__device__ __forceinline__ void drain_f64(uint32_t taddr, float* hi, float* lo) {
 #pragma unroll
-  for (int k = 0; k < 32; ++k) acc[k] += (double)__uint_as_float(r[k]);
-  tmem_ld32(taddr + 32, r);
-  tmem_ld_wait();
+  for (int c = 0; c < 32; c += 16) {
+    uint32_t r[16];
+    tmem_ld16(taddr + c, r);
+    tmem_ld_wait();
 #pragma unroll
-  for (int k = 0; k < 32; ++k) acc[32 + k] += (double)__uint_as_float(r[k]);
+    for (int k = 0; k < 16; ++k) two_sum_acc(hi[c + k], lo[c + k], __uint_as_float(r[k]));
+  }
 }
 
+// grid (pairs, splits of this piece); the CTA's partial goes to split column
+// split0 + blockIdx.y of nsplit_total
 __global__ void __launch_bounds__(GRAM_THREADS, 1)
-    k_gram_tf32x3(const float* __restrict__ A, long lda, int m, const float* __restrict__ B,
-                  long ldb, int n, long K, long kchunk, int sym, int tn,
-                  double* __restrict__ part) {
+    k_gram_tf32x3(const char* __restrict__ at, const char* __restrict__ bt, int nkb, int kbc,
+                  int sym, int tn, int split0, int nsplit_total, double* __restrict__ part) {
   extern __shared__ __align__(1024) char smem_dyn[];
   char* smem = (char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
-  // stage s: A hi | A lo | B hi | B lo
-  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) PipeBars bar;
   __shared__ uint32_t tmem_base;
+  __shared__ volatile int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5;
   int it, jt;
   {
@@ -89,103 +261,106 @@ __global__ void __launch_bounds__(GRAM_THREADS, 1)
       jt = pr / tn;
     }
   }
-  const long k0 = (long)blockIdx.y * kchunk;
-  const long k1 = min(K, k0 + kchunk);
-  const int nkb = (int)((k1 - k0 + KB - 1) / KB);
+  const bool same = sym && it == jt;
+  const int kb0 = blockIdx.y * kbc;
+  const int nst = max(0, min(nkb, kb0 + kbc) - kb0);
+  const int ngrp = (nst + DGRP - 1) / DGRP;
+  const char* ablk = at + ((long)it * nkb + kb0) * (2L * OPB);
+  const char* bblk = bt + ((long)jt * nkb + kb0) * (2L * OPB);
 
-  if (warp == 0) tmem_alloc(&tmem_base, 2 * GN);
+  if (warp == 2) tmem_alloc(&tmem_base, TM_BUFS * GN);
   if (tid == 0) {
-    mbar_init(&mbar[0], 1);
-    mbar_init(&mbar[1], 1);
+    pipe_init(bar, GRAM_DRAIN);
+    abort_flag = 0;
     fence_mbar_init();
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) tmem_relinquish();
+  if (warp == 2) tmem_relinquish();
   const uint32_t tmem = tmem_base;
-  constexpr uint32_t idesc = idesc_tf32(GM, GN, 0, 0);
-  // drain role: lane quadrant q (TMEM lanes 32q..), column half h
-  const int dq = warp & 3, dh = warp >> 2;
-  const uint32_t dlane = (uint32_t)(dq * 32) << 16;
-  double acc[64];
-#pragma unroll
-  for (int k = 0; k < 64; ++k) acc[k] = 0.0;
-
-  const int lc = tid & 7;
-  const int lr = tid >> 3;  // 0..31
   bool bad = false;
-  for (int kb = 0; kb < nkb; ++kb) {
-    const int s = kb & 1;
-    const int g = kb / DG;
-    const long kk0 = k0 + (long)kb * KB + 4 * lc;
-    float4 va[4], vb[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int r = lr + 32 * i;
-      const int ra = it * GM + r, rb = jt * GN + r;
-      const bool kin = kk0 < k1;
-      va[i] = (ra < m && kin) ? __ldg(reinterpret_cast<const float4*>(A + (long)ra * lda + kk0))
-                              : make_float4(0.f, 0.f, 0.f, 0.f);
-      vb[i] = (rb < n && kin) ? __ldg(reinterpret_cast<const float4*>(B + (long)rb * ldb + kk0))
-                              : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    if (kb >= 2) {
-      const bool ok = mbar_wait(&mbar[s], ((kb - 2) >> 1) & 1);
-      if (__syncthreads_or(!ok)) { bad = true; break; }
-    }
-    if (kb % DG == 0 && g >= 2) {
-      // group g-2 (same TMEM buffer) has completed: fold it into FP64
-      tc_fence_after();
-      drain_f64(tmem + (g & 1) * GN + dh * 64 + dlane, acc);
-      tc_fence_before();
-    }
-    char* st = smem + s * 4 * TILE_BYTES;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const uint32_t off = kmaj_off(lr + 32 * i, lc);
-      split_store(st, st + TILE_BYTES, off, va[i]);
-      split_store(st + 2 * TILE_BYTES, st + 3 * TILE_BYTES, off, vb[i]);
-    }
-    fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      const uint32_t d = tmem + (g & 1) * GN;
-      const uint32_t sa = smem_u32(st);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {  // K = 8 per instruction, 32 bytes
-        const uint64_t ahi = smem_desc_sw128(sa + q * 32, 16, 1024);
-        const uint64_t alo = smem_desc_sw128(sa + TILE_BYTES + q * 32, 16, 1024);
-        const uint64_t bhi = smem_desc_sw128(sa + 2 * TILE_BYTES + q * 32, 16, 1024);
-        const uint64_t blo = smem_desc_sw128(sa + 3 * TILE_BYTES + q * 32, 16, 1024);
-        mma_tf32(d, alo, bhi, idesc, ((kb % DG) | q) != 0);
-        mma_tf32(d, ahi, blo, idesc, 1);
-        mma_tf32(d, ahi, bhi, idesc, 1);
+
+  if (warp == 0) {
+    // ---------------------------------------------------------- producer
+    if ((tid & 31) == 0 && nst > 0) {
+      const uint32_t tx = same ? 2 * OPB : 4 * OPB;
+      int kb = 0;
+      for (; kb < nst; ++kb) {
+        const int s = kb % STAGES;
+        if (kb >= STAGES &&
+            !mbar_wait_or_abort(&bar.empty[s], (kb / STAGES - 1) & 1, &abort_flag)) {
+          bad = true;
+          break;
+        }
+        char* st = smem + s * STAGE_BYTES;
+        mbar_arrive_expect_tx(&bar.full[s], tx);
+        bulk_load(st, ablk + (long)kb * (2 * OPB), 2 * OPB, &bar.full[s]);
+        if (!same) bulk_load(st + 2 * OPB, bblk + (long)kb * (2 * OPB), 2 * OPB, &bar.full[s]);
       }
-      mma_commit(&mbar[s]);
+      // nothing may still write this CTA's shared memory when it exits
+      for (int j = max(0, kb - STAGES); j < kb; ++j)
+        if (!mbar_wait(&bar.full[j % STAGES], (j / STAGES) & 1)) bad = true;
+      if (bad) abort_flag = 1;
     }
-  }
-  if (!bad && nkb > 0) {
-    const int s = (nkb - 1) & 1;
-    const bool ok = mbar_wait(&mbar[s], ((nkb - 1) >> 1) & 1);
-    bad = __syncthreads_or(!ok);
-  }
-  tc_fence_after();
-  if (bad) {
-    if (tid == 0) atomicExch(&g_tc_error, 1);
+  } else if (warp == 1) {
+    // ---------------------------------------------------------- MMA issue
+    if ((tid & 31) == 0 && nst > 0) {
+      constexpr uint32_t idesc = idesc_tf32(GM, GN, 0, 0);
+      int kb = 0;
+      for (; kb < nst; ++kb) {
+        const int s = kb % STAGES, g = kb / DGRP, tb = g % TM_BUFS;
+        if (kb % DGRP == 0 && g >= TM_BUFS &&
+            !mbar_wait_or_abort(&bar.tempty[tb], (g / TM_BUFS - 1) & 1, &abort_flag)) {
+          bad = true;
+          break;
+        }
+        if (!mbar_wait_or_abort(&bar.full[s], (kb / STAGES) & 1, &abort_flag)) {
+          bad = true;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+        const uint32_t sb = same ? sa : sa + 2 * OPB;
+        issue_stage<false>(tmem + tb * GN, sa, sa + OPB, sb, sb + OPB, idesc, kb % DGRP == 0);
+        mma_commit(&bar.empty[s]);
+        if (kb % DGRP == DGRP - 1 || kb == nst - 1) mma_commit(&bar.tfull[tb]);
+      }
+      // no MMA may still run when the CTA exits
+      if (kb > 0 && !mbar_wait(&bar.empty[(kb - 1) % STAGES], ((kb - 1) / STAGES) & 1))
+        bad = true;
+      if (bad) abort_flag = 1;
+    }
   } else {
-    const int glast = (nkb - 1) / DG;
-    if (nkb > 0 && glast >= 1) drain_f64(tmem + ((glast - 1) & 1) * GN + dh * 64 + dlane, acc);
-    if (nkb > 0) drain_f64(tmem + (glast & 1) * GN + dh * 64 + dlane, acc);
-    double* P = part + ((long)blockIdx.x * gridDim.y + blockIdx.y) * GM * GN;
-    const int row = dq * 32 + (tid & 31);
+    // ---------------------------------------------------------- drain
+    const int dq = warp & 3, dc = (warp - 2) >> 2;  // lane quadrant, column quarter
+    const uint32_t dlane = (uint32_t)(dq * 32) << 16;
+    float ahi[32], alo[32];
 #pragma unroll
-    for (int k = 0; k < 64; ++k) P[(long)(dh * 64 + k) * GM + row] = acc[k];
+    for (int k = 0; k < 32; ++k) ahi[k] = alo[k] = 0.f;
+    for (int g = 0; g < ngrp; ++g) {
+      const int tb = g % TM_BUFS;
+      const bool ok = mbar_wait_or_abort(&bar.tfull[tb], (g / TM_BUFS) & 1, &abort_flag);
+      if (__any_sync(0xffffffffu, !ok)) { bad = true; break; }
+      tc_fence_after();
+      drain_f64(tmem + tb * GN + dc * 32 + dlane, ahi, alo);
+      tc_fence_before();
+      mbar_arrive(&bar.tempty[tb]);
+    }
+    if (!bad) {
+      double* P = part + ((long)blockIdx.x * nsplit_total + split0 + blockIdx.y) * GM * GN;
+      const int row = dq * 32 + (tid & 31);
+#pragma unroll
+      for (int k = 0; k < 32; ++k)
+        P[(long)(dc * 32 + k) * GM + row] = (double)ahi[k] + (double)alo[k];
+    }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, 2 * GN);
+  if (bad || abort_flag) {
+    if (tid == 64) atomicExch(&g_tc_error, 1);
+  }
+  if (warp == 2) tmem_dealloc(tmem, TM_BUFS * GN);
 }
 
 // C[i + j*ldc] = alpha * sum over splits (fixed order) of the FP64 partials;
@@ -206,170 +381,140 @@ __global__ void k_gram_reduce(const double* __restrict__ part, int nsplit, int m
 }
 
 // ------------------------------------------------------------------ rotation
-// Y[j][p] = sum_k X[k][p] Z(k, j) for a 128-point x RN-band tile.  A = X is
-// MN-major (points contiguous), B = Z^T is K-major (Zhi/Zlo given as [j][k]).
-// TMEM accumulates DR stages per buffer; drained sums add up in FP32
-// registers.
-constexpr int RN = 128;         // output bands per tile (MMA N)
-constexpr int DR = 2;
-constexpr int ROT_THREADS = 256;
-constexpr int ROT_A_BYTES = GM * KB * 4;   // 16 KB
-constexpr int ROT_B_BYTES = RN * KB * 4;   // 16 KB
-constexpr int ROT_STAGE = 2 * ROT_A_BYTES + 2 * ROT_B_BYTES;  // 64 KB
-
-// byte offset of (point p, band k) in the MN-major tile: each k-row holds 32
-// points (128 B) whose 32-byte chunks are XOR-swizzled with (k mod 4);
-// 4-row atoms (512 B) step along k (SBO = 512 B), 32-point blocks of 8
-// atoms (4 KB) step along the points (LBO = 4 KB)
-__device__ __forceinline__ uint32_t mnmaj_off(int p, int k) {
-  return (uint32_t)((p >> 5) * 4096 + (k >> 2) * 512 + (k & 3) * 128 +
-                    ((((p & 31) >> 3) ^ (k & 3)) << 5) + (p & 7) * 4);
-}
-
+// Y[j][p] = sum_k X[k][p] Z(k, j), output tiles of 128 points x 128 bands.
+// X and Z arrive pre-split and pre-tiled (k_tile_x, k_tile_z), so a stage is
+// two 32 KB bulk copies: X hi | lo (MN-major) and Z hi | lo (K-major).  Each
+// CTA walks tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (band tile
+// fastest, so the CTAs that share an X block run together and read it from
+// HBM once); the producer and the MMA warp run ahead into the next tile
+// while the drain warps finish the last one.  Drained sums add up in FP32.
 __device__ __forceinline__ void drain_f32(uint32_t taddr, float* acc) {
-  uint32_t r[32];
-  tmem_ld32(taddr, r);
-  tmem_ld_wait();
 #pragma unroll
-  for (int k = 0; k < 32; ++k) acc[k] += __uint_as_float(r[k]);
-  tmem_ld32(taddr + 32, r);
-  tmem_ld_wait();
+  for (int c = 0; c < 64; c += 16) {
+    uint32_t r[16];
+    tmem_ld16(taddr + c, r);
+    tmem_ld_wait();
 #pragma unroll
-  for (int k = 0; k < 32; ++k) acc[32 + k] += __uint_as_float(r[k]);
+    for (int k = 0; k < 16; ++k) acc[c + k] += __uint_as_float(r[k]);
+  }
 }
 
-__global__ void __launch_bounds__(ROT_THREADS, 1)
-    k_rotate_tf32x3(const float* __restrict__ X, long ldx, long npts, int kin,
-                    const float* __restrict__ Zhi, const float* __restrict__ Zlo, int kpad,
-                    int nout, float* __restrict__ Y, long ldy) {
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_rotate_tf32x3(const char* __restrict__ xt, const char* __restrict__ zt, long npts, int nkb,
+                    int nout, long ntiles, float* __restrict__ Y, long ldy) {
   extern __shared__ __align__(1024) char smem_dyn[];
   char* smem = (char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) PipeBars bar;
   __shared__ uint32_t tmem_base;
+  __shared__ volatile int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5;
-  const long p0 = (long)blockIdx.x * GM;
-  const int j0 = blockIdx.y * RN;
-  const int nkb = (kin + KB - 1) / KB;
-  if (warp == 0) tmem_alloc(&tmem_base, 2 * RN);
+  const int ntn = (nout + GN - 1) / GN;
+  const int ngrp = (nkb + DGRP - 1) / DGRP;
+  const long mytiles = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+
+  if (warp == 2) tmem_alloc(&tmem_base, TM_BUFS * GN);
   if (tid == 0) {
-    mbar_init(&mbar[0], 1);
-    mbar_init(&mbar[1], 1);
+    pipe_init(bar, NDRAIN);
+    abort_flag = 0;
     fence_mbar_init();
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) tmem_relinquish();
+  if (warp == 2) tmem_relinquish();
   const uint32_t tmem = tmem_base;
-  constexpr uint32_t idesc = idesc_tf32(GM, RN, 1, 0);
-  const int dq = warp & 3, dh = warp >> 2;
-  const uint32_t dlane = (uint32_t)(dq * 32) << 16;
-  float acc[64];
-#pragma unroll
-  for (int k = 0; k < 64; ++k) acc[k] = 0.f;
-  // X loader: 32 k-rows x 32 float4 -> 4 per thread; Z loader: 128 j x 8 chunks -> 4 per thread
-  const int xc = tid & 31, xr = tid >> 5;  // xr 0..7
-  const int zc = tid & 7, zr = tid >> 3;   // zr 0..31
   bool bad = false;
-  for (int kb = 0; kb < nkb; ++kb) {
-    const int s = kb & 1;
-    const int g = kb / DR;
-    float4 vx[4], vzh[4], vzl[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int k = kb * KB + xr + 8 * i;
-      const long p = p0 + 4 * xc;
-      vx[i] = (k < kin && p < npts)
-                  ? __ldg(reinterpret_cast<const float4*>(X + (long)k * ldx + p))
-                  : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int j = j0 + zr + 32 * i;
-      const long o = (long)j * kpad + kb * KB + 4 * zc;
-      const bool in = j < nout;
-      vzh[i] = in ? __ldg(reinterpret_cast<const float4*>(Zhi + o)) : make_float4(0.f, 0.f, 0.f, 0.f);
-      vzl[i] = in ? __ldg(reinterpret_cast<const float4*>(Zlo + o)) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    if (kb >= 2) {
-      const bool ok = mbar_wait(&mbar[s], ((kb - 2) >> 1) & 1);
-      if (__syncthreads_or(!ok)) { bad = true; break; }
-    }
-    if (kb % DR == 0 && g >= 2) {
-      tc_fence_after();
-      drain_f32(tmem + (g & 1) * RN + dh * 64 + dlane, acc);
-      tc_fence_before();
-    }
-    char* st = smem + s * ROT_STAGE;
-    char* ahi = st;
-    char* alo = st + ROT_A_BYTES;
-    char* bhi = st + 2 * ROT_A_BYTES;
-    char* blo = bhi + ROT_B_BYTES;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) split_store(ahi, alo, mnmaj_off(4 * xc, xr + 8 * i), vx[i]);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const uint32_t off = kmaj_off(zr + 32 * i, zc);
-      *reinterpret_cast<float4*>(bhi + off) = vzh[i];
-      *reinterpret_cast<float4*>(blo + off) = vzl[i];
-    }
-    fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      const uint32_t d = tmem + (g & 1) * RN;
-      const uint32_t sa = smem_u32(ahi), sl = smem_u32(alo);
-      const uint32_t sb = smem_u32(bhi), sbl = smem_u32(blo);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint64_t dah = smem_desc_sw128_b32(sa + q * 1024, 4096, 512);
-        const uint64_t dal = smem_desc_sw128_b32(sl + q * 1024, 4096, 512);
-        const uint64_t dbh = smem_desc_sw128(sb + q * 32, 16, 1024);
-        const uint64_t dbl = smem_desc_sw128(sbl + q * 32, 16, 1024);
-        mma_tf32(d, dal, dbh, idesc, ((kb % DR) | q) != 0);
-        mma_tf32(d, dah, dbl, idesc, 1);
-        mma_tf32(d, dah, dbh, idesc, 1);
+  const long nstage = mytiles * nkb;
+
+  if (warp == 0) {
+    // ---------------------------------------------------------- producer
+    if ((tid & 31) == 0) {
+      long c = 0;
+      for (; c < nstage && !bad; ++c) {
+        const long t = blockIdx.x + (c / nkb) * gridDim.x;
+        const int kb = (int)(c % nkb);
+        const long pt = t / ntn;
+        const int jt = (int)(t % ntn);
+        const int s = (int)(c % STAGES);
+        if (c >= STAGES &&
+            !mbar_wait_or_abort(&bar.empty[s], (int)(c / STAGES - 1) & 1, &abort_flag)) {
+          bad = true;
+          break;
+        }
+        char* st = smem + s * STAGE_BYTES;
+        mbar_arrive_expect_tx(&bar.full[s], 4 * OPB);
+        bulk_load(st, xt + (pt * nkb + kb) * (2L * OPB), 2 * OPB, &bar.full[s]);
+        bulk_load(st + 2 * OPB, zt + ((long)jt * nkb + kb) * (2L * OPB), 2 * OPB, &bar.full[s]);
       }
-      mma_commit(&mbar[s]);
+      for (long j = max(0L, c - STAGES); j < c; ++j)
+        if (!mbar_wait(&bar.full[j % STAGES], (int)(j / STAGES) & 1)) bad = true;
+      if (bad) abort_flag = 1;
     }
-  }
-  if (!bad && nkb > 0) {
-    const int s = (nkb - 1) & 1;
-    const bool ok = mbar_wait(&mbar[s], ((nkb - 1) >> 1) & 1);
-    bad = __syncthreads_or(!ok);
-  }
-  tc_fence_after();
-  if (bad) {
-    if (tid == 0) atomicExch(&g_tc_error, 1);
+  } else if (warp == 1) {
+    // ---------------------------------------------------------- MMA issue
+    if ((tid & 31) == 0) {
+      constexpr uint32_t idesc = idesc_tf32(GM, GN, 1, 0);
+      long c = 0;
+      for (; c < nstage; ++c) {
+        const int kb = (int)(c % nkb);
+        const long G = (c / nkb) * ngrp + kb / DGRP;  // accumulator group, over all tiles
+        const int tb = (int)(G % TM_BUFS), s = (int)(c % STAGES);
+        if (kb % DGRP == 0 && G >= TM_BUFS &&
+            !mbar_wait_or_abort(&bar.tempty[tb], (int)(G / TM_BUFS - 1) & 1, &abort_flag)) {
+          bad = true;
+          break;
+        }
+        if (!mbar_wait_or_abort(&bar.full[s], (int)(c / STAGES) & 1, &abort_flag)) {
+          bad = true;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+        issue_stage<true>(tmem + tb * GN, sa, sa + OPB, sa + 2 * OPB, sa + 3 * OPB, idesc,
+                          kb % DGRP == 0);
+        mma_commit(&bar.empty[s]);
+        if (kb % DGRP == DGRP - 1 || kb == nkb - 1) mma_commit(&bar.tfull[tb]);
+      }
+      if (c > 0 && !mbar_wait(&bar.empty[(c - 1) % STAGES], (int)((c - 1) / STAGES) & 1))
+        bad = true;
+      if (bad) abort_flag = 1;
+    }
   } else {
-    const int glast = (nkb - 1) / DR;
-    if (nkb > 0 && glast >= 1) drain_f32(tmem + ((glast - 1) & 1) * RN + dh * 64 + dlane, acc);
-    if (nkb > 0) drain_f32(tmem + (glast & 1) * RN + dh * 64 + dlane, acc);
-    const long p = p0 + dq * 32 + (tid & 31);
-    if (p < npts) {
+    // ---------------------------------------------------------- drain + store
+    const int dq = warp & 3, dh = (warp - 2) >> 2;
+    const uint32_t dlane = (uint32_t)(dq * 32) << 16;
+    long G = 0;
+    for (long i = 0; i < mytiles && !bad; ++i) {
+      const long t = blockIdx.x + i * gridDim.x;
+      const long p = (t / ntn) * GM + dq * 32 + (tid & 31);
+      const int j0 = (int)(t % ntn) * GN + dh * 64;
+      float acc[64];
 #pragma unroll
-      for (int k = 0; k < 64; ++k) {
-        const int j = j0 + dh * 64 + k;
-        if (j < nout) Y[(long)j * ldy + p] = acc[k];
+      for (int k = 0; k < 64; ++k) acc[k] = 0.f;
+      for (int g = 0; g < ngrp; ++g, ++G) {
+        const int tb = (int)(G % TM_BUFS);
+        const bool ok = mbar_wait_or_abort(&bar.tfull[tb], (int)(G / TM_BUFS) & 1, &abort_flag);
+        if (__any_sync(0xffffffffu, !ok)) { bad = true; break; }
+        tc_fence_after();
+        drain_f32(tmem + tb * GN + dh * 64 + dlane, acc);
+        tc_fence_before();
+        mbar_arrive(&bar.tempty[tb]);
+      }
+      if (!bad && p < npts) {
+#pragma unroll
+        for (int k = 0; k < 64; ++k)
+          if (j0 + k < nout) Y[(long)(j0 + k) * ldy + p] = acc[k];
       }
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, 2 * RN);
+  if (bad || abort_flag) {
+    if (tid == 64) atomicExch(&g_tc_error, 1);
+  }
+  if (warp == 2) tmem_dealloc(tmem, TM_BUFS * GN);
 }
 
-// Z (FP64, column-major kin x nout) -> Zhi/Zlo [j][kpad] FP32 with hi = tf32(z)
-__global__ void k_split_z(const double* __restrict__ Z, long ldz, int kin, int nout, int kpad,
-                          float* __restrict__ hi, float* __restrict__ lo) {
-  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long)nout * kpad) return;
-  const int k = (int)(idx % kpad), j = (int)(idx / kpad);
-  const float z = k < kin ? (float)Z[(long)j * ldz + k] : 0.f;
-  const float h = tf32_rna(z);
-  hi[idx] = h;
-  lo[idx] = z - h;
-}
 
 // ------------------------------------------------------------------ FP64
 // C tile 64 x 64 per block (256 threads, 4 x 4 each), K chunk per blockIdx.y,
@@ -475,37 +620,71 @@ int check_tc_error(cudaStream_t st) {
 
 }  // namespace
 
+// K split of the Gram product: one CTA per SM runs (pairs x splits) CTAs in
+// whole waves where it can, with chunks of at least 8 stages.
+long gram_splits(int npairs, long K) {
+  const long nsm = 148;
+  const long maxsplit = max(1L, K / (8L * KB));
+  long best = 1;
+  double best_eff = -1.0;
+  for (long w = 1; w <= 8; ++w) {
+    const long ns = min(maxsplit, max(1L, w * nsm / npairs));
+    const long ctas = (long)npairs * ns;
+    const long waves = (ctas + nsm - 1) / nsm;
+    const double eff = (double)ctas / (double)(waves * nsm);
+    if (eff > best_eff + 1e-3) { best_eff = eff; best = ns; }
+    if (ns == maxsplit) break;
+  }
+  return best;
+}
+
 int gram_f32(int m, int n, long K, const float* A, long lda, const float* B, long ldb,
              double alpha, double* C, long ldc, int sym, cudaStream_t st) {
   if (m <= 0 || n <= 0) return RS_OK;
-  if (K % 4 || lda % 4 || ldb % 4 ||
-      ((uintptr_t)A | (uintptr_t)B) % 16)
+  if (K % 4 || lda % 4 || ldb % 4 || ((uintptr_t)A | (uintptr_t)B) % 16)
     return fail(RS_EINVAL, "rs_gram_f32: K, lda, ldb must be multiples of 4, A/B 16-byte aligned");
-  if (sym && (m != n || A != B)) sym = 0;
+  if (K <= 0 || lda < K || ldb < K)
+    return fail(RS_EINVAL, "rs_gram_f32: K must be positive and at most lda, ldb");
+  if (sym && (m != n || A != B || lda != ldb)) sym = 0;
+  keep_pool_memory();
   const int tm = (m + GM - 1) / GM, tn = (n + GN - 1) / GN;
   const int npairs = sym ? tm * (tm + 1) / 2 : tm * tn;
-  // about two CTAs' worth of work per SM, at least 4*DG stages per chunk
-  long want = (296 + npairs - 1) / npairs;
-  long kchunk = (K + want - 1) / want;
-  kchunk = (kchunk + KB - 1) / KB * KB;
-  if (kchunk < 4 * DG * KB) kchunk = 4 * DG * KB;
-  long nsplit = (K + kchunk - 1) / kchunk;
-  if (nsplit < 1) nsplit = 1;
+  // K pieces of at most 2^19 values bound the packed copies (2 x 2^19 x 8 B
+  // per band); each piece runs in whole waves of K splits
+  const long piece = min(K, 1L << 19);
+  const long npieces = (K + piece - 1) / piece;
+  const int nkb = (int)((piece + KB - 1) / KB);
+  const int ns = (int)gram_splits(npairs, piece);
+  const int kbc = (nkb + ns - 1) / ns;
+  const int nsplit = (int)npieces * ns;
+  const size_t abytes = (size_t)tm * nkb * 2 * OPB, bbytes = sym ? 0 : (size_t)tn * nkb * 2 * OPB;
+  char* at = nullptr;
   double* part = nullptr;
-  RS_CUDA(cudaMallocAsync((void**)&part, sizeof(double) * npairs * nsplit * GM * GN, st));
-  const size_t smem = 2 * 4 * TILE_BYTES + 1024;
-  RS_CUDA(cudaFuncSetAttribute(k_gram_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem));
-  dim3 grid(npairs, (unsigned)nsplit);
-  k_gram_tf32x3<<<grid, GRAM_THREADS, smem, st>>>(A, lda, m, B, ldb, n, K, kchunk, sym, tm,
-                                                  part);
-  cudaError_t e = cudaGetLastError();
+  RS_CUDA(cudaMallocAsync((void**)&at, abytes + bbytes, st));
+  cudaError_t e = cudaMallocAsync((void**)&part, sizeof(double) * npairs * nsplit * GM * GN, st);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(at, st);
+    return cuda_status(e, "rs_gram_f32: work arrays");
+  }
+  char* bt = sym ? at : at + abytes;
+  e = cudaFuncSetAttribute(k_gram_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)TC_SMEM);
+  for (long pc = 0; pc < npieces && e == cudaSuccess; ++pc) {
+    const long k0 = pc * piece;
+    k_tile_rows<<<(unsigned)(tm * nkb), 256, 0, st>>>(A, lda, m, k0, K, nkb, at);
+    if (!sym) k_tile_rows<<<(unsigned)(tn * nkb), 256, 0, st>>>(B, ldb, n, k0, K, nkb, bt);
+    dim3 grid(npairs, ns);
+    k_gram_tf32x3<<<grid, GRAM_THREADS, TC_SMEM, st>>>(at, bt, nkb, kbc, sym, tm, (int)pc * ns,
+                                                       nsplit, part);
+    e = cudaGetLastError();
+  }
   if (e == cudaSuccess) {
-    k_gram_reduce<<<div_up((long)m * n, 256), 256, 0, st>>>(part, (int)nsplit, m, n, sym, tm,
-                                                            alpha, C, ldc);
+    k_gram_reduce<<<div_up((long)m * n, 256), 256, 0, st>>>(part, nsplit, m, n, sym, tm, alpha,
+                                                            C, ldc);
     e = cudaGetLastError();
   }
   cudaFreeAsync(part, st);
+  cudaFreeAsync(at, st);
   if (e != cudaSuccess) return cuda_status(e, "k_gram_tf32x3");
   return check_tc_error(st);
 }
@@ -515,19 +694,31 @@ int rotate_f32(long npts, int kin, int nout, const float* X, long ldx, const dou
   if (npts <= 0 || nout <= 0) return RS_OK;
   if (npts % 4 || ldx % 4 || (uintptr_t)X % 16)
     return fail(RS_EINVAL, "rs_rotate_f32: points and ldx must be multiples of 4");
-  const int kpad = (kin + KB - 1) / KB * KB;
-  const int npad = (nout + RN - 1) / RN * RN;
-  float *zh = nullptr;
-  RS_CUDA(cudaMallocAsync((void**)&zh, sizeof(float) * 2 * (size_t)npad * kpad, st));
-  float* zl = zh + (size_t)npad * kpad;
-  k_split_z<<<div_up((long)npad * kpad, 256), 256, 0, st>>>(Z, ldz, kin, nout, kpad, zh, zl);
-  const size_t smem = 2 * ROT_STAGE + 1024;
-  RS_CUDA(cudaFuncSetAttribute(k_rotate_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem));
-  dim3 grid(div_up(npts, GM), div_up(nout, RN));
-  k_rotate_tf32x3<<<grid, ROT_THREADS, smem, st>>>(X, ldx, npts, kin, zh, zl, kpad, nout, Y, ldy);
-  cudaError_t e = cudaGetLastError();
-  cudaFreeAsync(zh, st);
+  if (kin <= 0 || ldx < npts) return fail(RS_EINVAL, "rs_rotate_f32: bad kin or ldx");
+  keep_pool_memory();
+  const int nkb = (kin + KB - 1) / KB;
+  const long npt = div_up(npts, GM);
+  const int ntn = (nout + GN - 1) / GN;
+  char* xt = nullptr;
+  char* zt = nullptr;
+  const size_t xbytes = (size_t)npt * nkb * 2 * OPB, zbytes = (size_t)ntn * nkb * 2 * OPB;
+  RS_CUDA(cudaMallocAsync((void**)&xt, xbytes + zbytes, st));
+  zt = xt + xbytes;
+  k_tile_x<<<(unsigned)(npt * nkb), 256, 0, st>>>(X, ldx, npts, kin, nkb, xt);
+  k_tile_z<<<(unsigned)(ntn * nkb), 256, 0, st>>>(Z, ldz, kin, nout, nkb, zt);
+  cudaError_t e = cudaFuncSetAttribute(k_rotate_tf32x3,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+  if (e == cudaSuccess) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long ntiles = npt * ntn;
+    const long nblk = min(ntiles, (long)nsm);
+    k_rotate_tf32x3<<<(unsigned)nblk, TC_THREADS, TC_SMEM, st>>>(xt, zt, npts, nkb, nout, ntiles,
+                                                                 Y, ldy);
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(xt, st);
   if (e != cudaSuccess) return cuda_status(e, "k_rotate_tf32x3");
   return check_tc_error(st);
 }

@@ -15,6 +15,21 @@ static thread_local std::string g_last_error;
 
 void set_error(const std::string& msg) { g_last_error = msg; }
 
+// The H*psi, band and subspace kernels take their per-call work arrays (up to
+// tens of GB for a thousand bands) from the device's default stream-ordered
+// pool.  Let the pool keep freed memory instead of unmapping it at every
+// synchronisation, so repeated calls reuse it (as a caching allocator does).
+void keep_pool_memory() {
+  int dev = 0;
+  cudaMemPool_t pool;
+  if (cudaGetDevice(&dev) == cudaSuccess &&
+      cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+}
+
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
   return code;
@@ -161,20 +176,7 @@ extern "C" int rs_geom_create(rs_geom** out, int nx, int ny, int nz, int nf, dou
     return rs::fail(RS_EINVAL, "rs_geom_create: grid smaller than the stencil");
   const long N = (long)nx * ny * nz;
   if (N > (1L << 31) - 1) return rs::fail(RS_EINVAL, "rs_geom_create: grid too large");
-  // The H*psi and band solvers take their per-call work arrays (up to a few
-  // GB for a thousand bands) from the device's default stream-ordered pool.
-  // Let the pool keep freed memory instead of unmapping it at every
-  // synchronisation, so repeated calls reuse it (as a caching allocator does).
-  {
-    int dev = 0;
-    cudaMemPool_t pool;
-    if (cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-      uint64_t keep = UINT64_MAX;
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
-    cudaGetLastError();
-  }
+  rs::keep_pool_memory();
   rs_geom* g = new rs_geom;
   memset(g, 0, sizeof(*g));
   g->nx = nx; g->ny = ny; g->nz = nz; g->nf = nf;

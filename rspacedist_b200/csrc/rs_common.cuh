@@ -18,6 +18,8 @@ namespace rs {
 
 // thread-local message for rs_last_error()
 void set_error(const std::string& msg);
+// sets the default memory pool of the current device to keep freed memory
+void keep_pool_memory();
 int fail(int code, const std::string& msg);
 int cuda_status(cudaError_t e, const char* what);
 
