@@ -343,51 +343,146 @@ __global__ void k_axpy_b(long n, const T* __restrict__ a, const T* __restrict__ 
   const double d = sign * dp[(long)blockIdx.y * dstride];
   c[o] = (T)fma(d, (double)b[o], (double)a[o]);
 }
-__global__ void k_axpy_d_b(long n, const double* __restrict__ a, const double* __restrict__ b,
-                           const double* __restrict__ dp, long dstride, double* __restrict__ c) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const long o = (long)blockIdx.y * n + i;
-  c[o] = fma(dp[(long)blockIdx.y * dstride], b[o], a[o]);
-}
 
-// k_scale3 per band with t = tmp[j*tstride]
-template <class T>
-__global__ void k_scale3_b(long n, T* __restrict__ a, T* __restrict__ b, long nrp,
-                           double* __restrict__ r, const double* __restrict__ tmp, long tstride) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
-  const double t = tmp[(long)j * tstride];
-  if (i < n) {
-    const long o = (long)j * n + i;
-    a[o] = (T)((double)a[o] * t);
-    if (b) b[o] = (T)((double)b[o] * t);
+// ---- fused DIIS passes.  Each forms the trial vectors of ksdiis_r on the
+// fly, rounded to T exactly as the stored vectors were, and accumulates every
+// dot product it needs in the fixed tree order, so each band sees the same
+// values as with the vectors stored.  part layout: [dot][band][chunk].
+//
+// Trial-step sums (ksdiis8f.F90:285-300) with a1 = alambda_diis:
+//   rvre.hs, rvre.ss, ph1.hph1, ph1.sph1 with ph1 = ps + a1 rvre,
+//   hph1 = hs + a1 avre, sph1 = ss + a1 asvre (ph1 when S = 1).
+template <class T, bool SP>
+__global__ void k_diis_dots_a(long n, const T* __restrict__ ps, const T* __restrict__ rvre,
+                              const T* __restrict__ hs, const T* __restrict__ avre,
+                              const T* __restrict__ ss, const T* __restrict__ asvre,
+                              const double* __restrict__ a1p, long nblk,
+                              double* __restrict__ part) {
+  __shared__ double ws[8];
+  const int j = blockIdx.y, nb = gridDim.y;
+  const long off = (long)j * n;
+  const double a1 = *a1p;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+#pragma unroll 4
+  for (int k = 0; k < kTreePerLane; ++k) {
+    const long i = base + (long)k * kTreeLanes;
+    if (i < n) {
+      const long o = off + i;
+      const double r = (double)rvre[o], h = (double)hs[o], p = (double)ps[o];
+      const double s = SP ? (double)ss[o] : p;
+      const T p1 = (T)fma(a1, r, p);
+      const T h1 = (T)fma(a1, (double)avre[o], h);
+      const T s1 = SP ? (T)fma(a1, (double)asvre[o], s) : p1;
+      acc[0] = fma(r, h, acc[0]);
+      acc[1] = fma(r, s, acc[1]);
+      acc[2] = fma((double)p1, (double)h1, acc[2]);
+      acc[3] = fma((double)p1, (double)s1, acc[3]);
+    }
   }
-  if (i < nrp) r[(long)j * nrp + i] = r[(long)j * nrp + i] * t;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    const double v = tree_fold256(acc[d], ws);
+    if (threadIdx.x == 0) part[((long)d * nb + j) * nblk + blockIdx.x] = v;
+  }
 }
 
-// new_j = c1 y1_j + c0 y0_j (ksdiis_r_03 with two vectors; the rp form
-// starts from 0), c = cc + j*cstride
-// (y0 and out may be the same array: each element is read before it is written)
-template <class T>
-__global__ void k_comb2_b(long n, const T* y0, const T* __restrict__ y1,
-                          const double* __restrict__ cc, long cstride, T* out) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double* c = cc + (long)blockIdx.y * cstride;
-  const long o = (long)blockIdx.y * n + i;
-  out[o] = (T)fma(c[1], (double)y1[o], c[0] * (double)y0[o]);
+// DIIS matrix sums (ksdiis8f.F90:321-404) with the step lam of band j:
+//   ps.ss, rvv0.rvv0, ps.sph1, rvv0.rvv1, ph1.sph1, rvv1.rvv1 with
+//   ph1 = ps + lam rvre, hph1 = hs + lam avre, sph1 = ss + lam asvre,
+//   rvv1 = hph1 - sval sph1.
+template <class T, bool SP>
+__global__ void k_diis_dots_b(long n, const T* __restrict__ ps, const T* __restrict__ rvre,
+                              const T* __restrict__ hs, const T* __restrict__ avre,
+                              const T* __restrict__ ss, const T* __restrict__ asvre,
+                              const T* __restrict__ rvv0, const Sc* __restrict__ sc,
+                              const double* __restrict__ sval, long nblk,
+                              double* __restrict__ part) {
+  __shared__ double ws[8];
+  const int j = blockIdx.y, nb = gridDim.y;
+  const long off = (long)j * n;
+  const double lam = sc[j].lam, ev = -1.0 * sval[j];
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+#pragma unroll 4
+  for (int k = 0; k < kTreePerLane; ++k) {
+    const long i = base + (long)k * kTreeLanes;
+    if (i < n) {
+      const long o = off + i;
+      const double p = (double)ps[o];
+      const double s = SP ? (double)ss[o] : p;
+      const double v0 = (double)rvv0[o];
+      const T p1 = (T)fma(lam, (double)rvre[o], p);
+      const T h1 = (T)fma(lam, (double)avre[o], (double)hs[o]);
+      const T s1 = SP ? (T)fma(lam, (double)asvre[o], s) : p1;
+      const double v1 = (double)(T)fma(ev, (double)s1, (double)h1);
+      acc[0] = fma(p, s, acc[0]);
+      acc[1] = fma(v0, v0, acc[1]);
+      acc[2] = fma(p, (double)s1, acc[2]);
+      acc[3] = fma(v0, v1, acc[3]);
+      acc[4] = fma((double)p1, (double)s1, acc[4]);
+      acc[5] = fma(v1, v1, acc[5]);
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 6; ++d) {
+    const double v = tree_fold256(acc[d], ws);
+    if (threadIdx.x == 0) part[((long)d * nb + j) * nblk + blockIdx.x] = v;
+  }
 }
-__global__ void k_comb2_rp_b(long n, const double* y0, const double* __restrict__ y1,
-                             const double* __restrict__ cc, long cstride, double* out) {
+
+// chunk sums -> out[d][j * ostride] (times dV where scale[d]); grid (nb, ndot)
+struct DotOuts {
+  double* out[6];
+  int scale[6];
+};
+__global__ void k_dots_final(long nblk, const double* __restrict__ part, double dx, double dy,
+                             double dz, DotOuts o, long ostride) {
+  __shared__ double ws[8];
+  const int j = blockIdx.x, d = blockIdx.y, nb = gridDim.x;
+  const double* p = part + ((long)d * nb + j) * nblk;
+  double acc = 0.0;
+  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + p[k];
+  const double s = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) o.out[d][(long)j * ostride] = o.scale[d] ? s * dx * dy * dz : s;
+}
+
+// The DIIS combination (ksdiis8f.F90:549-600) of band j with the normalised
+// trial vectors: y1 = tmp * (y + lam dy), new = c1 y1 + c0 y for psi, S psi
+// (with an S metric) and H psi.
+template <class T, bool SP>
+__global__ void k_diis_comb(long n, T* ps, const T* __restrict__ rvre, T* hs,
+                            const T* __restrict__ avre, T* ss, const T* __restrict__ asvre,
+                            const Sc* __restrict__ sc) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double* c = cc + (long)blockIdx.y * cstride;
+  const Sc& q = sc[blockIdx.y];
+  const double lam = q.lam, t = q.tmp, c0 = q.c[0], c1 = q.c[1];
   const long o = (long)blockIdx.y * n + i;
+  const double p = (double)ps[o];
+  const T p1 = (T)((double)(T)fma(lam, (double)rvre[o], p) * t);
+  ps[o] = (T)fma(c1, (double)p1, c0 * p);
+  if (SP) {
+    const double s = (double)ss[o];
+    const T s1 = (T)((double)(T)fma(lam, (double)asvre[o], s) * t);
+    ss[o] = (T)fma(c1, (double)s1, c0 * s);
+  }
+  const double h = (double)hs[o];
+  const T h1 = (T)((double)(T)fma(lam, (double)avre[o], h) * t);
+  hs[o] = (T)fma(c1, (double)h1, c0 * h);
+}
+__global__ void k_diis_comb_rp(long n, double* rps, const double* __restrict__ rpsep,
+                               const Sc* __restrict__ sc) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Sc& q = sc[blockIdx.y];
+  const long o = (long)blockIdx.y * n + i;
+  const double r = rps[o];
+  const double r1 = fma(q.lam, rpsep[o], r) * q.tmp;
   double acc = 0.0;
-  acc = fma(c[0], y0[o], acc);
-  acc = fma(c[1], y1[o], acc);
-  out[o] = acc;
+  acc = fma(q.c[0], r, acc);
+  acc = fma(q.c[1], r1, acc);
+  rps[o] = acc;
 }
 
 __global__ void k_diis_lambda_b(int nb, Sc* sc, const double* __restrict__ sval, double a1,
@@ -727,32 +822,32 @@ static int ksdiis(BandCtx<T>& c, const rs_solver_prm* prm, int l_hsv, double* sv
   const bool sp = c.sep();
   const int M = c.M;
   // a block of B bands runs each step of the band loop at once; its work
-  // vectors (phi1, H phi1, two residuals, the preconditioned residual and its
-  // H image, plus S phi1 and the S image with an S metric) stay within ~8 GB
-  const int nvec = sp ? 8 : 6;
-  const long per_band = (long)nvec * N * (long)sizeof(T) + 2 * nrp * (long)sizeof(double);
+  // vectors (the residual, the preconditioned residual and its H image, plus
+  // its S image with an S metric) stay within ~8 GB.  The trial vectors
+  // phi1, H phi1, S phi1 and the second residual are formed on the fly by
+  // the fused passes.
+  const int nvec = sp ? 4 : 3;
+  const long per_band = (long)nvec * N * (long)sizeof(T) + nrp * (long)sizeof(double);
   const int B = (int)std::min<long>(std::min<long>(M, 65535),
                                     std::max<long>(1, (8L << 30) / per_band));
   T* wv = nullptr;
   double* wd = nullptr;
   RS_CUDA(cudaMallocAsync((void**)&wv, sizeof(T) * (size_t)nvec * B * N, c.st));
-  const size_t nd = (size_t)2 * B * (nrp > 0 ? nrp : 1) + 2 * (M + 1) + 1;
+  const size_t nd = (size_t)B * (nrp > 0 ? nrp : 1) + 2 * (M + 1) + 1;
   cudaError_t e = cudaMallocAsync((void**)&wd, sizeof(double) * nd, c.st);
   Sc* scb = nullptr;
+  double* dpart = nullptr;  // chunk sums of the fused passes: [6][B][nblk]
   if (e == cudaSuccess) e = cudaMallocAsync((void**)&scb, sizeof(Sc) * B, c.st);
   if (e == cudaSuccess) e = cudaMemsetAsync(scb, 0, sizeof(Sc) * B, c.st);
+  if (e == cudaSuccess)
+    e = cudaMallocAsync((void**)&dpart, sizeof(double) * 6 * (size_t)B * c.nblk, c.st);
   if (e != cudaSuccess) rc = cuda_status(e, "ksdiis: work arrays");
   const size_t BN = (size_t)B * N;
-  T* ph1 = wv;
-  T* hph1 = ph1 + BN;
-  T* rvv0 = hph1 + BN;
-  T* rvv1 = rvv0 + BN;
-  T* rvre = rvv1 + BN;
+  T* rvv0 = wv;
+  T* rvre = rvv0 + BN;
   T* avre = rvre + BN;
-  T* sph1 = sp ? avre + BN : ph1;
-  T* asvre = sp ? sph1 + BN : nullptr;
-  double* rph1 = wd;
-  double* rpsep = rph1 + (size_t)B * (nrp > 0 ? nrp : 1);
+  T* asvre = sp ? avre + BN : nullptr;
+  double* rpsep = wd;
   double* dval = rpsep + (size_t)B * (nrp > 0 ? nrp : 1);
   double* dres = dval + M + 1;
   double* da1 = dres + M + 1;
@@ -773,9 +868,8 @@ static int ksdiis(BandCtx<T>& c, const rs_solver_prm* prm, int l_hsv, double* sv
     T* ss = sp ? c.band(c.spsi, b0) : ps;      // S phi0
     T* hs = c.band(c.hpsi, b0);                // H phi0, computed afresh each sweep
     double* rps = c.rpb(c.rp, b0);
-    T* sph1v = sp ? sph1 : ph1;
     const dim3 gv(div_up(N, 256), nb), gr(div_up(nrp > 0 ? nrp : 1, 256), nb);
-    const dim3 g3(div_up(std::max(N, nrp), 256), nb);
+    const dim3 gd((unsigned)c.nblk, nb);
     const unsigned gs = div_up(nb, 128);
     for (int jiter = 1; jiter + 1 <= prm->ndiismax && !rc; ++jiter) {
       if ((rc = c.apply_h(ps, rps, hs, nb))) break;
@@ -788,39 +882,43 @@ static int ksdiis(BandCtx<T>& c, const rs_solver_prm* prm, int l_hsv, double* sv
       if ((rc = c.nl_dot(rvre, rpsep, nb))) break;
       if ((rc = c.apply_h(rvre, rpsep, avre, nb))) break;
       if (sp && (rc = c.apply_s(rvre, rpsep, asvre, nb))) break;
-      // trial step with alambda_diis
-      if (nrp) k_axpy_d_b<<<gr, 256, 0, c.st>>>(nrp, rps, rpsep, da1, 0, rph1);
-      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, ps, rvre, da1, 0, 1.0, ph1);
-      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, hs, avre, da1, 0, 1.0, hph1);
-      if (sp) k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, ss, asvre, da1, 0, 1.0, sph1);
-      pdot(rvre, hs, nb, &scb->s[0], kScStride, 0);
-      pdot(rvre, ss, nb, &scb->s[1], kScStride, 0);
-      pdot(ph1, hph1, nb, &scb->s[2], kScStride, 0);
-      pdot(ph1, sph1v, nb, &scb->s[3], kScStride, 0);
+      // trial step with alambda_diis: the four line-search sums in one pass
+      if (sp)
+        k_diis_dots_a<T, true><<<gd, kTreeLanes, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre, da1,
+                                                            c.nblk, dpart);
+      else
+        k_diis_dots_a<T, false><<<gd, kTreeLanes, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre,
+                                                             da1, c.nblk, dpart);
+      {
+        DotOuts o{};
+        for (int d = 0; d < 4; ++d) { o.out[d] = &scb->s[d]; o.scale[d] = 0; }
+        k_dots_final<<<dim3(nb, 4), kTreeLanes, 0, c.st>>>(c.nblk, dpart, c.dx, c.dy, c.dz, o,
+                                                          kScStride);
+      }
       k_diis_lambda_b<<<gs, 128, 0, c.st>>>(nb, scb, dval + b0, a1, c.dx, c.dy, c.dz,
                                             prm->alambda_min, prm->alambda_max);
-      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, ps, rvre, &scb->lam, kScStride, 1.0, ph1);
-      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, hs, avre, &scb->lam, kScStride, 1.0, hph1);
-      if (sp) k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, ss, asvre, &scb->lam, kScStride, 1.0, sph1);
-      if (nrp) k_axpy_d_b<<<gr, 256, 0, c.st>>>(nrp, rps, rpsep, &scb->lam, kScStride, rph1);
-      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, hs, ss, dval + b0, 1, -1.0, rvv0);
-      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, hph1, sph1v, dval + b0, 1, -1.0, rvv1);
-      pdot(ps, ss, nb, &scb->rs[0], kScStride, 1);
-      pdot(rvv0, rvv0, nb, &scb->rr[0], kScStride, 1);
-      pdot(ps, sph1v, nb, &scb->rs[1], kScStride, 1);
-      pdot(rvv0, rvv1, nb, &scb->rr[1], kScStride, 1);
-      pdot(ph1, sph1v, nb, &scb->rs[3], kScStride, 1);
-      pdot(rvv1, rvv1, nb, &scb->rr[3], kScStride, 1);
+      // the 2x2 DIIS matrices at the step lam, in one pass
+      if (sp)
+        k_diis_dots_b<T, true><<<gd, kTreeLanes, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre,
+                                                            rvv0, scb, dval + b0, c.nblk, dpart);
+      else
+        k_diis_dots_b<T, false><<<gd, kTreeLanes, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre,
+                                                             rvv0, scb, dval + b0, c.nblk, dpart);
+      {
+        DotOuts o{};
+        double* outs[6] = {&scb->rs[0], &scb->rr[0], &scb->rs[1],
+                           &scb->rr[1], &scb->rs[3], &scb->rr[3]};
+        for (int d = 0; d < 6; ++d) { o.out[d] = outs[d]; o.scale[d] = 1; }
+        k_dots_final<<<dim3(nb, 6), kTreeLanes, 0, c.st>>>(c.nblk, dpart, c.dx, c.dy, c.dz, o,
+                                                          kScStride);
+      }
       k_diis_norm_b<<<gs, 128, 0, c.st>>>(nb, scb);
-      k_scale3_b<T><<<g3, 256, 0, c.st>>>(N, ph1, hph1, nrp, rph1, &scb->tmp, kScStride);
-      if (sp) k_scale3_b<T><<<gv, 256, 0, c.st>>>(N, sph1, rvv1, 0, nullptr, &scb->tmp, kScStride);
-      else k_scale3_b<T><<<gv, 256, 0, c.st>>>(N, rvv1, nullptr, 0, nullptr, &scb->tmp, kScStride);
       k_diis_scale_mats_b<<<gs, 128, 0, c.st>>>(nb, scb);
       k_diis_solve_b<<<gs, 128, 0, c.st>>>(nb, scb, prm->eps_eig_diis, dres + b0);
-      k_comb2_b<T><<<gv, 256, 0, c.st>>>(N, ps, ph1, &scb->c[0], kScStride, ps);
-      if (sp) k_comb2_b<T><<<gv, 256, 0, c.st>>>(N, ss, sph1, &scb->c[0], kScStride, ss);
-      k_comb2_b<T><<<gv, 256, 0, c.st>>>(N, hs, hph1, &scb->c[0], kScStride, hs);
-      if (nrp) k_comb2_rp_b<<<gr, 256, 0, c.st>>>(nrp, rps, rph1, &scb->c[0], kScStride, rps);
+      // combination with the normalised trial vectors (formed again on the fly)
+      if (sp) k_diis_comb<T, true><<<gv, 256, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre, scb);
+      else k_diis_comb<T, false><<<gv, 256, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre, scb);
+      if (nrp) k_diis_comb_rp<<<gr, 256, 0, c.st>>>(nrp, rps, rpsep, scb);
       e = cudaGetLastError();
       if (e != cudaSuccess) rc = cuda_status(e, "ksdiis");
     }
@@ -840,6 +938,7 @@ static int ksdiis(BandCtx<T>& c, const rs_solver_prm* prm, int l_hsv, double* sv
   if (wv) cudaFreeAsync(wv, c.st);
   if (wd) cudaFreeAsync(wd, c.st);
   if (scb) cudaFreeAsync(scb, c.st);
+  if (dpart) cudaFreeAsync(dpart, c.st);
   c.release();
   return rc;
 }
