@@ -1,6 +1,7 @@
 // syev.cu -- FP64 dense kernels of the subspace step on the GPU:
-//  * symmetric eigensolver (parallel cyclic Jacobi, round-robin pairing), the
-//    replacement of dsyev / pdsyevd in rayleighritz_r
+//  * symmetric eigensolver (block Jacobi: round-robin pairing of 32-index
+//    blocks, 64 x 64 subproblems in shared memory, batched FP64 tile
+//    updates), the replacement of dsyev / pdsyevd in rayleighritz_r
 //    (rayleigh-ritz8f.F90:89; rayleigh-ritz8f_sclpck.F90:268);
 //  * Cholesky factorisation and triangular inverse for Cholesky-QR, which
 //    spans the same vectors in the same order as kukan's block Gram-Schmidt
@@ -12,12 +13,9 @@
 #include "reduce.cuh"
 #include <algorithm>
 
-#include <cooperative_groups.h>
-
 #include "rs_common.cuh"
 
 namespace rs {
-namespace cg = cooperative_groups;
 namespace {
 
 // pairs of round r of the circle method over ne (even) players
@@ -34,84 +32,193 @@ struct Rot {
   double c, s;
 };
 
-// rotation angle zeroing a_pq (same formula as the CPU oracle's Jacobi)
-__device__ __forceinline__ void jac_params(const double* __restrict__ A, int n, int ne, int r,
-                                           int t, Rot* __restrict__ rot) {
-  int p, q;
-  rr_pair(r, t, ne, &p, &q);
-  Rot o{p, q, 1.0, 0.0};
-  if (q < n) {
-    const double apq = A[(long)p * n + q];
-    if (apq != 0.0) {
-      const double app = A[(long)p * n + p], aqq = A[(long)q * n + q];
-      const double theta = (aqq - app) / (2.0 * apq);
-      const double tt = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-      const double c = 1.0 / sqrt(tt * tt + 1.0);
-      o.c = c;
-      o.s = tt * c;
-    }
-  }
-  rot[t] = o;
+// ------------------------------------------------ block Jacobi eigensolver
+// The padded matrix (np = nbe*32 indices, nbe even) is split into 32-index
+// blocks; a sweep is nbe-1 rounds of the circle method over the blocks.  In a
+// round every block pair P = (I, J) is one 64 x 64 subproblem:
+//  * k_bjac_solve: one CTA runs a cyclic Jacobi sweep of the subproblem in
+//    shared memory (63 rounds of 32 disjoint rotations, the rotation and the
+//    exact zeroing of each annihilated element as in the scalar method),
+//    writes the rotated 64 x 64 block back and keeps Q_P (the product of its
+//    rotations);
+//  * k_bjac_update: every other tile, A(P1, P2) <- Q_P1^T A(P1, P2) Q_P2 for
+//    P1 > P2 (mirrored to (P2, P1), so A stays exactly symmetric), and the
+//    eigenvectors V(:, P) <- V(:, P) Q_P.
+// Padding indices have zero couplings, so their rotations are exact
+// identities and the real n x n problem is untouched by them.
+constexpr int JB = 32;
+constexpr int JB2 = 2 * JB;
+constexpr int JLD = JB2 + 1;  // padded smem row
+constexpr int kBjThreads = 256;
+
+__device__ __forceinline__ int bj_index(int I, int J, int k) {
+  return k < JB ? I * JB + k : J * JB + (k - JB);
 }
 
-// A <- J^T A J on every 2x2 block (P, Q) of the pairing, V <- V J
-__device__ __forceinline__ void jac_apply(double* __restrict__ A, double* __restrict__ V, int n,
-                                          int npair, const Rot* __restrict__ rot, long idx) {
-  const long nblk = (long)npair * npair;
-  if (idx < nblk) {
-    const Rot P = rot[idx % npair], Q = rot[idx / npair];
-    if (P.q < n && Q.q < n) {
-      const double apr = A[(long)P.p * n + Q.p], aps = A[(long)P.p * n + Q.q];
-      const double aqr = A[(long)P.q * n + Q.p], aqs = A[(long)P.q * n + Q.q];
-      // rows: new_p = c a_p - s a_q, new_q = s a_p + c a_q
+// rotation (c, s) zeroing S[p][q] (same formula as the scalar sweep)
+__device__ __forceinline__ Rot bj_params(const double (*S)[JLD], int p, int q) {
+  Rot o{p, q, 1.0, 0.0};
+  const double apq = S[p][q];
+  if (apq != 0.0) {
+    const double app = S[p][p], aqq = S[q][q];
+    const double theta = (aqq - app) / (2.0 * apq);
+    const double tt = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+    const double c = 1.0 / sqrt(tt * tt + 1.0);
+    o.c = c;
+    o.s = tt * c;
+  }
+  return o;
+}
+
+__global__ void __launch_bounds__(kBjThreads) k_bjac_solve(double* __restrict__ A, int np,
+                                                           int nbe, int round,
+                                                           double* __restrict__ Qbuf) {
+  extern __shared__ double bj_sm[];
+  double(*S)[JLD] = reinterpret_cast<double(*)[JLD]>(bj_sm);  // [JB2][JLD]
+  double(*Q)[JLD] = S + JB2;
+  __shared__ Rot rot[JB];
+  const int tid = threadIdx.x;
+  int I, J;
+  rr_pair(round, blockIdx.x, nbe, &I, &J);
+  for (int e = tid; e < JB2 * JB2; e += kBjThreads) {
+    const int r = e / JB2, c = e % JB2;
+    S[r][c] = A[(long)bj_index(I, J, r) * np + bj_index(I, J, c)];
+    Q[r][c] = r == c ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  for (int ir = 0; ir < JB2 - 1; ++ir) {
+    if (tid < JB) {
+      int p, q;
+      rr_pair(ir, tid, JB2, &p, &q);
+      rot[tid] = bj_params(S, p, q);
+    }
+    __syncthreads();
+    // S <- J^T S J on the 2x2 blocks of every two rotations
+    for (int k = tid; k < JB * JB; k += kBjThreads) {
+      const Rot P = rot[k % JB], R = rot[k / JB];
+      const double apr = S[P.p][R.p], aps = S[P.p][R.q];
+      const double aqr = S[P.q][R.p], aqs = S[P.q][R.q];
       const double rpr = P.c * apr - P.s * aqr, rps = P.c * aps - P.s * aqs;
       const double rqr = P.s * apr + P.c * aqr, rqs = P.s * aps + P.c * aqs;
-      // columns; on the pair's own 2x2 block the annihilated element is set
-      // to zero exactly (its computed value is rounding noise of size
-      // eps*|a_pp|, which would stall convergence for large n)
-      A[(long)P.p * n + Q.p] = Q.c * rpr - Q.s * rps;
-      A[(long)P.p * n + Q.q] = P.p == Q.p ? 0.0 : Q.s * rpr + Q.c * rps;
-      A[(long)P.q * n + Q.p] = P.p == Q.p ? 0.0 : Q.c * rqr - Q.s * rqs;
-      A[(long)P.q * n + Q.q] = Q.s * rqr + Q.c * rqs;
-    } else if (P.q >= n && Q.q < n && P.p < n) {
-      // P pairs a real index with the dummy: only the column rotation of Q
-      const double ar = A[(long)P.p * n + Q.p], as = A[(long)P.p * n + Q.q];
-      A[(long)P.p * n + Q.p] = Q.c * ar - Q.s * as;
-      A[(long)P.p * n + Q.q] = Q.s * ar + Q.c * as;
-    } else if (Q.q >= n && P.q < n && Q.p < n) {
-      const double ap = A[(long)P.p * n + Q.p], aq = A[(long)P.q * n + Q.p];
-      A[(long)P.p * n + Q.p] = P.c * ap - P.s * aq;
-      A[(long)P.q * n + Q.p] = P.s * ap + P.c * aq;
+      S[P.p][R.p] = R.c * rpr - R.s * rps;
+      S[P.p][R.q] = P.p == R.p ? 0.0 : R.s * rpr + R.c * rps;
+      S[P.q][R.p] = P.p == R.p ? 0.0 : R.c * rqr - R.s * rqs;
+      S[P.q][R.q] = R.s * rqr + R.c * rqs;
     }
-  } else {
-    const long v = idx - nblk;
-    if (v >= (long)npair * n) return;
-    const Rot Q = rot[v / n];
-    const int i = (int)(v % n);
-    if (Q.q >= n) return;
-    // V column-major: column k at V + k*n
-    const double vp = V[(long)Q.p * n + i], vq = V[(long)Q.q * n + i];
-    V[(long)Q.p * n + i] = Q.c * vp - Q.s * vq;
-    V[(long)Q.q * n + i] = Q.s * vp + Q.c * vq;
+    // Q <- Q J
+    for (int k = tid; k < JB * JB2; k += kBjThreads) {
+      const Rot R = rot[k / JB2];
+      const int i = k % JB2;
+      const double qp = Q[i][R.p], qq = Q[i][R.q];
+      Q[i][R.p] = R.c * qp - R.s * qq;
+      Q[i][R.q] = R.s * qp + R.c * qq;
+    }
+    __syncthreads();
+  }
+  double* Qo = Qbuf + (long)blockIdx.x * JB2 * JB2;
+  for (int e = tid; e < JB2 * JB2; e += kBjThreads) {
+    const int r = e / JB2, c = e % JB2;
+    A[(long)bj_index(I, J, r) * np + bj_index(I, J, c)] = S[r][c];
+    Qo[e] = Q[r][c];  // row-major Q[r][c]
   }
 }
 
-// one cyclic sweep: ne-1 rounds of (rotation parameters, apply), separated by
-// grid-wide barriers of a cooperative launch (all blocks are co-resident)
-constexpr int kJacThreads = 1024;
-__global__ void __launch_bounds__(kJacThreads) k_jac_sweep(double* __restrict__ A, double* __restrict__ V, int n, int ne,
-                            Rot* __restrict__ rot) {
-  cg::grid_group grid = cg::this_grid();
-  const int npair = ne / 2;
-  const long nwork = (long)npair * npair + (long)npair * n;
-  const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long stride = (long)gridDim.x * blockDim.x;
-  for (int r = 0; r < ne - 1; ++r) {
-    for (long t = tid; t < npair; t += stride) jac_params(A, n, ne, r, (int)t, rot);
-    grid.sync();
-    for (long idx = tid; idx < nwork; idx += stride) jac_apply(A, V, n, npair, rot, idx);
-    grid.sync();
+// C (64 x 64, smem) = X^T Y or X Y for 64 x 64 smem operands; 256 threads,
+// a 4 x 4 output block each (rows ty + 16 a, columns tx + 16 b)
+template <bool XT>
+__device__ __forceinline__ void bj_gemm(const double (*X)[JLD], const double (*Y)[JLD],
+                                        double (*C)[JLD]) {
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4] = {};
+  for (int k = 0; k < JB2; ++k) {
+    double x[4], y[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) x[a] = XT ? X[k][ty + 16 * a] : X[ty + 16 * a][k];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) y[b] = Y[k][tx + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
   }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) C[ty + 16 * a][tx + 16 * b] = acc[a][b];
+}
+
+// blocks [0, ntile): A tiles (P1 > P2) of the round; then V tiles (64 rows of
+// V x the 64 columns of one pair).  V is column-major: (i, k) at V[k*np + i].
+__global__ void __launch_bounds__(kBjThreads) k_bjac_update(double* __restrict__ A,
+                                                            double* __restrict__ V, int np,
+                                                            int nbe, int round,
+                                                            const double* __restrict__ Qbuf) {
+  extern __shared__ double bj_sm[];
+  double(*X)[JLD] = reinterpret_cast<double(*)[JLD]>(bj_sm);
+  double(*Y)[JLD] = X + JB2;
+  double(*T)[JLD] = Y + JB2;
+  const int tid = threadIdx.x;
+  const int npair = nbe / 2;
+  const int ntile = npair * (npair - 1) / 2;
+  const int bx = blockIdx.x;
+  if (bx < ntile) {
+    int p1 = (int)((sqrtf(8.f * bx + 1.f) + 1.f) * 0.5f);  // bx = p1 (p1 - 1) / 2 + p2
+    while (p1 * (p1 - 1) / 2 > bx) --p1;
+    while ((p1 + 1) * p1 / 2 <= bx) ++p1;
+    const int p2 = bx - p1 * (p1 - 1) / 2;
+    int I1, J1, I2, J2;
+    rr_pair(round, p1, nbe, &I1, &J1);
+    rr_pair(round, p2, nbe, &I2, &J2);
+    const double* Q1 = Qbuf + (long)p1 * JB2 * JB2;
+    const double* Q2 = Qbuf + (long)p2 * JB2 * JB2;
+    for (int e = tid; e < JB2 * JB2; e += kBjThreads) {
+      const int r = e / JB2, c = e % JB2;
+      X[r][c] = Q1[e];
+      Y[r][c] = A[(long)bj_index(I1, J1, r) * np + bj_index(I2, J2, c)];
+    }
+    __syncthreads();
+    bj_gemm<true>(X, Y, T);  // T = Q1^T B
+    __syncthreads();
+    for (int e = tid; e < JB2 * JB2; e += kBjThreads) X[e / JB2][e % JB2] = Q2[e];
+    __syncthreads();
+    bj_gemm<false>(T, X, Y);  // Y = T Q2
+    __syncthreads();
+    for (int e = tid; e < JB2 * JB2; e += kBjThreads) {
+      const int r = e / JB2, c = e % JB2;
+      const double v = Y[r][c];
+      A[(long)bj_index(I1, J1, r) * np + bj_index(I2, J2, c)] = v;
+      A[(long)bj_index(I2, J2, c) * np + bj_index(I1, J1, r)] = v;
+    }
+  } else {
+    const int v = bx - ntile;
+    const int p = v % npair, rt = v / npair;
+    int I, J;
+    rr_pair(round, p, nbe, &I, &J);
+    const double* Qp = Qbuf + (long)p * JB2 * JB2;
+    for (int e = tid; e < JB2 * JB2; e += kBjThreads) {
+      Y[e / JB2][e % JB2] = Qp[e];
+      const int r = e % JB2, c = e / JB2;  // consecutive threads: consecutive rows of V
+      X[r][c] = V[(long)bj_index(I, J, c) * np + rt * JB2 + r];
+    }
+    __syncthreads();
+    bj_gemm<false>(X, Y, T);  // T = V(rows, P) Q
+    __syncthreads();
+    for (int e = tid; e < JB2 * JB2; e += kBjThreads) {
+      const int r = e % JB2, c = e / JB2;
+      V[(long)bj_index(I, J, c) * np + rt * JB2 + r] = T[r][c];
+    }
+  }
+}
+
+// padded copy A' (np x np) = [A 0; 0 0] and V' = I: a zero coupling is
+// never rotated, so the padding indices stay exactly decoupled
+__global__ void k_bjac_pad(const double* __restrict__ A, int n, int np, double* __restrict__ Ap,
+                           double* __restrict__ V) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long)np * np) return;
+  const int r = (int)(e / np), c = (int)(e % np);
+  Ap[e] = (r < n && c < n) ? A[(long)r * n + c] : 0.0;
+  V[e] = r == c ? 1.0 : 0.0;
 }
 
 // sums of squares of the off-diagonal and of all elements: chunk sums of the
@@ -153,25 +260,21 @@ __global__ void k_offdiag_fold(long nblk, const double* __restrict__ part, doubl
   }
 }
 
-__global__ void k_eye(double* __restrict__ V, int n) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < (long)n * n) V[k] = (k / n == k % n) ? 1.0 : 0.0;
-}
-
-// ascending stable order of the diagonal; columns of V permuted, each made to
-// have its largest-magnitude component positive
+// ascending stable order of the diagonal of the leading n x n block (row
+// stride ld); columns of V permuted, each made to have its largest-magnitude
+// component positive
 __global__ void k_sort_eig(const double* __restrict__ A, const double* __restrict__ V, int n,
-                           double* __restrict__ w, double* __restrict__ Z) {
+                           int ld, double* __restrict__ w, double* __restrict__ Z) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double di = A[(long)i * n + i];
+  const double di = A[(long)i * ld + i];
   int rank = 0;
   for (int j = 0; j < n; ++j) {
-    const double dj = A[(long)j * n + j];
+    const double dj = A[(long)j * ld + j];
     if (dj < di || (dj == di && j < i)) ++rank;
   }
   w[rank] = di;
-  const double* v = V + (long)i * n;
+  const double* v = V + (long)i * ld;
   int im = 0;
   for (int k = 1; k < n; ++k)
     if (fabs(v[k]) > fabs(v[im])) im = k;
@@ -297,55 +400,53 @@ __global__ void k_trinv_cols(const double* __restrict__ LT, int n, double* __res
 }  // namespace
 
 // A (n x n, symmetric, device) is overwritten; w (device, n) eigenvalues
-// ascending, Z (device, n x n column-major) eigenvectors.  work: 2*n*n + ...
+// ascending, Z (device, n x n column-major) eigenvectors.  Sweeps of the
+// block method until the off-diagonal norm is below 1e-15 of the norm.
 int syev_jacobi(int n, double* A, double* w, double* Z, int max_sweeps, cudaStream_t st,
                 int* sweeps_out) {
   if (n <= 0) return RS_OK;
-  const int ne = n + (n & 1);
-  const int npair = ne / 2;
-  double* V = nullptr;
-  Rot* rot = nullptr;
-  double* od = nullptr;
-  RS_CUDA(cudaMallocAsync((void**)&V, sizeof(double) * (size_t)n * n, st));
-  RS_CUDA(cudaMallocAsync((void**)&rot, sizeof(Rot) * npair, st));
-  const long oblk = tree_chunks((long)n * n);
-  RS_CUDA(cudaMallocAsync((void**)&od, sizeof(double) * (2 + 2 * oblk), st));
-  k_eye<<<div_up((long)n * n, 256), 256, 0, st>>>(V, n);
-  int sweep = 0, rc = RS_OK;
-  // the cooperative grid: one 1024-thread block per SM (fewer blocks make
-  // the grid barrier cheaper), at most one block per 1024 work items
-  int dev = 0, nsm = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jac_sweep, kJacThreads, 0);
-  const long nwork = (long)npair * npair + (long)npair * n;
-  const unsigned coop_grid = (unsigned)std::max(
-      1L, std::min((long)nsm * std::min(std::max(per_sm, 1), 1),
-                   (nwork + kJacThreads - 1) / kJacThreads));
-  for (; sweep < max_sweeps; ++sweep) {
+  const int nb = (n + JB - 1) / JB;
+  const int nbe = std::max(2, nb + (nb & 1));
+  const int np = nbe * JB;
+  const int npair = nbe / 2;
+  const long nn = (long)np * np;
+  double *Ap = nullptr, *V = nullptr, *Qb = nullptr, *od = nullptr;
+  const long oblk = tree_chunks(nn);
+  RS_CUDA(cudaMallocAsync((void**)&Ap, sizeof(double) * (2 * nn + (long)npair * JB2 * JB2 +
+                                                          2 + 2 * oblk), st));
+  V = Ap + nn;
+  Qb = V + nn;
+  od = Qb + (long)npair * JB2 * JB2;
+  k_bjac_pad<<<div_up(nn, 256), 256, 0, st>>>(A, n, np, Ap, V);
+  const int usm = 3 * JB2 * JLD * (int)sizeof(double), ssm = 2 * JB2 * JLD * (int)sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(k_bjac_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       usm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_bjac_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, ssm);
+  int sweep = 0, rc = e == cudaSuccess ? RS_OK : cuda_status(e, "k_bjac_update");
+  const unsigned nupd = (unsigned)(npair * (npair - 1) / 2 + npair * npair);
+  for (; rc == RS_OK && sweep < max_sweeps; ++sweep) {
     double h[2];
-    k_offdiag_part<<<(unsigned)oblk, kTreeLanes, 0, st>>>(A, n, od + 2);
+    k_offdiag_part<<<(unsigned)oblk, kTreeLanes, 0, st>>>(Ap, np, od + 2);
     k_offdiag_fold<<<1, kTreeLanes, 0, st>>>(oblk, od + 2, od);
-    cudaError_t e = cudaMemcpyAsync(h, od, sizeof(h), cudaMemcpyDeviceToHost, st);
+    e = cudaMemcpyAsync(h, od, sizeof(h), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { rc = cuda_status(e, "syev_jacobi"); break; }
     if (h[0] == 0.0 || h[0] <= 1e-30 * h[1]) break;
-    {
-      int nn = n, nne = ne;
-      void* args[] = {&A, &V, &nn, &nne, &rot};
-      e = cudaLaunchCooperativeKernel((void*)k_jac_sweep, coop_grid, kJacThreads, args, 0, st);
+    for (int r = 0; r < nbe - 1; ++r) {
+      k_bjac_solve<<<npair, kBjThreads, ssm, st>>>(Ap, np, nbe, r, Qb);
+      k_bjac_update<<<nupd, kBjThreads, usm, st>>>(Ap, V, np, nbe, r, Qb);
     }
-    if (e != cudaSuccess) { rc = cuda_status(e, "k_jac_sweep"); break; }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) rc = cuda_status(e, "k_bjac");
   }
   if (rc == RS_OK && sweep >= max_sweeps) rc = fail(RS_ENUMERIC, "syev: Jacobi did not converge");
   if (rc == RS_OK) {
-    k_sort_eig<<<div_up(n, 128), 128, 0, st>>>(A, V, n, w, Z);
-    cudaError_t e = cudaGetLastError();
+    k_sort_eig<<<div_up(n, 128), 128, 0, st>>>(Ap, V, n, np, w, Z);
+    e = cudaGetLastError();
     if (e != cudaSuccess) rc = cuda_status(e, "k_sort_eig");
   }
-  cudaFreeAsync(V, st);
-  cudaFreeAsync(rot, st);
-  cudaFreeAsync(od, st);
+  cudaFreeAsync(Ap, st);
   if (sweeps_out) *sweeps_out = sweep;
   return rc;
 }

@@ -162,7 +162,7 @@ def test_scf_diag_fp32_converges_like_fp64(system, oracle):
 def test_syev_matches_lapack(cuda, built_lib):
     from rspacedist_b200 import kukan as K
     rng = np.random.default_rng(2)
-    for n in (1, 2, 7, 20, 161):
+    for n in (1, 2, 7, 20, 97, 161, 300):
         a = rng.standard_normal((n, n))
         a = a + a.T
         w, Z, sw = K.syev(T(a))
