@@ -331,6 +331,33 @@ def run_reference(args):
     }), flush=True)
 
 
+def run_diag_profile(dtype_name):
+    """One scf_diag call (RR + DIIS) on the Si512 cell with 1100 smooth start
+    bands, run once to warm the memory pool and once more between
+    cudaProfilerStart/Stop, so that `ncu --profile-from-start off` lists the
+    kernels of exactly one call.  Prints the wall time of the profiled call."""
+    import torch
+    from rspacedist_b200 import kukan as K, lib, scf
+    cell = make_cell()
+    g = K.Geometry(cell)
+    dt = torch.float32 if dtype_name == "f32" else torch.float64
+    veff = torch.tensor(scf.model_local_potential(cell), device="cuda").to(dt)
+    dij = torch.tensor(cell.dij, device="cuda")
+    sss = torch.tensor(cell.sss, device="cuda")
+    b = K.Bands(g, scf.smooth_start_bands_device(cell.shape, NB, 0, dt), sss)
+    K.orthogonalization(b, 1)
+    prm = lib.solver_prm(ncgscf=0)
+    K.scf_diag(b, veff, dij, 1, prm)
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    t = time.perf_counter()
+    K.scf_diag(b, veff, dij, 2, prm)
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
+    print(json.dumps({"scf_diag": dtype_name, "seconds": round(time.perf_counter() - t, 4),
+                      "bands": NB, "grid": [GRID] * 3}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -342,8 +369,12 @@ def main():
                     help="bands per sweep (default 1100; smaller values for profiling only)")
     ap.add_argument("--scf-iters", type=int, default=3,
                     help="SCF iterations timed per path on the Si512 cell (0 skips the leg)")
+    ap.add_argument("--diag-profile", choices=["f32", "f64"],
+                    help="run one profiled scf_diag call of the SCF leg and exit")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.diag_profile:
+        run_diag_profile(args.diag_profile)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

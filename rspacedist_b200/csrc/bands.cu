@@ -30,6 +30,9 @@ int launch_gather(const rs_geom* g, const double* mat, const double* rp, const T
 int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
                          const double* rp, const float* psi, float* hpsi, int nb,
                          cudaStream_t st);
+bool spsi_f32_fast_ok(const rs_geom* g);
+int launch_spsi_f32_fast(const rs_geom* g, const double* sss, const double* rp, const float* psi,
+                         float* out, int nb, cudaStream_t st);
 int gram_f32(int m, int n, long K, const float* A, long lda, const float* B, long ldb,
              double alpha, double* C, long ldc, int sym, cudaStream_t st);
 int gram_f64(int m, int n, long K, const double* A, long lda, const double* B, long ldb,
@@ -614,6 +617,10 @@ struct BandCtx {
     if (!sss) {
       if (out != x) RS_CUDA(cudaMemcpyAsync(out, x, sizeof(T) * N * nb, cudaMemcpyDeviceToDevice, st));
       return RS_OK;
+    }
+    if constexpr (sizeof(T) == 4) {
+      if (spsi_f32_fast_ok(g))
+        return launch_spsi_f32_fast(g, sss, r, (const float*)x, (float*)out, nb, st);
     }
     return launch_gather<T, 2>(g, sss, r, x, nullptr, out, nb, st);
   }

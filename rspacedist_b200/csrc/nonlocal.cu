@@ -258,8 +258,15 @@ extern "C" int rs_spsi_f64(const rs_geom* g, const double* sss, const double* rp
   RS_NEED_G("rs_spsi_f64");
   return rs::launch_gather<double, 2>(g, sss, rp, psi, nullptr, spsi, nb, rs::as_stream(stream));
 }
+namespace rs {
+bool spsi_f32_fast_ok(const rs_geom* g);
+int launch_spsi_f32_fast(const rs_geom* g, const double* sss, const double* rp, const float* psi,
+                         float* out, int nb, cudaStream_t st);
+}  // namespace rs
 extern "C" int rs_spsi_f32(const rs_geom* g, const double* sss, const double* rp,
                            const float* psi, float* spsi, int nb, void* stream) {
   RS_NEED_G("rs_spsi_f32");
+  if (rs::spsi_f32_fast_ok(g))
+    return rs::launch_spsi_f32_fast(g, sss, rp, psi, spsi, nb, rs::as_stream(stream));
   return rs::launch_gather<float, 2>(g, sss, rp, psi, nullptr, spsi, nb, rs::as_stream(stream));
 }

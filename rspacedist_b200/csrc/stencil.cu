@@ -27,26 +27,43 @@ __global__ void k_kslaplacian(StencilArgs<T> s, const T* __restrict__ psi,
   out[(long)b * N + p] = acc;
 }
 
-// ksprecondition (ksprecondition8f.F90:8-39).
+// ksprecondition (ksprecondition8f.F90:8-39).  One block per run of kPrecRows
+// x-rows of one band: the row pointers and their periodic neighbours are set
+// up once, threads walk x with branch wraps (no integer division per point).
+constexpr int kPrecRows = 4;
 template <class T>
 __global__ void k_precondition(int nx, int ny, int nz, const T* __restrict__ in,
                                T* __restrict__ out, int nb) {
   const long N = (long)nx * ny * nz;
-  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int b = blockIdx.y;
-  if (p >= N || b >= nb) return;
-  const int ix = (int)(p % nx), iy = (int)((p / nx) % ny), iz = (int)(p / ((long)nx * ny));
   const T* v = in + (long)b * N;
+  T* o = out + (long)b * N;
   const T c = (T)(1.0 / 12.0), h = (T)0.5;
-  const long row = ((long)iz * ny + iy) * nx;
-  T t = c * v[row + wrapi(ix - 1, nx)];
-  t = fma(c, v[((long)iz * ny + wrapi(iy - 1, ny)) * nx + ix], t);
-  t = fma(c, v[(wrapi(iz - 1, nz) * ny + iy) * nx + ix], t);
-  t = fma(h, v[p], t);
-  t = fma(c, v[(wrapi(iz + 1, nz) * ny + iy) * nx + ix], t);
-  t = fma(c, v[((long)iz * ny + wrapi(iy + 1, ny)) * nx + ix], t);
-  t = fma(c, v[row + wrapi(ix + 1, nx)], t);
-  out[(long)b * N + p] = t;
+  const long nrow = (long)ny * nz;
+  for (int r = 0; r < kPrecRows; ++r) {
+    const long row = (long)blockIdx.x * kPrecRows + r;
+    if (row >= nrow) return;
+    const int iy = (int)(row % ny), iz = (int)(row / ny);
+    const int iym = iy == 0 ? ny - 1 : iy - 1, iyp = iy == ny - 1 ? 0 : iy + 1;
+    const int izm = iz == 0 ? nz - 1 : iz - 1, izp = iz == nz - 1 ? 0 : iz + 1;
+    const T* r0 = v + row * nx;
+    const T* rym = v + ((long)iz * ny + iym) * nx;
+    const T* ryp = v + ((long)iz * ny + iyp) * nx;
+    const T* rzm = v + ((long)izm * ny + iy) * nx;
+    const T* rzp = v + ((long)izp * ny + iy) * nx;
+    T* orow = o + row * nx;
+    for (int ix = threadIdx.x; ix < nx; ix += blockDim.x) {
+      const int ixm = ix == 0 ? nx - 1 : ix - 1, ixp = ix == nx - 1 ? 0 : ix + 1;
+      T t = c * r0[ixm];
+      t = fma(c, rym[ix], t);
+      t = fma(c, rzm[ix], t);
+      t = fma(h, r0[ix], t);
+      t = fma(c, rzp[ix], t);
+      t = fma(c, ryp[ix], t);
+      t = fma(c, r0[ixp], t);
+      orow[ix] = t;
+    }
+  }
 }
 
 // scf_hartee_laplacian (scf_hartree8f.F90:949-1004): the x pass starts from
@@ -147,8 +164,10 @@ int launch_kslaplacian(const rs_geom* g, const T* psi, const T* veff, T* out, in
 template <class T>
 int launch_precondition(const rs_geom* g, const T* in, T* out, int nb, cudaStream_t st) {
   if (nb <= 0) return RS_OK;
-  dim3 grid(div_up(g->N, 256), nb);
-  k_precondition<T><<<grid, 256, 0, st>>>(g->nx, g->ny, g->nz, in, out, nb);
+  const long nrow = (long)g->ny * g->nz;
+  const int thr = g->nx >= 128 ? 128 : (g->nx + 31) / 32 * 32;
+  dim3 grid((unsigned)div_up(nrow, kPrecRows), nb);
+  k_precondition<T><<<grid, thr, 0, st>>>(g->nx, g->ny, g->nz, in, out, nb);
   RS_LAUNCH_CHECK("k_precondition");
   return RS_OK;
 }
