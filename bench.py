@@ -65,54 +65,93 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+    """SM clock, its maximum, power and the clock-event reasons of this
+    process's GPU, read through NVML every 5 ms while the timed region runs
+    (nvidia-smi every 200 ms when NVML is not importable).  Reads only."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index=0):
         self.index = index
-        self.rows = []
+        self.samples = []  # (sm_mhz, max_mhz, set of reasons)
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+        h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        return pynvml, h
 
     def __enter__(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self.t = threading.Thread(target=self._poll_nvml, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t = threading.Thread(target=self._read_smi, daemon=True)
             self.t.start()
         except Exception:
             self.proc = None
         return self
 
-    def _read(self):
+    def _poll_nvml(self):
+        nv, h = self.nvml
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self.stop.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = get_reasons(h)
+                self.samples.append((sm, mx, {n for n, b in zip(self.NAMES, bits) if r & b}))
+            except Exception:
+                pass
+            self.stop.wait(0.005)
+
+    def _read_smi(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            r = [x.strip() for x in line.split(",")]
+            if len(r) >= 9 and r[1].replace(".", "").isdigit() and r[2].replace(".", "").isdigit():
+                self.samples.append((float(r[1]), float(r[2]),
+                                     {n for n, v in zip(self.NAMES, r[5:9])
+                                      if v.lower() == "active"}))
 
     def __exit__(self, *exc):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.nvml or self.proc:
+            self.t.join(timeout=5)
 
     def summary(self):
-        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm = [x[0] for x in self.samples]
         reasons = set()
-        for r in self.rows:
-            if len(r) >= 9:
-                for nm, v in zip(names, r[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(nm)
+        for x in self.samples:
+            reasons |= x[2]
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+                "sm_max_mhz": max(x[1] for x in self.samples) if sm else None,
+                "reasons": sorted(reasons), "samples": len(self.samples),
+                "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 def run_gpu(args):
@@ -358,6 +397,55 @@ def run_diag_profile(dtype_name):
                       "bands": NB, "grid": [GRID] * 3}), flush=True)
 
 
+def run_gemm_profile(npts):
+    """The subspace contractions of the Rayleigh-Ritz step at the Si512 band
+    count: Psi^T H Psi (rs_gram_f32, 1100 x 1100 over npts points) and the
+    rotation Psi Z (rs_rotate_f32), random FP32 operands, each timed with CUDA
+    events after one warm call; the error is against FP64 torch products.
+    Prints one JSON line; the flop counts are the algorithmic 2 M^2 npts."""
+    import ctypes as C
+    import torch
+    from rspacedist_b200 import lib
+    lib.load()
+    M = NB
+    p = lambda t: C.c_void_p(t.data_ptr())
+    s = lambda: C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    A = torch.randn((M, npts), generator=g, device="cuda", dtype=torch.float32)
+    B = torch.randn((M, npts), generator=g, device="cuda", dtype=torch.float32)
+    G = torch.empty((M, M), dtype=torch.float64, device="cuda")
+    Z = torch.randn((M, M), generator=g, device="cuda", dtype=torch.float64) / M ** 0.5
+    Y = torch.empty((M, npts), dtype=torch.float32, device="cuda")
+
+    def ev(fn, n=3):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / n
+
+    flop = 2.0 * M * M * npts
+    out = {"gemm_profile": {"bands": M, "points": npts}}
+    tg = ev(lambda: lib.call("rs_gram_f32", M, M, npts, p(A), npts, p(B), npts, 1.0, p(G), M,
+                             0, s()))
+    ref = (A.double() @ B.double().T).T
+    out["gram_ms"] = round(tg, 3)
+    out["gram_tflops"] = round(flop / tg / 1e9, 1)
+    out["gram_rel_err"] = float((G - ref).abs().max() / ref.abs().max())
+    del ref
+    tr = ev(lambda: lib.call("rs_rotate_f32", npts, M, M, p(A), npts, p(Z), M, p(Y), npts, s()))
+    ref = Z @ A.double()
+    out["rotate_ms"] = round(tr, 3)
+    out["rotate_tflops"] = round(flop / tr / 1e9, 1)
+    out["rotate_rel_err"] = float((Y.double() - ref).abs().max() / ref.abs().max())
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -371,9 +459,13 @@ def main():
                     help="SCF iterations timed per path on the Si512 cell (0 skips the leg)")
     ap.add_argument("--diag-profile", choices=["f32", "f64"],
                     help="run one profiled scf_diag call of the SCF leg and exit")
+    ap.add_argument("--gemm-profile", type=int, metavar="POINTS",
+                    help="time the tensor-core Gram and rotation at 1100 bands x POINTS and exit")
     args = ap.parse_args()
     if args.diag_profile:
         run_diag_profile(args.diag_profile)
+    elif args.gemm_profile:
+        run_gemm_profile(args.gemm_profile)
     elif args.impl == "reference":
         run_reference(args)
     else:
