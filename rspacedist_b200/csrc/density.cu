@@ -130,68 +130,137 @@ static_assert(sizeof(CgScalars) <= 16 * sizeof(double), "CG scalars fit the work
 
 constexpr int kCgBatch = 16;
 
-__device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
-// -1/2 lap v at (ix, iy, iz) = point p, in k_hartree_lap's order (x with the
-// diagonal, y, z), NF fixed at compile time
-template <int NF>
-__device__ __forceinline__ double hlap_at(int nx, int ny, int nz, const HartreeCoefs& c,
-                                          const double* __restrict__ v, int p, int ix, int iy,
-                                          int iz) {
-  const int pl = nx * ny;
-  const int row = p - ix;
-  const int col = p - iz * pl;  // iy*nx + ix
-  double acc = c.cx[NF] * __ldg(v + row + wrap1(ix - NF, nx));
-#pragma unroll
-  for (int m = NF - 1; m >= 1; --m) acc = fma(c.cx[m], __ldg(v + row + wrap1(ix - m, nx)), acc);
-  acc = fma(c.diag, __ldg(v + p), acc);
-#pragma unroll
-  for (int m = 1; m <= NF; ++m) acc = fma(c.cx[m], __ldg(v + row + wrap1(ix + m, nx)), acc);
-  const int zb = iz * pl + ix;
-#pragma unroll
-  for (int m = NF; m >= 1; --m) acc = fma(c.cy[m], __ldg(v + zb + wrap1(iy - m, ny) * nx), acc);
-#pragma unroll
-  for (int m = 1; m <= NF; ++m) acc = fma(c.cy[m], __ldg(v + zb + wrap1(iy + m, ny) * nx), acc);
-#pragma unroll
-  for (int m = NF; m >= 1; --m) acc = fma(c.cz[m], __ldg(v + wrap1(iz - m, nz) * pl + col), acc);
-#pragma unroll
-  for (int m = 1; m <= NF; ++m) acc = fma(c.cz[m], __ldg(v + wrap1(iz + m, nz) * pl + col), acc);
-  return acc;
+// ap = A p by a z-march, in k_hartree_lap's multiply-add order (x terms from
+// the first product, then y, then z; scf_hartree8f.F90:949-1004).  A CTA owns a
+// 32 x 16 tile of an xy plane for a run of z planes; each thread one point.
+//  * halo'd planes (the tile plus NF points on each side in x and y) are
+//    copied into a ring of hz_ring(NF) shared-memory slots with 8-byte
+//    cp.async, HZ_AHEAD planes ahead of use; x and y terms read the ring;
+//  * the z terms come from a register queue of the thread's own column
+//    (planes z-NF .. z+NF), so each plane crosses HBM about once;
+//  * one __syncthreads per plane orders the ring reuse.
+// The staging index of every element is computed once with a full modulo,
+// so any grid of at least one point per axis is handled.
+constexpr int HZ_TX = 32, HZ_TY = 16, HZ_THREADS = HZ_TX * HZ_TY, HZ_AHEAD = 7;
+__host__ __device__ constexpr int hz_ring(int nf) { return nf + HZ_AHEAD + 1; }
+__host__ __device__ constexpr int hz_plane(int nf) { return (HZ_TX + 2 * nf) * (HZ_TY + 2 * nf); }
+constexpr int HZ_STAGE_MAX = 4;  // staged elements per thread (hz_plane(6) = 44 * 28 = 1232)
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit_hz() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait_hz() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ int wrapm(long i, int n) {
+  long r = i % n;
+  return (int)(r < 0 ? r + n : r);
 }
 
-// ap = A p and the chunk sums of p.ap.  A thread's 16 points are kTreeLanes
-// apart: their coordinates are stepped forward instead of divided out.
 template <int NF>
-__global__ void __launch_bounds__(kTreeLanes) k_cg_lap_pap(int nx, int ny, int nz,
-                                                           HartreeCoefs c,
-                                                           const double* __restrict__ p,
-                                                           double* __restrict__ ap,
-                                                           double* __restrict__ part,
-                                                           const CgScalars* __restrict__ s) {
+__global__ void __launch_bounds__(HZ_THREADS, 2) k_hlap_zmarch(int nx, int ny, int nz,
+                                                               int zchunk, HartreeCoefs c,
+                                                               const double* __restrict__ p,
+                                                               double* __restrict__ ap,
+                                                               const CgScalars* __restrict__ s) {
+  if (s->done) return;
+  constexpr int HX = HZ_TX + 2 * NF, HY = HZ_TY + 2 * NF, PL = HX * HY, RING = hz_ring(NF);
+  constexpr int NST = (PL + HZ_THREADS - 1) / HZ_THREADS;
+  static_assert(NST <= HZ_STAGE_MAX, "staging slots");
+  extern __shared__ double hz_sm[];  // [RING][HY][HX]
+  const int tid = threadIdx.x, tx = tid % HZ_TX, ty = tid / HZ_TX;
+  const int ntx = (nx + HZ_TX - 1) / HZ_TX, nty = (ny + HZ_TY - 1) / HZ_TY;
+  const int tile = blockIdx.x % (ntx * nty), zc = blockIdx.x / (ntx * nty);
+  const int x0 = (tile % ntx) * HZ_TX, y0 = (tile / ntx) * HZ_TY;
+  const int zs = zc * zchunk, ze = min(zs + zchunk, nz);
+  const long plane = (long)nx * ny;
+  const int gx = x0 + tx, gy = y0 + ty;
+  const bool active = gx < nx && gy < ny;
+  const long own = active ? (long)gy * nx + gx : 0;
+  // in-plane source offsets of this thread's staged elements (the same every plane)
+  int soff[NST], doff[NST];
+#pragma unroll
+  for (int k = 0; k < NST; ++k) {
+    const int e = tid + k * HZ_THREADS;
+    if (e < PL) {
+      const int r = e / HX, q = e % HX;
+      soff[k] = (int)((long)wrapm(y0 - NF + r, ny) * nx + wrapm(x0 - NF + q, nx));
+      doff[k] = e;
+    } else {
+      soff[k] = -1;
+      doff[k] = 0;
+    }
+  }
+  // planes z in [zs - NF, ze + NF + HZ_AHEAD); the ring slot of plane z is
+  // (z - zs + NF) mod RING, kept as a running counter
+  auto wrapz = [&](int z) {
+    while (z < 0) z += nz;
+    while (z >= nz) z -= nz;
+    return z;
+  };
+  auto slot = [&](int z) { return (z - zs + NF) % RING; };
+  auto stage = [&](int z) {
+    const double* src = p + (long)wrapz(z) * plane;
+    double* dst = hz_sm + slot(z) * PL;
+#pragma unroll
+    for (int k = 0; k < NST; ++k)
+      if (soff[k] >= 0) cp_async8(dst + doff[k], src + soff[k]);
+    cp_commit_hz();
+  };
+  double q[2 * NF + 1];  // q[k]: plane z-NF+k at (gx, gy)
+#pragma unroll
+  for (int k = 0; k < NF; ++k) q[k] = __ldg(p + (long)wrapz(zs - NF + k) * plane + own);
+#pragma unroll
+  for (int k = 0; k < NF + HZ_AHEAD; ++k) stage(zs + k);
+  const int lc = (ty + NF) * HX + tx + NF;  // this thread's point in a staged plane
+  for (int z = zs; z < ze; ++z) {
+    cp_wait_hz<HZ_AHEAD - 1>();  // planes up to z+NF have landed (this thread's copies)
+    __syncthreads();             // ... everyone's; plane z-1's slot is free
+    stage(z + NF + HZ_AHEAD);
+    if (z == zs) {
+#pragma unroll
+      for (int k = 0; k < NF; ++k) q[NF + k] = hz_sm[slot(zs + k) * PL + lc];
+    }
+    q[2 * NF] = hz_sm[slot(z + NF) * PL + lc];
+    const double* cur = hz_sm + slot(z) * PL;
+    double acc = c.cx[NF] * cur[lc - NF];
+#pragma unroll
+    for (int m = NF - 1; m >= 1; --m) acc = fma(c.cx[m], cur[lc - m], acc);
+    acc = fma(c.diag, cur[lc], acc);
+#pragma unroll
+    for (int m = 1; m <= NF; ++m) acc = fma(c.cx[m], cur[lc + m], acc);
+#pragma unroll
+    for (int m = NF; m >= 1; --m) acc = fma(c.cy[m], cur[lc - m * HX], acc);
+#pragma unroll
+    for (int m = 1; m <= NF; ++m) acc = fma(c.cy[m], cur[lc + m * HX], acc);
+#pragma unroll
+    for (int m = NF; m >= 1; --m) acc = fma(c.cz[m], q[NF - m], acc);
+#pragma unroll
+    for (int m = 1; m <= NF; ++m) acc = fma(c.cz[m], q[NF + m], acc);
+    if (active) ap[(long)z * plane + own] = acc;
+#pragma unroll
+    for (int k = 0; k < 2 * NF; ++k) q[k] = q[k + 1];
+  }
+  cp_wait_hz<0>();
+}
+
+// chunk sums of p.ap in the reduction tree's order, from the stored ap
+__global__ void __launch_bounds__(kTreeLanes) k_cg_pap(long N, const double* __restrict__ p,
+                                                       const double* __restrict__ ap,
+                                                       double* __restrict__ part,
+                                                       const CgScalars* __restrict__ s) {
   if (s->done) return;
   __shared__ double ws[8];
-  const int N = nx * ny * nz;
-  const int base = blockIdx.x * kTreeChunk + threadIdx.x;
-  int iz = base / (nx * ny);
-  int rem = base - iz * nx * ny;
-  int iy = rem / nx, ix = rem - iy * nx;
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
   double acc = 0.0;
-#pragma unroll 2
+#pragma unroll 4
   for (int k = 0; k < kTreePerLane; ++k) {
-    const int i = base + k * kTreeLanes;
-    if (i < N) {
-      const double a = hlap_at<NF>(nx, ny, nz, c, p, i, ix, iy, iz);
-      ap[i] = a;
-      acc = fma(p[i], a, acc);
-    }
-    ix += kTreeLanes;
-    while (ix >= nx) {
-      ix -= nx;
-      if (++iy == ny) {
-        iy = 0;
-        ++iz;
-      }
-    }
+    const long i = base + (long)k * kTreeLanes;
+    if (i < N) acc = fma(p[i], ap[i], acc);
   }
   const double t = tree_fold256(acc, ws);
   if (threadIdx.x == 0) part[blockIdx.x] = t;
@@ -307,6 +376,22 @@ __global__ void k_cg_dir(long N, const CgScalars* __restrict__ s, const double* 
   p[i] = fma(s->beta, p[i], r[i]);
 }
 
+constexpr size_t hz_smem(int nf) { return sizeof(double) * hz_ring(nf) * hz_plane(nf); }
+
+// shared-memory limits of the z-march kernels (above 48 KB for nfh >= 4)
+int hlap_zmarch_attr(int nfh) {
+  cudaError_t e = cudaSuccess;
+  switch (nfh) {
+    case 1: e = cudaFuncSetAttribute(k_hlap_zmarch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz_smem(1)); break;
+    case 2: e = cudaFuncSetAttribute(k_hlap_zmarch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz_smem(2)); break;
+    case 3: e = cudaFuncSetAttribute(k_hlap_zmarch<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz_smem(3)); break;
+    case 4: e = cudaFuncSetAttribute(k_hlap_zmarch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz_smem(4)); break;
+    case 5: e = cudaFuncSetAttribute(k_hlap_zmarch<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz_smem(5)); break;
+    default: e = cudaFuncSetAttribute(k_hlap_zmarch<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz_smem(6)); break;
+  }
+  return e == cudaSuccess ? RS_OK : cuda_status(e, "k_hlap_zmarch");
+}
+
 int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double zmax,
                double epsvh, int ncgmin, int ncgmax, int ncgres, const double* rho, double* vh,
                double* work, int* iters, double* dp_out, cudaStream_t st) {
@@ -334,16 +419,22 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
   if ((rc = launch_hartree_lap(nx, ny, nz, nfh, hc, vh, ap, st))) return rc;
   k_cg_init<<<gN, 256, 0, st>>>(N, b, ap, avhs, r, p);
   if ((rc = tree_dot<double>(N, r, r, &sc->r1r, part, st))) return rc;
+  // A p by the z-march stencil, then the p.Ap chunk sums (tree order)
+  const int ztiles = (int)(div_up(nx, HZ_TX) * div_up(ny, HZ_TY));
+  const int nzc = (nz + 63) / 64;
+  const int zchunk = (nz + nzc - 1) / nzc;
+  const unsigned gz = (unsigned)(ztiles * nzc);
+  if ((rc = hlap_zmarch_attr(nfh))) return rc;
   auto lap = [&](const double* x, double* ax) {
-    const unsigned gb = (unsigned)nblk;
     switch (nfh) {
-      case 1: k_cg_lap_pap<1><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
-      case 2: k_cg_lap_pap<2><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
-      case 3: k_cg_lap_pap<3><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
-      case 4: k_cg_lap_pap<4><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
-      case 5: k_cg_lap_pap<5><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
-      default: k_cg_lap_pap<6><<<gb, kTreeLanes, 0, st>>>(nx, ny, nz, hc, x, ax, part, sc); break;
+      case 1: k_hlap_zmarch<1><<<gz, HZ_THREADS, hz_smem(1), st>>>(nx, ny, nz, zchunk, hc, x, ax, sc); break;
+      case 2: k_hlap_zmarch<2><<<gz, HZ_THREADS, hz_smem(2), st>>>(nx, ny, nz, zchunk, hc, x, ax, sc); break;
+      case 3: k_hlap_zmarch<3><<<gz, HZ_THREADS, hz_smem(3), st>>>(nx, ny, nz, zchunk, hc, x, ax, sc); break;
+      case 4: k_hlap_zmarch<4><<<gz, HZ_THREADS, hz_smem(4), st>>>(nx, ny, nz, zchunk, hc, x, ax, sc); break;
+      case 5: k_hlap_zmarch<5><<<gz, HZ_THREADS, hz_smem(5), st>>>(nx, ny, nz, zchunk, hc, x, ax, sc); break;
+      default: k_hlap_zmarch<6><<<gz, HZ_THREADS, hz_smem(6), st>>>(nx, ny, nz, zchunk, hc, x, ax, sc); break;
     }
+    k_cg_pap<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, x, ax, part, sc);
   };
   CgScalars hs;
   hs.done = 0;
