@@ -519,12 +519,13 @@ def run_hartree_profile(n):
     K.scf_hartree((n, n, n), 4, xm, rho_d, vh, 1e-12, ncgmax=50)
     torch.cuda.synchronize()
     vh.zero_()
-    t = time.perf_counter()
-    it, dp = K.scf_hartree((n, n, n), 4, xm, rho_d, vh, 1e-12)
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        t = time.perf_counter()
+        it, dp = K.scf_hartree((n, n, n), 4, xm, rho_d, vh, 1e-12)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t
     print(json.dumps({"hartree_profile": {"grid": [n] * 3, "cell_bohr": a}, "iterations": it,
-                      "dp": dp, "ms": round(dt * 1e3, 2),
+                      "dp": dp, "ms": round(dt * 1e3, 2), "clocks": clk.summary(),
                       "us_per_iter": round(dt / it * 1e6, 1),
                       "gbs_at_88_bytes_per_point": round(88 * n ** 3 / (dt / it) / 1e9, 1)}),
           flush=True)

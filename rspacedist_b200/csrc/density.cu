@@ -248,6 +248,132 @@ __global__ void __launch_bounds__(HZ_THREADS, 2) k_hlap_zmarch(int nx, int ny, i
   cp_wait_hz<0>();
 }
 
+// The same z-march with two x-neighbouring points per thread, for even NF and
+// even nx: 16-byte staging copies and 16-byte shared loads (x terms of both
+// points from NF+1 double2 loads, y terms and the z queue as double2), about
+// half the instructions per point.  64 x 16 tiles, one CTA per SM.
+constexpr int HZ2_TX = 64, HZ2_TY = 16, HZ2_THREADS = (HZ2_TX / 2) * HZ2_TY, HZ2_AHEAD = 5;
+__host__ __device__ constexpr int hz2_ring(int nf) { return nf + HZ2_AHEAD + 1; }
+__host__ __device__ constexpr int hz2_plane(int nf) { return (HZ2_TX + 2 * nf) * (HZ2_TY + 2 * nf); }
+
+__device__ __forceinline__ void cp_async16_hz(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+template <int NF>
+__global__ void __launch_bounds__(HZ2_THREADS, 1) k_hlap_zmarch2(int nx, int ny, int nz,
+                                                                 int zchunk, HartreeCoefs c,
+                                                                 const double* __restrict__ p,
+                                                                 double* __restrict__ ap,
+                                                                 const CgScalars* __restrict__ s) {
+  static_assert(NF % 2 == 0, "double2 path needs an even halo");
+  if (s->done) return;
+  constexpr int HX = HZ2_TX + 2 * NF, HY = HZ2_TY + 2 * NF, PL = HX * HY, RING = hz2_ring(NF);
+  constexpr int PL2 = PL / 2, NST = (PL2 + HZ2_THREADS - 1) / HZ2_THREADS;
+  extern __shared__ double2 hz2_sm[];  // [RING][HY][HX / 2]
+  const int tid = threadIdx.x, tx = tid % (HZ2_TX / 2), ty = tid / (HZ2_TX / 2);
+  const int ntx = (nx + HZ2_TX - 1) / HZ2_TX, nty = (ny + HZ2_TY - 1) / HZ2_TY;
+  const int tile = blockIdx.x % (ntx * nty), zc = blockIdx.x / (ntx * nty);
+  const int x0 = (tile % ntx) * HZ2_TX, y0 = (tile / ntx) * HZ2_TY;
+  const int zs = zc * zchunk, ze = min(zs + zchunk, nz);
+  const long plane = (long)nx * ny;
+  const int gx = x0 + 2 * tx, gy = y0 + ty;
+  const bool active = gx < nx && gy < ny;  // nx even: gx + 1 < nx as well
+  const long own = active ? (long)gy * nx + gx : 0;
+  int soff[NST], doff[NST];
+#pragma unroll
+  for (int k = 0; k < NST; ++k) {
+    const int e = tid + k * HZ2_THREADS;  // double2 index in the staged plane
+    if (e < PL2) {
+      const int r = e / (HX / 2), q2 = e % (HX / 2);
+      soff[k] = (int)((long)wrapm(y0 - NF + r, ny) * nx + wrapm(x0 - NF + 2 * q2, nx));
+      doff[k] = e;
+    } else {
+      soff[k] = -1;
+      doff[k] = 0;
+    }
+  }
+  auto wrapz = [&](int z) {
+    while (z < 0) z += nz;
+    while (z >= nz) z -= nz;
+    return z;
+  };
+  auto slot = [&](int z) { return (z - zs + NF) % RING; };
+  auto stage = [&](int z) {
+    const double* src = p + (long)wrapz(z) * plane;
+    double2* dst = hz2_sm + slot(z) * PL2;
+#pragma unroll
+    for (int k = 0; k < NST; ++k)
+      if (soff[k] >= 0) cp_async16_hz(dst + doff[k], src + soff[k]);
+    cp_commit_hz();
+  };
+  double2 q[2 * NF + 1];
+#pragma unroll
+  for (int k = 0; k < NF; ++k)
+    q[k] = __ldg(reinterpret_cast<const double2*>(p + (long)wrapz(zs - NF + k) * plane + own));
+#pragma unroll
+  for (int k = 0; k < NF + HZ2_AHEAD; ++k) stage(zs + k);
+  const int lc2 = (ty + NF) * (HX / 2) + tx + NF / 2;  // this thread's pair, double2 index
+  for (int z = zs; z < ze; ++z) {
+    cp_wait_hz<HZ2_AHEAD - 1>();
+    __syncthreads();
+    stage(z + NF + HZ2_AHEAD);
+    if (z == zs) {
+#pragma unroll
+      for (int k = 0; k < NF; ++k) q[NF + k] = hz2_sm[slot(zs + k) * PL2 + lc2];
+    }
+    q[2 * NF] = hz2_sm[slot(z + NF) * PL2 + lc2];
+    const double2* cur = hz2_sm + slot(z) * PL2;
+    double v[2 * NF + 2];  // x - NF .. x + NF + 1
+#pragma unroll
+    for (int k = 0; k <= NF; ++k) {
+      const double2 w = cur[lc2 - NF / 2 + k];
+      v[2 * k] = w.x;
+      v[2 * k + 1] = w.y;
+    }
+    double a0 = c.cx[NF] * v[0], a1 = c.cx[NF] * v[1];
+#pragma unroll
+    for (int m = NF - 1; m >= 1; --m) {
+      a0 = fma(c.cx[m], v[NF - m], a0);
+      a1 = fma(c.cx[m], v[NF + 1 - m], a1);
+    }
+    a0 = fma(c.diag, v[NF], a0);
+    a1 = fma(c.diag, v[NF + 1], a1);
+#pragma unroll
+    for (int m = 1; m <= NF; ++m) {
+      a0 = fma(c.cx[m], v[NF + m], a0);
+      a1 = fma(c.cx[m], v[NF + 1 + m], a1);
+    }
+#pragma unroll
+    for (int m = NF; m >= 1; --m) {
+      const double2 w = cur[lc2 - m * (HX / 2)];
+      a0 = fma(c.cy[m], w.x, a0);
+      a1 = fma(c.cy[m], w.y, a1);
+    }
+#pragma unroll
+    for (int m = 1; m <= NF; ++m) {
+      const double2 w = cur[lc2 + m * (HX / 2)];
+      a0 = fma(c.cy[m], w.x, a0);
+      a1 = fma(c.cy[m], w.y, a1);
+    }
+#pragma unroll
+    for (int m = NF; m >= 1; --m) {
+      a0 = fma(c.cz[m], q[NF - m].x, a0);
+      a1 = fma(c.cz[m], q[NF - m].y, a1);
+    }
+#pragma unroll
+    for (int m = 1; m <= NF; ++m) {
+      a0 = fma(c.cz[m], q[NF + m].x, a0);
+      a1 = fma(c.cz[m], q[NF + m].y, a1);
+    }
+    if (active) *reinterpret_cast<double2*>(ap + (long)z * plane + own) = make_double2(a0, a1);
+#pragma unroll
+    for (int k = 0; k < 2 * NF; ++k) q[k] = q[k + 1];
+  }
+  cp_wait_hz<0>();
+}
+
 // chunk sums of p.ap in the reduction tree's order, from the stored ap
 __global__ void __launch_bounds__(kTreeLanes) k_cg_pap(long N, const double* __restrict__ p,
                                                        const double* __restrict__ ap,
@@ -377,6 +503,7 @@ __global__ void k_cg_dir(long N, const CgScalars* __restrict__ s, const double* 
 }
 
 constexpr size_t hz_smem(int nf) { return sizeof(double) * hz_ring(nf) * hz_plane(nf); }
+constexpr size_t hz2_smem(int nf) { return sizeof(double) * hz2_ring(nf) * hz2_plane(nf); }
 
 // shared-memory limits of the z-march kernels (above 48 KB for nfh >= 4)
 int hlap_zmarch_attr(int nfh) {
@@ -388,6 +515,13 @@ int hlap_zmarch_attr(int nfh) {
     case 4: e = cudaFuncSetAttribute(k_hlap_zmarch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz_smem(4)); break;
     case 5: e = cudaFuncSetAttribute(k_hlap_zmarch<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz_smem(5)); break;
     default: e = cudaFuncSetAttribute(k_hlap_zmarch<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz_smem(6)); break;
+  }
+  if (e == cudaSuccess && nfh % 2 == 0) {
+    switch (nfh) {
+      case 2: e = cudaFuncSetAttribute(k_hlap_zmarch2<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz2_smem(2)); break;
+      case 4: e = cudaFuncSetAttribute(k_hlap_zmarch2<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz2_smem(4)); break;
+      default: e = cudaFuncSetAttribute(k_hlap_zmarch2<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz2_smem(6)); break;
+    }
   }
   return e == cudaSuccess ? RS_OK : cuda_status(e, "k_hlap_zmarch");
 }
@@ -420,12 +554,23 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
   k_cg_init<<<gN, 256, 0, st>>>(N, b, ap, avhs, r, p);
   if ((rc = tree_dot<double>(N, r, r, &sc->r1r, part, st))) return rc;
   // A p by the z-march stencil, then the p.Ap chunk sums (tree order)
-  const int ztiles = (int)(div_up(nx, HZ_TX) * div_up(ny, HZ_TY));
+  const bool pairs = nfh % 2 == 0 && nx % 2 == 0;
+  const int ztiles = pairs ? (int)(div_up(nx, HZ2_TX) * div_up(ny, HZ2_TY))
+                           : (int)(div_up(nx, HZ_TX) * div_up(ny, HZ_TY));
   const int nzc = (nz + 63) / 64;
   const int zchunk = (nz + nzc - 1) / nzc;
   const unsigned gz = (unsigned)(ztiles * nzc);
   if ((rc = hlap_zmarch_attr(nfh))) return rc;
   auto lap = [&](const double* x, double* ax) {
+    if (pairs) {
+      switch (nfh) {
+        case 2: k_hlap_zmarch2<2><<<gz, HZ2_THREADS, hz2_smem(2), st>>>(nx, ny, nz, zchunk, hc, x, ax, sc); break;
+        case 4: k_hlap_zmarch2<4><<<gz, HZ2_THREADS, hz2_smem(4), st>>>(nx, ny, nz, zchunk, hc, x, ax, sc); break;
+        default: k_hlap_zmarch2<6><<<gz, HZ2_THREADS, hz2_smem(6), st>>>(nx, ny, nz, zchunk, hc, x, ax, sc); break;
+      }
+      k_cg_pap<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, x, ax, part, sc);
+      return;
+    }
     switch (nfh) {
       case 1: k_hlap_zmarch<1><<<gz, HZ_THREADS, hz_smem(1), st>>>(nx, ny, nz, zchunk, hc, x, ax, sc); break;
       case 2: k_hlap_zmarch<2><<<gz, HZ_THREADS, hz_smem(2), st>>>(nx, ny, nz, zchunk, hc, x, ax, sc); break;
