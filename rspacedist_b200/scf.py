@@ -31,6 +31,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
+from . import checkpoint as CK
 from . import kukan as K
 from . import lib as L
 from .system import Cell
@@ -164,7 +165,16 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
             looplimit: int = 200, prm=None, nbrydn: int = 20, eta: float = 0.02,
             seed: int = 0, zval: float = 4.0, epsvh: float = 1e-12, vloc=None, rho0=None,
             psi0=None, log=None, profile: bool = False, smearing: bool = True,
-            tf: float = 3.0e-3) -> ScfResult:
+            tf: float = 3.0e-3, restart_dir: str | None = None,
+            save_dir: str | None = None) -> ScfResult:
+    """kukan's SCF loop (kukan8f.F90:513-680) over the C ABI.
+
+    restart_dir: start from kukan restart files there (wfc.00000.000 for the
+    bands, rho.00000 for the start density, vht.00000 for the Hartree warm
+    start; missing density or potential files fall back to the model start).
+    save_dir: write the same files after the last iteration (the last input
+    density as rho.*, the output density as r_o.*), as write_wf and
+    write_rhovht do."""
     dev = torch.device("cuda")
     g = K.Geometry(cell)
     N, shape = cell.N, cell.shape
@@ -172,7 +182,14 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
     h, xmax = cell.h, cell.xmax
     dvol = h[0] * h[1] * h[2]
     f64 = torch.float64
-    if psi0 is None:
+    rho_start = vh_start = None
+    if restart_dir is not None:
+        psi = torch.empty((M, N), dtype=dtype, device=dev)
+        CK.read_wf(restart_dir, M, shape, out=psi)
+        got = CK.read_rho(restart_dir, shape)
+        rho_start = None if got is None else got[0]
+        vh_start = CK.read_vht(restart_dir, shape)
+    elif psi0 is None:
         psi = smooth_start_bands_device(shape, M, seed, dtype)
     else:
         psi = torch.as_tensor(np.ascontiguousarray(psi0), device=dev).to(dtype)
@@ -183,10 +200,14 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
     occ[:nocc] = 2.0
     vloc_t = torch.tensor(model_local_potential(cell) if vloc is None else vloc, dtype=f64,
                           device=dev)
+    if rho_start is not None:
+        rho0 = rho_start
     rho_o = torch.tensor(atomic_density(cell, zval) if rho0 is None else rho0, dtype=f64,
                          device=dev)
     rho_i = torch.zeros(N, dtype=f64, device=dev)
     vh_d = torch.zeros(8 * N, dtype=f64, device=dev)
+    if vh_start is not None:
+        vh_d.copy_(torch.from_numpy(vh_start))
     veff64 = torch.empty(N, dtype=f64, device=dev)
     veff32 = torch.empty(N, dtype=torch.float32, device=dev) if dtype == torch.float32 else None
     veff = veff64 if veff32 is None else veff32
@@ -242,5 +263,10 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
     res.sval = np.array(b.sval)
     occ_h = occ.cpu().numpy()
     res.eband = float(np.sum(occ_h * res.sval))
+    if save_dir is not None:
+        CK.write_wf(save_dir, b.psi, res.sval, shape)
+        CK.write_rho(save_dir, rho_i, shape)
+        CK.write_rho(save_dir, rho_o, shape, name="r_o")
+        CK.write_vht(save_dir, vh_d, shape)
     mixer.close()
     return res

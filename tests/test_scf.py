@@ -29,3 +29,23 @@ def test_scf_matches_oracle(ref, dtype, tol_e, tol_band):
     assert res.converged, res.diff[-5:]
     np.testing.assert_allclose(np.sort(res.sval)[:16], r["sval"][:16], atol=tol_band)
     assert abs(res.eband - r["eband"]) / cell.natom < tol_e
+
+
+def test_scf_restart_files(ref, tmp_path):
+    """A converged run writes kukan's restart files (wfc, rho, r_o, vht); a
+    run restarted from them starts converged: its first charge difference is
+    already below the stopping rule, and its eigenvalues match."""
+    from rspacedist_b200 import checkpoint as CK, lib, scf
+    cell, r = ref
+    prm = lib.solver_prm(ncgscf=3)
+    a = scf.run_scf(cell, 20, 16, dtype=torch.float64, prm=prm, looplimit=100,
+                    psi0=scf.smooth_start_bands(cell.shape, 20, 0), save_dir=str(tmp_path))
+    assert a.converged
+    for name in ("wfc.00000.000", "rho.00000", "r_o.00000", "vht.00000"):
+        assert (tmp_path / name).exists(), name
+    sv, _ = CK.read_wf(str(tmp_path), 20, cell.shape)
+    assert np.array_equal(sv, a.sval)
+    b = scf.run_scf(cell, 20, 16, dtype=torch.float64, prm=lib.solver_prm(ncgscf=0),
+                    looplimit=3, restart_dir=str(tmp_path))
+    assert b.diff[0] < 1e-5, b.diff
+    np.testing.assert_allclose(np.sort(b.sval)[:16], np.sort(a.sval)[:16], atol=1e-6)
