@@ -531,6 +531,58 @@ def run_hartree_profile(n):
           flush=True)
 
 
+def run_batch_profile(ncell, nbands):
+    """H psi of a set of small independent cells (16 Si8 + 16 C8 by default,
+    20 bands each, grids 22^3-36^3): a loop of single-cell rs_hpsi_f32 calls
+    against one persistent rs_hpsi_batch launch, direct and as a CUDA graph
+    replay, each timed with CUDA events on a side stream over 20 repetitions.
+    Prints one JSON line."""
+    import torch
+    from rspacedist_b200 import kukan as K, system as S
+    cells = S.small_cell_set(ncell)
+    geoms = [K.Geometry(c) for c in cells]
+    veff = [torch.tensor(S.smooth_veff(c, i), dtype=torch.float32, device="cuda")
+            for i, c in enumerate(cells)]
+    dij = [torch.tensor(c.dij, dtype=torch.float64, device="cuda") for c in cells]
+    psi = [torch.tensor(S.random_bands(c, nbands, i), dtype=torch.float32, device="cuda")
+           for i, c in enumerate(cells)]
+    rp = [K.nonlocaloperation_01(g, p) for g, p in zip(geoms, psi)]
+    out = [torch.empty_like(p) for p in psi]
+    plan = K.HpsiBatch(geoms, [nbands] * ncell)
+    plan.set(veff, dij, rp, psi, out)
+    st = torch.cuda.Stream()
+    reps = 20
+
+    def timed(fn):
+        with torch.cuda.stream(st):
+            for _ in range(3):
+                fn()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            for _ in range(reps):
+                fn()
+            b.record(st)
+        st.synchronize()
+        return a.elapsed_time(b) / reps
+
+    def loop():
+        for g, v, d, r, p, o in zip(geoms, veff, dij, rp, psi, out):
+            K.hpsi(g, v, d, r, p, out=o)
+
+    t_loop = timed(loop)
+    t_batch = timed(lambda: plan.run(graph=False))
+    t_graph = timed(lambda: plan.run(graph=True))
+    pts = sum(c.N for c in cells) * nbands
+    print(json.dumps({"batch_profile": {"cells": ncell, "bands": nbands,
+                                        "grids": sorted({c.shape[0] for c in cells}),
+                                        "band_points": pts},
+                      "per_cell_calls_ms": round(t_loop, 4), "batched_ms": round(t_batch, 4),
+                      "batched_graph_ms": round(t_graph, 4),
+                      "speedup_graph_vs_calls": round(t_loop / t_graph, 2),
+                      "autotuned": plan.info()}), flush=True)
+    plan.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -548,8 +600,13 @@ def main():
                     help="time the tensor-core Gram and rotation at 1100 bands x POINTS and exit")
     ap.add_argument("--hartree-profile", type=int, metavar="N",
                     help="time the Hartree CG solve on an N^3 dense grid and exit")
+    ap.add_argument("--batch-profile", type=int, metavar="CELLS",
+                    help="time H*psi of CELLS small cells, per-cell calls vs one batched "
+                         "launch, and exit")
     args = ap.parse_args()
-    if args.hartree_profile:
+    if args.batch_profile:
+        run_batch_profile(args.batch_profile, 20)
+    elif args.hartree_profile:
         run_hartree_profile(args.hartree_profile)
     elif args.diag_profile:
         run_diag_profile(args.diag_profile)

@@ -292,6 +292,33 @@ int rs_hartree_cg_noalloc(int nx, int ny, int nz, int nfh, double xmax, double y
                           double zmax, double epsvh, int ncgmin, int ncgmax, int ncgres,
                           const double* rho, double* vh, int* iters, double* dp, void* stream);
 
+/* ---- many small cells in one launch --------------------------------------- */
+/* H psi (FP32 bands) of ncell independent cells, each as rs_hpsi_f32 would
+ * compute it through the per-point gather (kslaplacian_r then
+ * nonlocaloperation_r_02 per cell: kslaplacian8f.F90:23-261,
+ * nonlocaloperation8f.F90:149-235), in one persistent launch over a device
+ * table of the cells, for sets of small cells (tens of 20-40^3 grids) that a
+ * launch per cell would leave mostly idle.
+ *   rs_hpsi_batch_create: plan over the geometries and band counts nb[c];
+ *   rs_hpsi_batch_set_f32: per-cell device pointers (veff, D per atom,
+ *     <p|psi>, psi, H psi); waits for the device, so no run may be in flight;
+ *   rs_hpsi_batch_run_f32: the first run times the candidate launch shapes
+ *     and keeps the fastest (rs_hpsi_batch_info reports it); with use_graph
+ *     and a non-null stream the launch is captured once into a CUDA graph and
+ *     replayed on later runs (a new set_f32 drops the graph).
+ * Returns 0, or a negative status (rs_last_error). */
+typedef struct rs_hpsi_batch rs_hpsi_batch;
+int rs_hpsi_batch_create(rs_hpsi_batch** plan, int ncell, const rs_geom* const* geoms,
+                         const int* nb);
+int rs_hpsi_batch_set_f32(rs_hpsi_batch* plan, const float* const* veff,
+                          const double* const* dij, const double* const* rp,
+                          const float* const* psi, float* const* hpsi);
+int rs_hpsi_batch_run_f32(rs_hpsi_batch* plan, int use_graph, void* stream);
+/* the autotuned shape; returns 1 before the first run */
+int rs_hpsi_batch_info(const rs_hpsi_batch* plan, int* threads_per_cta, int* bands_per_item,
+                       int* ctas_per_sm);
+int rs_hpsi_batch_destroy(rs_hpsi_batch* plan);
+
 /* ---- fixed-tree reductions (shared order with the oracle) --------------- */
 /* out(dev, 1 double) = sum_i a_i b_i in the documented block tree. */
 int rs_dot_f64(long n, const double* a, const double* b, double* out, void* stream);

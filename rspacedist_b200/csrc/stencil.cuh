@@ -21,26 +21,34 @@ struct GradCoefs {
   double a[9];
 };
 
+// i in (-n, 2n) wrapped into [0, n) (stencil offsets are below the grid size:
+// rs_geom_create requires 2 nf < n on every axis)
+__device__ __forceinline__ int wrap_near(int i, int n) {
+  return i < 0 ? i + n : (i >= n ? i - n : i);
+}
+
 // acc + (-1/2 lap + veff) psi at (ix,iy,iz): x terms with the diagonal, then
 // y, then z, one fma each (kslaplacian8f.F90:207-261).
 template <class T>
 __device__ __forceinline__ T stencil_point(const StencilArgs<T>& s, const T* __restrict__ v,
                                            int ix, int iy, int iz, T vloc, T acc) {
-  const long nx = s.nx, ny = s.ny, nz = s.nz;
-  const long row = ((long)iz * ny + iy) * nx;
-  const long p = row + ix;
-  for (int m = s.nf; m >= 1; --m) acc = fma(s.cx[m], __ldg(v + row + wrapi(ix - m, nx)), acc);
+  const int nx = s.nx, ny = s.ny, nz = s.nz;
+  const long plane = (long)nx * ny;
+  const T* row = v + (long)iz * plane + (long)iy * nx;  // (iy, iz) row
+  const T* col = v + (long)iy * nx + ix;                  // (ix, iy) column, z stride plane
+  for (int m = s.nf; m >= 1; --m) acc = fma(s.cx[m], __ldg(row + wrap_near(ix - m, nx)), acc);
   const T diag = s.c0 + vloc;
-  acc = fma(diag, __ldg(v + p), acc);
-  for (int m = 1; m <= s.nf; ++m) acc = fma(s.cx[m], __ldg(v + row + wrapi(ix + m, nx)), acc);
+  acc = fma(diag, __ldg(row + ix), acc);
+  for (int m = 1; m <= s.nf; ++m) acc = fma(s.cx[m], __ldg(row + wrap_near(ix + m, nx)), acc);
+  const T* pl = v + (long)iz * plane + ix;
   for (int m = s.nf; m >= 1; --m)
-    acc = fma(s.cy[m], __ldg(v + ((long)iz * ny + wrapi(iy - m, ny)) * nx + ix), acc);
+    acc = fma(s.cy[m], __ldg(pl + (long)wrap_near(iy - m, ny) * nx), acc);
   for (int m = 1; m <= s.nf; ++m)
-    acc = fma(s.cy[m], __ldg(v + ((long)iz * ny + wrapi(iy + m, ny)) * nx + ix), acc);
+    acc = fma(s.cy[m], __ldg(pl + (long)wrap_near(iy + m, ny) * nx), acc);
   for (int m = s.nf; m >= 1; --m)
-    acc = fma(s.cz[m], __ldg(v + (wrapi(iz - m, nz) * ny + iy) * nx + ix), acc);
+    acc = fma(s.cz[m], __ldg(col + (long)wrap_near(iz - m, nz) * plane), acc);
   for (int m = 1; m <= s.nf; ++m)
-    acc = fma(s.cz[m], __ldg(v + (wrapi(iz + m, nz) * ny + iy) * nx + ix), acc);
+    acc = fma(s.cz[m], __ldg(col + (long)wrap_near(iz + m, nz) * plane), acc);
   return acc;
 }
 

@@ -242,6 +242,55 @@ class Mixer:
             pass
 
 
+class HpsiBatch:
+    """H psi of many small cells in one persistent launch (rs_hpsi_batch_*).
+
+    geoms: Geometry per cell; bands: band count per cell.  set() takes per-cell
+    torch CUDA tensors (veff FP32, dij FP64 per atom, rp FP64, psi and out
+    FP32 [nb][N]); run() applies H to every cell, autotuning the launch on
+    the first call and replaying a CUDA graph of it when graph=True."""
+
+    def __init__(self, geoms, bands):
+        L.load()
+        self.geoms = list(geoms)
+        self.bands = [int(b) for b in bands]
+        n = len(self.geoms)
+        garr = (C.c_void_p * n)(*[g.handle.value for g in self.geoms])
+        barr = (C.c_int * n)(*self.bands)
+        self.h = C.c_void_p()
+        L.call("rs_hpsi_batch_create", C.byref(self.h), n, garr, barr)
+        self._keep = []
+
+    def set(self, veff, dij, rp, psi, out):
+        n = len(self.geoms)
+        arr = lambda ts: (C.c_void_p * n)(*[t.data_ptr() for t in ts])
+        for g, nb, v, ps, o in zip(self.geoms, self.bands, veff, psi, out):
+            _need(v, torch.float32, g.N, "veff")
+            _need(ps, torch.float32, nb * g.N, "psi")
+            _need(o, torch.float32, nb * g.N, "out")
+        self._keep = [list(veff), list(dij), list(rp), list(psi), list(out)]
+        L.call("rs_hpsi_batch_set_f32", self.h, arr(veff), arr(dij), arr(rp), arr(psi), arr(out))
+
+    def run(self, graph: bool = False):
+        L.call("rs_hpsi_batch_run_f32", self.h, 1 if graph else 0, _stream())
+
+    def info(self):
+        t, b, c = C.c_int(), C.c_int(), C.c_int()
+        L.load().rs_hpsi_batch_info(self.h, C.byref(t), C.byref(b), C.byref(c))
+        return {"threads_per_cta": t.value, "bands_per_item": b.value, "ctas_per_sm": c.value}
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            L.load().rs_hpsi_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def force_eig(g: Geometry, dij, sss, psi, sval, occ):
     """Nonlocal force on every atom (force_eig_r), as a (natom, 3) FP64 tensor.
     dij/sss are per-atom (natom, P, P) FP64 device tensors (sss None for NC),

@@ -254,3 +254,19 @@ def smooth_veff(cell: Cell, seed: int = 0, amp: float = 0.3) -> np.ndarray:
 def random_bands(cell: Cell, nb: int, seed: int = 0) -> np.ndarray:
     rng = np.random.default_rng(seed)
     return rng.standard_normal((nb, cell.N)) * 0.1
+
+
+def small_cell_set(count: int = 32, seed: int = 2, spacing: float = 0.30):
+    """Independent small periodic cells, alternately Si8 (PAW dataset) and C8
+    (NC dataset) diamond cubic: lattice constants 10.26 / 6.74 bohr scaled by
+    U[0.97, 1.03], atoms jittered by 0.03 bohr, grids of even size with
+    spacing close to `spacing` (about 22^3 to 36^3)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        name, a0 = (("si_paw", 10.26), ("c_ncps", 6.74))[k % 2]
+        a = a0 * rng.uniform(0.97, 1.03)
+        n = 2 * int(round(a / (2 * spacing)))
+        pos = diamond_positions(1, a, 0.03, int(rng.integers(1 << 30)))
+        out.append(make_cell(a, n, pos, load_dataset(name)))
+    return out
