@@ -108,6 +108,15 @@ int rs_density_f64(long N, int nb, const double* occ, const double* psi, double*
                    void* stream);
 int rs_density_f32(long N, int nb, const double* occ, const float* psi, double* rho,
                    void* stream);
+
+/* Occupation matrices of the projectors (scf_charge_atomicocc,
+ * scf_charge8f.F90:146-213; real bands, one spin, one k point):
+ * atocc[a][ij] = sum_l fnele[l] <p_i|psi_l> <psi_l|p_j> (doubled for i != j),
+ * ij running over i <= j with j outer, nprjmx (nprjmx + 1) / 2 entries per
+ * atom.  rp is rspsep as rs_nonlocal_dot returns it ([M][natom][nprjmx]), fnele
+ * the occupations (device).  Every atom is handled; kukan uses the PAW ones. */
+int rs_atomicocc(const rs_geom* g, const double* rp, const double* fnele, int M, double* atocc,
+                 void* stream);
 /* trans_c2d_smtcharge + interpolation, forward branch, nmesh=2
  * (trans8f.F90:8-47, interpolation8f.F90:8-100): out(dev) has 8*nx*ny*nz. */
 int rs_interp_c2d(int nx, int ny, int nz, int nf, const double* in, double* out,

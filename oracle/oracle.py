@@ -220,6 +220,20 @@ def diffcharge(rho_o, rho_i, h, xmax):
                             *(C.c_double(v) for v in h), *(C.c_double(v) for v in xmax))
 
 
+def atomicocc(nprj, nprjmx, rp, fnele):
+    """scf_charge_atomicocc: rp [M][natom][nprjmx], fnele [M] ->
+    atocc [natom][nprjmx (nprjmx+1) / 2] (packed upper triangle, j outer)."""
+    L = lib()
+    nprj = np.ascontiguousarray(nprj, np.int32)
+    natom = nprj.size
+    rp = _f64(rp)
+    fnele = _f64(fnele)
+    M = fnele.size
+    out = np.zeros((natom, nprjmx * (nprjmx + 1) // 2))
+    L.orc_atomicocc(natom, nprjmx, _i(nprj), M, _d(rp), _d(fnele), _d(out))
+    return out
+
+
 class Broyden:
     """scf_chargemixing with modified Broyden history (one spin, grid density)."""
 

@@ -77,6 +77,12 @@ void orc_veff_sum(long n, const double* vx, const double* vloc, const double* vh
  * block tree. */
 double orc_diffcharge(long n, const double* rho_o, const double* rho_i, double dx, double dy,
                       double dz, double xmax, double ymax, double zmax);
+/* scf_charge_atomicocc (scf_charge8f.F90:146-213), real bands, one spin, one
+ * k point: atocc[a][ij] = sum_l fnele[l] * t, t = rp[l][a][i] rp[l][a][j]
+ * (doubled for i != j), ij over i <= j with j outer (packed upper triangle),
+ * each band added as fma(fnele, t, atocc) in band order. */
+void orc_atomicocc(int natom, int nprjmx, const int* nprj, int M, const double* rp,
+                   const double* fnele, double* atocc);
 /* scf_chargemixing_broyden (scf_chargemixing8f.F90:214-657), one spin, grid
  * density only (norm-conserving atoms): modified Broyden with history nbrydn
  * and mixing ratio eta.  Dot products use the fixed block tree times dV. */

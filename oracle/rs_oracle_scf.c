@@ -141,6 +141,30 @@ double orc_diffcharge(long n, const double* rho_o, const double* rho_i, double d
   return sqrt(s * dx * dy * dz / (8.0 * xmax * ymax * zmax));
 }
 
+/* Occupation matrices of the projectors, restated from scf_charge_atomicocc
+ * (scf_charge8f.F90:146-213) for nrc = 0, nums = nspv = 1, numk = 1: the loop
+ * order there is band l, then j, then i <= j, and every atom's matrix is a
+ * sum over bands in order. */
+void orc_atomicocc(int natom, int nprjmx, const int* nprj, int M, const double* rp,
+                   const double* fnele, double* atocc) {
+  const int npack = nprjmx * (nprjmx + 1) / 2;
+  for (long k = 0; k < (long)natom * npack; ++k) atocc[k] = 0.0;
+  for (int a = 0; a < natom; ++a) {
+    double* occ = atocc + (long)a * npack;
+    for (int l = 0; l < M; ++l) {
+      const double* r = rp + ((long)l * natom + a) * nprjmx;
+      int ij = 0;
+      for (int j = 0; j < nprj[a]; ++j)
+        for (int i = 0; i <= j; ++i) {
+          double t = r[i] * r[j];
+          if (i != j) t = 2.0 * t;
+          occ[ij] = fma(fnele[l], t, occ[ij]);
+          ++ij;
+        }
+    }
+  }
+}
+
 /* ------------------------------------------------------------------------ */
 /* Modified Broyden mixing, restated from scf_chargemixing
  * (scf_chargemixing8f.F90:59-168) and scf_chargemixing_broyden (:214-657)

@@ -642,6 +642,47 @@ extern "C" int rs_density_f32(long N, int nb, const double* occ, const float* ps
   return RS_OK;
 }
 
+namespace rs {
+namespace {
+// scf_charge_atomicocc (scf_charge8f.F90:146-213), real bands, one spin: one
+// thread per (atom, packed pair i <= j), the bands summed in order with one
+// fma each, as the Fortran loop does.
+__global__ void k_atomicocc(int natom, int nprjmx, const int* __restrict__ nprj, int M,
+                            const double* __restrict__ rp, const double* __restrict__ fnele,
+                            double* __restrict__ atocc) {
+  const int npack = nprjmx * (nprjmx + 1) / 2;
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)natom * npack) return;
+  const int a = (int)(idx / npack), ij = (int)(idx % npack);
+  int j = 0;
+  while ((j + 1) * (j + 2) / 2 <= ij) ++j;
+  const int i = ij - j * (j + 1) / 2;
+  double acc = 0.0;
+  if (j < nprj[a]) {
+    for (int l = 0; l < M; ++l) {
+      const double* r = rp + ((long)l * natom + a) * nprjmx;
+      double t = r[i] * r[j];
+      if (i != j) t = 2.0 * t;
+      acc = fma(fnele[l], t, acc);
+    }
+  }
+  atocc[idx] = acc;
+}
+}  // namespace
+}  // namespace rs
+
+extern "C" int rs_atomicocc(const rs_geom* g, const double* rp, const double* fnele, int M,
+                            double* atocc, void* stream) {
+  if (!g || M < 0 || (M > 0 && (!rp || !fnele)) || !atocc)
+    return rs::fail(RS_EINVAL, "rs_atomicocc: bad arguments");
+  const long n = (long)g->natom * (g->nprjmx * (g->nprjmx + 1) / 2);
+  if (n == 0) return RS_OK;
+  rs::k_atomicocc<<<rs::div_up(n, 128), 128, 0, rs::as_stream(stream)>>>(
+      g->natom, g->nprjmx, g->d_nprj, M, rp, fnele, atocc);
+  RS_LAUNCH_CHECK("k_atomicocc");
+  return RS_OK;
+}
+
 extern "C" int rs_interp_c2d(int nx, int ny, int nz, int nf, const double* in, double* out,
                              void* stream) {
   if (nf < 1 || nf > 8 || nx < 2 * nf || ny < 2 * nf || nz < 2 * nf)

@@ -242,6 +242,18 @@ class Mixer:
             pass
 
 
+def scf_charge_atomicocc(g: Geometry, rp, fnele):
+    """Projector occupation matrices: [natom][nprjmx (nprjmx+1)/2] FP64, packed
+    upper triangle with j outer (scf_charge_atomicocc)."""
+    M = fnele.numel()
+    _need(fnele, torch.float64, M, "fnele")
+    _need(rp, torch.float64, M * g.natom * g.nprjmx, "rp")
+    out = torch.empty((g.natom, g.nprjmx * (g.nprjmx + 1) // 2), dtype=torch.float64,
+                      device=rp.device)
+    L.call("rs_atomicocc", g.handle, _ptr(rp), _ptr(fnele), M, _ptr(out), _stream())
+    return out
+
+
 class HpsiBatch:
     """H psi of many small cells in one persistent launch (rs_hpsi_batch_*).
 

@@ -210,3 +210,19 @@ def test_hpsi_f32_ragged_tiles(oracle, cuda, built_lib, n):
     ref = oracle.hpsi(sysk, psi, rp)
     out = K.hpsi(g, T(veff, torch.float32), T(cell.dij), T(rp), T(psi, torch.float32))
     np.testing.assert_allclose(out.cpu().numpy(), ref, atol=F32_RTOL * np.abs(ref).max())
+
+
+def test_atomicocc_bit_exact(oracle, cuda, built_lib, si8):
+    """scf_charge_atomicocc: GPU occupation matrices equal the oracle's bit for
+    bit, and their diagonal is sum_l f_l <p_i|psi_l>^2."""
+    from rspacedist_b200 import kukan as K
+    g = K.Geometry(si8)
+    rng = np.random.default_rng(5)
+    M = 20
+    rp = rng.standard_normal((M, si8.natom, si8.nprjmx))
+    f = rng.uniform(0.0, 2.0, M)
+    got = K.scf_charge_atomicocc(g, T(rp), T(f)).cpu().numpy()
+    ref = oracle.atomicocc(si8.nprj, si8.nprjmx, rp, f)
+    assert np.array_equal(got, ref)
+    diag = [j * (j + 1) // 2 + j for j in range(si8.nprjmx)]
+    np.testing.assert_allclose(ref[:, diag], np.einsum("l,lai->ai", f, rp ** 2), rtol=1e-13)

@@ -314,3 +314,21 @@ def test_broyden_first_step_is_linear_and_it_solves_a_fixed_point(oracle):
     for _ in range(101):
         lin = lin + 0.3 * (A @ lin + c - lin)
     assert np.linalg.norm(lin - fix) > 1e-3 * np.linalg.norm(fix)
+
+
+def test_atomicocc_known_answer(oracle):
+    """scf_charge_atomicocc restated: packed upper triangle (j outer, i <= j),
+    off-diagonal entries doubled, equal to sum_l f_l r_i r_j from numpy."""
+    rng = np.random.default_rng(3)
+    M, natom, P = 7, 3, 4
+    rp = rng.standard_normal((M, natom, P))
+    f = rng.uniform(0, 2, M)
+    got = oracle.atomicocc(np.array([4, 4, 2]), P, rp, f)
+    full = np.einsum("l,lai,laj->aij", f, rp, rp)
+    for a, npa in enumerate((4, 4, 2)):
+        ij = 0
+        for j in range(P):
+            for i in range(j + 1):
+                want = 0.0 if j >= npa else full[a, i, j] * (1.0 if i == j else 2.0)
+                assert abs(got[a, ij] - want) <= 1e-13 * max(1.0, abs(want))
+                ij += 1
