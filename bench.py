@@ -519,7 +519,9 @@ def run_hartree_profile(n):
     K.scf_hartree((n, n, n), 4, xm, rho_d, vh, 1e-12, ncgmax=50)
     torch.cuda.synchronize()
     vh.zero_()
-    with ClockSampler(torch.cuda.current_device()) as clk:
+    side = torch.cuda.Stream()  # a real stream: the solve replays its batches as a graph
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk, torch.cuda.stream(side):
         t = time.perf_counter()
         it, dp = K.scf_hartree((n, n, n), 4, xm, rho_d, vh, 1e-12)
         torch.cuda.synchronize()

@@ -128,7 +128,7 @@ struct CgScalars {
 };
 static_assert(sizeof(CgScalars) <= 16 * sizeof(double), "CG scalars fit the work array");
 
-constexpr int kCgBatch = 16;
+constexpr int kCgBatch = 50;  // iterations per host check (800 = 16 batches)
 
 
 // ap = A p by a z-march, in k_hartree_lap's multiply-add order (x terms from
@@ -437,15 +437,19 @@ __global__ void __launch_bounds__(kTreeLanes) k_cg_update_rr(long N, CgScalars* 
 
 // r2r = fold(part); beta, dp and the stopping rule of scf_hartree_cg
 // (restart every ncgres; at least ncgmin, at most ncgmax iterations)
+// The iteration number is kept on the device (s->iters), so a batch of
+// iterations is the same sequence of launches every time and can be replayed
+// as one CUDA graph.
 __global__ void k_cg_fold_beta(long nblk, const double* __restrict__ part, CgScalars* s,
-                               int loop, int ncgres, int ncgmin, int ncgmax, double epsvh,
-                               double ddx, double ddy, double ddz, double vol) {
+                               int ncgres, int ncgmin, int ncgmax, double epsvh, double ddx,
+                               double ddy, double ddz, double vol) {
   if (s->done) return;
   __shared__ double ws[8];
   double acc = 0.0;
   for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + part[k];
   const double t = tree_fold256(acc, ws);
   if (threadIdx.x == 0) {
+    const int loop = s->iters + 1;
     s->r2r = t;
     double beta = t / s->r1r;
     if (loop % ncgres == 0) beta = 0.0;
@@ -584,19 +588,49 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
   CgScalars hs;
   hs.done = 0;
   const int lmax = ncgmax > ncgmin ? ncgmax : ncgmin;
-  for (int loop = 1; loop <= lmax && !hs.done; loop += kCgBatch) {
-    for (int l = loop; l < loop + kCgBatch && l <= lmax; ++l) {
+  // batches of kCgBatch iterations; every kernel returns at once after the
+  // stopping test has fired, so a batch may run past the last iteration.  On
+  // a stream other than the legacy one the batch is captured once as a CUDA
+  // graph and replayed.
+  auto batch = [&]() {
+    for (int l = 0; l < kCgBatch; ++l) {
       lap(p, ap);
       k_cg_fold_alpha<<<1, kTreeLanes, 0, st>>>(nblk, part, sc);
       k_cg_update_rr<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, vh, p, ap, avhs, b, r, part);
-      k_cg_fold_beta<<<1, kTreeLanes, 0, st>>>(nblk, part, sc, l, ncgres, ncgmin, ncgmax, epsvh,
+      k_cg_fold_beta<<<1, kTreeLanes, 0, st>>>(nblk, part, sc, ncgres, ncgmin, lmax, epsvh,
                                                ddx, ddy, ddz, vol);
       k_cg_dir<<<gN, 256, 0, st>>>(N, sc, r, p);
     }
-    RS_LAUNCH_CHECK("hartree_cg iteration");
-    RS_CUDA(cudaMemcpyAsync(&hs, sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
-    RS_CUDA(cudaStreamSynchronize(st));
+  };
+  cudaGraphExec_t exec = nullptr;
+  if (st != nullptr) {
+    cudaGraph_t gph = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      batch();
+      cudaError_t e = cudaStreamEndCapture(st, &gph);
+      if (e == cudaSuccess && cudaGraphInstantiate(&exec, gph, 0) != cudaSuccess) exec = nullptr;
+      if (gph) cudaGraphDestroy(gph);
+    }
+    cudaGetLastError();  // a failed capture falls back to plain launches
   }
+  rc = RS_OK;
+  for (int loop = 1; loop <= lmax && !hs.done; loop += kCgBatch) {
+    if (exec) {
+      const cudaError_t e = cudaGraphLaunch(exec, st);
+      if (e != cudaSuccess) { rc = cuda_status(e, "hartree_cg graph"); break; }
+    } else {
+      batch();
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { rc = cuda_status(e, "hartree_cg iteration"); break; }
+    if (cudaMemcpyAsync(&hs, sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      rc = cuda_status(cudaGetLastError(), "hartree_cg");
+      break;
+    }
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (rc) return rc;
   if (iters) *iters = hs.iters;
   if (dp_out) *dp_out = hs.dp;
   return RS_OK;

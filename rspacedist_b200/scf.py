@@ -176,6 +176,20 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
     density as rho.*, the output density as r_o.*), as write_wf and
     write_rhovht do."""
     dev = torch.device("cuda")
+    # the loop runs on a stream of its own (launches are stream-ordered there
+    # and the Hartree solve can replay its iteration batches as CUDA graphs)
+    side = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        res = _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, zval,
+                       epsvh, vloc, rho0, psi0, log, profile, smearing, tf, restart_dir,
+                       save_dir, dev)
+    side.synchronize()
+    return res
+
+
+def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, zval, epsvh,
+             vloc, rho0, psi0, log, profile, smearing, tf, restart_dir, save_dir, dev):
     g = K.Geometry(cell)
     N, shape = cell.N, cell.shape
     dshape = tuple(2 * s for s in shape)

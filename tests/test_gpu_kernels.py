@@ -169,6 +169,14 @@ def test_hartree_bit_exact(oracle, cuda, built_lib):
     it, dp = K.scf_hartree(shape, 4, xmax, T(rho), vh)
     assert it == itref and dp == dpref
     assert np.array_equal(vh.cpu().numpy(), vref)
+    # on a stream of its own the solve replays its iteration batches as a graph
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        vh2 = T(vh0)
+        it2, dp2 = K.scf_hartree(shape, 4, xmax, T(rho), vh2)
+    st.synchronize()
+    assert it2 == itref and dp2 == dpref
+    assert np.array_equal(vh2.cpu().numpy(), vref)
 
 
 @pytest.mark.parametrize("n", [1, 4095, 4096, 4097, 300000])
