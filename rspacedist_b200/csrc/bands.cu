@@ -514,20 +514,15 @@ __global__ void k_diis_solve_b(int nb, Sc* sc, double eps_eig, double* __restric
   if (j < nb) diis_solve(sc + j, eps_eig, resid + j);
 }
 
-__global__ void k_gather_bands_d(long n, int M, const int* __restrict__ rank,
-                                 const double* __restrict__ src, double* __restrict__ dst) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n * M) return;
-  const int j = (int)(i / n);
-  dst[(long)rank[j] * n + (i % n)] = src[i];
-}
+// dst band dband[k] = src band sband[k] for k < K (bands of n values)
 template <class T>
-__global__ void k_permute_bands(long n, int M, const int* __restrict__ rank,
-                                const T* __restrict__ src, T* __restrict__ dst) {
+__global__ void k_move_bands(long n, int K, const int* __restrict__ sband, const T* __restrict__ src,
+                             const int* __restrict__ dband, T* __restrict__ dst) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n * M) return;
-  const int j = (int)(i / n);
-  dst[(long)rank[j] * n + (i % n)] = src[i];
+  if (i >= n * K) return;
+  const int k = (int)(i / n);
+  const long e = i % n;
+  dst[(long)dband[k] * n + e] = src[(long)sband[k] * n + e];
 }
 
 }  // namespace
@@ -1004,22 +999,39 @@ static int reorder(BandCtx<T>& c, double* sval_h, double* resid_h) {
   std::copy(t.begin(), t.end(), sval_h);
   for (int j = 0; j < M; ++j) t[rank[j]] = resid_h[j];
   std::copy(t.begin(), t.end(), resid_h);
-  int* drank = nullptr;
+  // only the bands whose position changes move: they form a permutation of
+  // their own, so gathering them into a buffer and scattering them to their
+  // ranks reorders the arrays (nothing moves when the order already holds)
+  std::vector<int> mv;  // [from..., to...]
+  for (int j = 0; j < M; ++j)
+    if (rank[j] != j) mv.push_back(j);
+  const int K = (int)mv.size();
+  if (K == 0) return RS_OK;
+  for (int k = 0; k < K; ++k) mv.push_back(rank[mv[k]]);
+  std::vector<int> seq(K);
+  for (int k = 0; k < K; ++k) seq[k] = k;
+  int* dmv = nullptr;
   void* tmp = nullptr;
-  RS_CUDA(cudaMallocAsync((void**)&drank, sizeof(int) * M, c.st));
-  RS_CUDA(cudaMallocAsync(&tmp, sizeof(T) * (size_t)N * M, c.st));
-  RS_CUDA(cudaMemcpyAsync(drank, rank.data(), sizeof(int) * M, cudaMemcpyHostToDevice, c.st));
+  RS_CUDA(cudaMallocAsync((void**)&dmv, sizeof(int) * 3 * K, c.st));
+  RS_CUDA(cudaMallocAsync(&tmp, std::max(sizeof(T) * (size_t)N, sizeof(double) * nrp) * K, c.st));
+  mv.insert(mv.end(), seq.begin(), seq.end());  // [from | to | 0..K-1]
+  RS_CUDA(cudaMemcpyAsync(dmv, mv.data(), sizeof(int) * 3 * K, cudaMemcpyHostToDevice, c.st));
+  const int* from = dmv;
+  const int* to = dmv + K;
+  const int* slot = dmv + 2 * K;
   T* arrs[2] = {c.psi, c.sep() ? c.spsi : nullptr};
   for (T* a : arrs) {
     if (!a) continue;
-    k_permute_bands<T><<<div_up(N * M, 256), 256, 0, c.st>>>(N, M, drank, a, (T*)tmp);
-    cudaMemcpyAsync(a, tmp, sizeof(T) * N * M, cudaMemcpyDeviceToDevice, c.st);
+    k_move_bands<T><<<div_up(N * K, 256), 256, 0, c.st>>>(N, K, from, a, slot, (T*)tmp);
+    k_move_bands<T><<<div_up(N * K, 256), 256, 0, c.st>>>(N, K, slot, (T*)tmp, to, a);
   }
   if (nrp) {
-    k_gather_bands_d<<<div_up((long)nrp * M, 256), 256, 0, c.st>>>(nrp, M, drank, c.rp, (double*)tmp);
-    cudaMemcpyAsync(c.rp, tmp, sizeof(double) * nrp * M, cudaMemcpyDeviceToDevice, c.st);
+    k_move_bands<double><<<div_up((long)nrp * K, 256), 256, 0, c.st>>>(nrp, K, from, c.rp, slot,
+                                                                        (double*)tmp);
+    k_move_bands<double><<<div_up((long)nrp * K, 256), 256, 0, c.st>>>(nrp, K, slot,
+                                                                        (double*)tmp, to, c.rp);
   }
-  cudaFreeAsync(drank, c.st);
+  cudaFreeAsync(dmv, c.st);
   cudaFreeAsync(tmp, c.st);
   cudaError_t e = cudaStreamSynchronize(c.st);
   if (e != cudaSuccess) return cuda_status(e, "reorderstates");
