@@ -72,7 +72,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, extra), srcs))
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-lcublas"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -12,8 +12,12 @@
 // producer, MMA issuer, drain warps) streams them through shared memory.
 // Gram products split K into chunks whose partial tiles are summed in FP64
 // in a fixed order.  FP64 operands use tiled FP64 kernels (CUDA cores).
+#include <cublas_v2.h>
 #include <math.h>
+#include <stdint.h>
 
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "rs_common.cuh"
@@ -516,96 +520,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 }
 
 
-// ------------------------------------------------------------------ FP64
-// C tile 64 x 64 per block (256 threads, 4 x 4 each), K chunk per blockIdx.y,
-// partials summed in a fixed order by k_gram_reduce64.
-constexpr int DT = 64;
-constexpr int DK = 16;
-
-__global__ void __launch_bounds__(256) k_gram_f64(const double* __restrict__ A, long lda, int m,
-                                                  const double* __restrict__ B, long ldb, int n,
-                                                  long K, long kchunk, double* __restrict__ part) {
-  __shared__ double As[DK][DT + 1], Bs[DK][DT + 1];
-  const int tid = threadIdx.x;
-  const int ti = tid % 16, tj = tid / 16;
-  const int i0 = blockIdx.x % ((m + DT - 1) / DT) * DT;
-  const int j0 = blockIdx.x / ((m + DT - 1) / DT) * DT;
-  const long k0 = (long)blockIdx.y * kchunk, k1 = min(K, k0 + kchunk);
-  double acc[4][4] = {};
-  for (long kb = k0; kb < k1; kb += DK) {
-    for (int e = tid; e < DK * DT; e += 256) {
-      const int kk = e % DK, r = e / DK;
-      const long k = kb + kk;
-      As[kk][r] = (i0 + r < m && k < k1) ? A[(long)(i0 + r) * lda + k] : 0.0;
-      Bs[kk][r] = (j0 + r < n && k < k1) ? B[(long)(j0 + r) * ldb + k] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < DK; ++kk) {
-      double a[4], b[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) { a[q] = As[kk][ti + 16 * q]; b[q] = Bs[kk][tj + 16 * q]; }
-#pragma unroll
-      for (int x = 0; x < 4; ++x)
-#pragma unroll
-        for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
-    }
-    __syncthreads();
-  }
-  double* P = part + ((long)blockIdx.y * gridDim.x + blockIdx.x) * DT * DT;
-#pragma unroll
-  for (int x = 0; x < 4; ++x)
-#pragma unroll
-    for (int y = 0; y < 4; ++y) P[(tj + 16 * y) * DT + ti + 16 * x] = acc[x][y];
-}
-
-__global__ void k_gram_reduce64(const double* __restrict__ part, int nsplit, int ntile, int m,
-                                int n, double alpha, double* __restrict__ C, long ldc) {
-  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long)m * n) return;
-  const int i = (int)(idx % m), j = (int)(idx / m);
-  const int tiles_i = (m + DT - 1) / DT;
-  const int t = (j / DT) * tiles_i + i / DT;
-  double s = 0.0;
-  for (int sp = 0; sp < nsplit; ++sp)
-    s += part[((long)sp * ntile + t) * DT * DT + (j % DT) * DT + (i % DT)];
-  C[(long)j * ldc + i] = alpha * s;
-}
-
-// Y[j][p] = sum_k X[k][p] Z(k,j); block = 128 points x 32 bands, 4 per thread in bands
-__global__ void __launch_bounds__(256) k_rotate_f64(const double* __restrict__ X, long ldx,
-                                                    long npts, int kin,
-                                                    const double* __restrict__ Z, long ldz,
-                                                    int nout, double* __restrict__ Y, long ldy) {
-  __shared__ double Zs[32][33];
-  const int tid = threadIdx.x;
-  const long p = (long)blockIdx.x * 128 + (tid % 128);
-  const int jg = tid / 128;  // 0..1
-  const int j0 = blockIdx.y * 32;
-  double acc[16] = {};
-  for (int kb = 0; kb < kin; kb += 32) {
-    for (int e = tid; e < 32 * 32; e += 256) {
-      const int kk = e % 32, jj = e / 32;
-      Zs[kk][jj] = (kb + kk < kin && j0 + jj < nout) ? Z[(long)(j0 + jj) * ldz + kb + kk] : 0.0;
-    }
-    __syncthreads();
-    const int kn = min(32, kin - kb);
-    if (p < npts)
-      for (int kk = 0; kk < kn; ++kk) {
-        const double x = X[(long)(kb + kk) * ldx + p];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = fma(x, Zs[kk][jg * 16 + q], acc[q]);
-      }
-    __syncthreads();
-  }
-  if (p < npts)
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int j = j0 + jg * 16 + q;
-      if (j < nout) Y[(long)j * ldy + p] = acc[q];
-    }
-}
-
 int check_tc_error(cudaStream_t st) {
   int h = 0;
   RS_CUDA(cudaMemcpyFromSymbolAsync(&h, g_tc_error, sizeof(int), 0, cudaMemcpyDeviceToHost, st));
@@ -723,34 +637,63 @@ int rotate_f32(long npts, int kin, int nout, const float* X, long ldx, const dou
   return check_tc_error(st);
 }
 
+// ------------------------------------------------------------------ FP64
+// The plain FP64 path (the drop-in baseline) runs its subspace products as
+// library DGEMMs: one cuBLAS handle per device, bound to the caller's stream
+// for each call.  cuBLAS is deterministic run to run; its sums are not the
+// oracle's order, so these products are checked to 1e-12, not bit for bit.
+cublasHandle_t cublas_handle() {
+  static std::mutex mu;
+  static std::map<int, cublasHandle_t> handles;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = handles.find(dev);
+  if (it != handles.end()) return it->second;
+  cublasHandle_t h = nullptr;
+  if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return nullptr;
+  handles[dev] = h;
+  return h;
+}
+
+int cublas_status(cublasStatus_t s, const char* what) {
+  if (s == CUBLAS_STATUS_SUCCESS) return RS_OK;
+  return fail(RS_ECUDA, std::string(what) + ": cuBLAS status " + std::to_string((int)s));
+}
+
+// C[i + j*ldc] = alpha sum_k A[i*lda + k] B[j*ldb + k]  (C = alpha A B^T)
 int gram_f64(int m, int n, long K, const double* A, long lda, const double* B, long ldb,
              double alpha, double* C, long ldc, cudaStream_t st) {
   if (m <= 0 || n <= 0) return RS_OK;
-  const int ti = (m + DT - 1) / DT, tj = (n + DT - 1) / DT;
-  const int ntile = ti * tj;
-  long kchunk = 8192;
-  long nsplit = (K + kchunk - 1) / kchunk;
-  if (nsplit < 1) nsplit = 1;
-  while (nsplit * ntile > 65536 * 4) { kchunk *= 2; nsplit = (K + kchunk - 1) / kchunk; }
-  double* part = nullptr;
-  RS_CUDA(cudaMallocAsync((void**)&part, sizeof(double) * nsplit * ntile * DT * DT, st));
-  dim3 grid(ntile, (unsigned)nsplit);
-  k_gram_f64<<<grid, 256, 0, st>>>(A, lda, m, B, ldb, n, K, kchunk, part);
-  k_gram_reduce64<<<div_up((long)m * n, 256), 256, 0, st>>>(part, (int)nsplit, ntile, m, n,
-                                                            alpha, C, ldc);
-  cudaError_t e = cudaGetLastError();
-  cudaFreeAsync(part, st);
-  if (e != cudaSuccess) return cuda_status(e, "k_gram_f64");
-  return RS_OK;
+  if (K > INT32_MAX || lda > INT32_MAX || ldb > INT32_MAX)
+    return fail(RS_EINVAL, "rs_gram_f64: K and leading dimensions must fit in 32 bits");
+  keep_pool_memory();
+  cublasHandle_t h = cublas_handle();
+  if (!h) return fail(RS_ECUDA, "rs_gram_f64: cublasCreate failed");
+  int rc = cublas_status(cublasSetStream(h, st), "rs_gram_f64");
+  const double beta = 0.0;
+  if (!rc)
+    rc = cublas_status(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, m, n, (int)K, &alpha, A,
+                                   (int)lda, B, (int)ldb, &beta, C, (int)ldc),
+                       "rs_gram_f64");
+  return rc;
 }
 
+// Y[j*ldy + p] = sum_k X[k*ldx + p] Z[j*ldz + k]  (Y = X Z, column-major)
 int rotate_f64(long npts, int kin, int nout, const double* X, long ldx, const double* Z, long ldz,
                double* Y, long ldy, cudaStream_t st) {
   if (npts <= 0 || nout <= 0) return RS_OK;
-  dim3 grid(div_up(npts, 128), div_up(nout, 32));
-  k_rotate_f64<<<grid, 256, 0, st>>>(X, ldx, npts, kin, Z, ldz, nout, Y, ldy);
-  RS_LAUNCH_CHECK("k_rotate_f64");
-  return RS_OK;
+  if (npts > INT32_MAX || ldx > INT32_MAX || ldy > INT32_MAX)
+    return fail(RS_EINVAL, "rs_rotate_f64: sizes must fit in 32 bits");
+  cublasHandle_t h = cublas_handle();
+  if (!h) return fail(RS_ECUDA, "rs_rotate_f64: cublasCreate failed");
+  int rc = cublas_status(cublasSetStream(h, st), "rs_rotate_f64");
+  const double one = 1.0, zero = 0.0;
+  if (!rc)
+    rc = cublas_status(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)npts, nout, kin, &one, X,
+                                   (int)ldx, Z, (int)ldz, &zero, Y, (int)ldy),
+                       "rs_rotate_f64");
+  return rc;
 }
 
 }  // namespace rs
