@@ -287,6 +287,18 @@ int rs_force_nl_f64(const rs_geom* g, const double* dij, const double* sss, cons
 int rs_force_nl_f32(const rs_geom* g, const double* dij, const double* sss, const float* psi,
                     const double* sval, const double* occ, int nb, double* fxyz, void* stream);
 
+/* rs_hartree_cg for the mixed-precision path: the same CG (restart every
+ * ncgres, the same stopping rule on the residual) with p, A p and r in FP32
+ * and vh, every dot product and every residual norm in FP64.  The residual
+ * is recomputed in FP64 as b - A vh ("reliable update") whenever its FP32
+ * recurrence has dropped tenfold since the last recomputation, and before
+ * the solve stops, so the attainable accuracy is that of the FP64 solve.
+ * rho and vh are FP64 as in rs_hartree_cg.  Grids with odd nx or odd nfh run
+ * the FP64 iteration. */
+int rs_hartree_cg_f32(int nx, int ny, int nz, int nfh, double xmax, double ymax, double zmax,
+                      double epsvh, int ncgmin, int ncgmax, int ncgres, const double* rho,
+                      double* vh, int* iters, double* dp, void* stream);
+
 /* rs_hartree_cg for callers that cannot allocate device memory (a host code
  * that handed all device memory to its own pool, a framework whose caching
  * allocator owns the GPU, work issued where the driver's allocation lock must

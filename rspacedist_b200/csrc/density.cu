@@ -124,7 +124,9 @@ static InterpW interp_weights(int nf) {
 // iterations instead of after each one.
 struct CgScalars {
   double r1r, pap, r2r, alph, beta, dp, bve;
+  double r2ref;  // mixed solve: r.r at the last FP64 residual
   int done, iters;
+  int upd;       // mixed solve: recompute the residual in FP64 now
 };
 static_assert(sizeof(CgScalars) <= 16 * sizeof(double), "CG scalars fit the work array");
 
@@ -261,14 +263,18 @@ __device__ __forceinline__ void cp_async16_hz(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
-template <int NF>
+// RES: the residual of the mixed solve instead, out32 = (float)(b - A p), only
+// when s->upd is set.
+template <int NF, bool RES = false>
 __global__ void __launch_bounds__(HZ2_THREADS, 1) k_hlap_zmarch2(int nx, int ny, int nz,
                                                                  int zchunk, HartreeCoefs c,
                                                                  const double* __restrict__ p,
                                                                  double* __restrict__ ap,
-                                                                 const CgScalars* __restrict__ s) {
+                                                                 const CgScalars* __restrict__ s,
+                                                                 const double* __restrict__ b = nullptr,
+                                                                 float* __restrict__ out32 = nullptr) {
   static_assert(NF % 2 == 0, "double2 path needs an even halo");
-  if (s->done) return;
+  if (s->done || (RES && !s->upd)) return;
   constexpr int HX = HZ2_TX + 2 * NF, HY = HZ2_TY + 2 * NF, PL = HX * HY, RING = hz2_ring(NF);
   constexpr int PL2 = PL / 2, NST = (PL2 + HZ2_THREADS - 1) / HZ2_THREADS;
   extern __shared__ double2 hz2_sm[];  // [RING][HY][HX / 2]
@@ -367,7 +373,15 @@ __global__ void __launch_bounds__(HZ2_THREADS, 1) k_hlap_zmarch2(int nx, int ny,
       a0 = fma(c.cz[m], q[NF + m].x, a0);
       a1 = fma(c.cz[m], q[NF + m].y, a1);
     }
-    if (active) *reinterpret_cast<double2*>(ap + (long)z * plane + own) = make_double2(a0, a1);
+    if (active) {
+      const long o = (long)z * plane + own;
+      if (RES) {
+        const double2 bb = *reinterpret_cast<const double2*>(b + o);
+        *reinterpret_cast<float2*>(out32 + o) = make_float2((float)(bb.x - a0), (float)(bb.y - a1));
+      } else {
+        *reinterpret_cast<double2*>(ap + o) = make_double2(a0, a1);
+      }
+    }
 #pragma unroll
     for (int k = 0; k < 2 * NF; ++k) q[k] = q[k + 1];
   }
@@ -506,6 +520,276 @@ __global__ void k_cg_dir(long N, const CgScalars* __restrict__ s, const double* 
   p[i] = fma(s->beta, p[i], r[i]);
 }
 
+// ---------------------------------------------------------------- mixed CG
+// The Hartree CG of the mixed path: the same iteration as hartree_cg (kukan's
+// recurrences, restart, stopping rule, device-side folds and graph batches),
+// with the vectors p, A p, r, A x and b in FP32 and the solution vh, every dot
+// product and every residual norm in FP64.  The A p stencil is the paired
+// z-march in FP32.
+template <int NF>
+__global__ void __launch_bounds__(HZ2_THREADS, 1) k_hlap_zmarch2f(int nx, int ny, int nz,
+                                                                  int zchunk, HartreeCoefs c,
+                                                                  const float* __restrict__ p,
+                                                                  float* __restrict__ ap,
+                                                                  const CgScalars* __restrict__ s) {
+  static_assert(NF % 2 == 0, "float2 path needs an even halo");
+  if (s->done) return;
+  constexpr int HX = HZ2_TX + 2 * NF, HY = HZ2_TY + 2 * NF, PL = HX * HY, RING = hz2_ring(NF);
+  constexpr int PL2 = PL / 2, NST = (PL2 + HZ2_THREADS - 1) / HZ2_THREADS;
+  extern __shared__ float2 hzf_sm[];  // [RING][HY][HX / 2]
+  float cx[NF + 1], cy[NF + 1], cz[NF + 1];
+#pragma unroll
+  for (int m = 1; m <= NF; ++m) {
+    cx[m] = (float)c.cx[m];
+    cy[m] = (float)c.cy[m];
+    cz[m] = (float)c.cz[m];
+  }
+  const float diag = (float)c.diag;
+  const int tid = threadIdx.x, tx = tid % (HZ2_TX / 2), ty = tid / (HZ2_TX / 2);
+  const int ntx = (nx + HZ2_TX - 1) / HZ2_TX, nty = (ny + HZ2_TY - 1) / HZ2_TY;
+  const int tile = blockIdx.x % (ntx * nty), zc = blockIdx.x / (ntx * nty);
+  const int x0 = (tile % ntx) * HZ2_TX, y0 = (tile / ntx) * HZ2_TY;
+  const int zs = zc * zchunk, ze = min(zs + zchunk, nz);
+  const long plane = (long)nx * ny;
+  const int gx = x0 + 2 * tx, gy = y0 + ty;
+  const bool active = gx < nx && gy < ny;
+  const long own = active ? (long)gy * nx + gx : 0;
+  int soff[NST], doff[NST];
+#pragma unroll
+  for (int k = 0; k < NST; ++k) {
+    const int e = tid + k * HZ2_THREADS;
+    if (e < PL2) {
+      const int r = e / (HX / 2), q2 = e % (HX / 2);
+      soff[k] = (int)((long)wrapm(y0 - NF + r, ny) * nx + wrapm(x0 - NF + 2 * q2, nx));
+      doff[k] = e;
+    } else {
+      soff[k] = -1;
+      doff[k] = 0;
+    }
+  }
+  auto wrapz = [&](int z) {
+    while (z < 0) z += nz;
+    while (z >= nz) z -= nz;
+    return z;
+  };
+  auto slot = [&](int z) { return (z - zs + NF) % RING; };
+  auto stage = [&](int z) {
+    const float* src = p + (long)wrapz(z) * plane;
+    float2* dst = hzf_sm + slot(z) * PL2;
+#pragma unroll
+    for (int k = 0; k < NST; ++k)
+      if (soff[k] >= 0) cp_async8(dst + doff[k], src + soff[k]);
+    cp_commit_hz();
+  };
+  float2 q[2 * NF + 1];
+#pragma unroll
+  for (int k = 0; k < NF; ++k)
+    q[k] = __ldg(reinterpret_cast<const float2*>(p + (long)wrapz(zs - NF + k) * plane + own));
+#pragma unroll
+  for (int k = 0; k < NF + HZ2_AHEAD; ++k) stage(zs + k);
+  const int lc2 = (ty + NF) * (HX / 2) + tx + NF / 2;
+  for (int z = zs; z < ze; ++z) {
+    cp_wait_hz<HZ2_AHEAD - 1>();
+    __syncthreads();
+    stage(z + NF + HZ2_AHEAD);
+    if (z == zs) {
+#pragma unroll
+      for (int k = 0; k < NF; ++k) q[NF + k] = hzf_sm[slot(zs + k) * PL2 + lc2];
+    }
+    q[2 * NF] = hzf_sm[slot(z + NF) * PL2 + lc2];
+    const float2* cur = hzf_sm + slot(z) * PL2;
+    float v[2 * NF + 2];
+#pragma unroll
+    for (int k = 0; k <= NF; ++k) {
+      const float2 w = cur[lc2 - NF / 2 + k];
+      v[2 * k] = w.x;
+      v[2 * k + 1] = w.y;
+    }
+    float a0 = cx[NF] * v[0], a1 = cx[NF] * v[1];
+#pragma unroll
+    for (int m = NF - 1; m >= 1; --m) {
+      a0 = fmaf(cx[m], v[NF - m], a0);
+      a1 = fmaf(cx[m], v[NF + 1 - m], a1);
+    }
+    a0 = fmaf(diag, v[NF], a0);
+    a1 = fmaf(diag, v[NF + 1], a1);
+#pragma unroll
+    for (int m = 1; m <= NF; ++m) {
+      a0 = fmaf(cx[m], v[NF + m], a0);
+      a1 = fmaf(cx[m], v[NF + 1 + m], a1);
+    }
+#pragma unroll
+    for (int m = NF; m >= 1; --m) {
+      const float2 w = cur[lc2 - m * (HX / 2)];
+      a0 = fmaf(cy[m], w.x, a0);
+      a1 = fmaf(cy[m], w.y, a1);
+    }
+#pragma unroll
+    for (int m = 1; m <= NF; ++m) {
+      const float2 w = cur[lc2 + m * (HX / 2)];
+      a0 = fmaf(cy[m], w.x, a0);
+      a1 = fmaf(cy[m], w.y, a1);
+    }
+#pragma unroll
+    for (int m = NF; m >= 1; --m) {
+      a0 = fmaf(cz[m], q[NF - m].x, a0);
+      a1 = fmaf(cz[m], q[NF - m].y, a1);
+    }
+#pragma unroll
+    for (int m = 1; m <= NF; ++m) {
+      a0 = fmaf(cz[m], q[NF + m].x, a0);
+      a1 = fmaf(cz[m], q[NF + m].y, a1);
+    }
+    if (active) *reinterpret_cast<float2*>(ap + (long)z * plane + own) = make_float2(a0, a1);
+#pragma unroll
+    for (int k = 0; k < 2 * NF; ++k) q[k] = q[k + 1];
+  }
+  cp_wait_hz<0>();
+}
+
+__global__ void __launch_bounds__(kTreeLanes) k_cg_pap_f(long N, const float* __restrict__ p,
+                                                         const float* __restrict__ ap,
+                                                         double* __restrict__ part,
+                                                         const CgScalars* __restrict__ s) {
+  if (s->done) return;
+  __shared__ double ws[8];
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  double acc = 0.0;
+#pragma unroll 4
+  for (int k = 0; k < kTreePerLane; ++k) {
+    const long i = base + (long)k * kTreeLanes;
+    if (i < N) acc = fma((double)p[i], (double)ap[i], acc);
+  }
+  const double t = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// vh += alpha p (FP64), r -= alpha A p (FP32), r.r chunk sums (FP64)
+__global__ void __launch_bounds__(kTreeLanes) k_cg_update_f(long N, const CgScalars* s,
+                                                            double* __restrict__ vh,
+                                                            const float* __restrict__ p,
+                                                            const float* __restrict__ ap,
+                                                            float* __restrict__ r,
+                                                            double* __restrict__ part) {
+  if (s->done) return;
+  __shared__ double ws[8];
+  const double alph = s->alph;
+  const float alf = (float)alph;
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  double acc = 0.0;
+#pragma unroll 4
+  for (int k = 0; k < kTreePerLane; ++k) {
+    const long i = base + (long)k * kTreeLanes;
+    if (i < N) {
+      vh[i] = fma(alph, (double)p[i], vh[i]);
+      const float ri = fmaf(-alf, ap[i], r[i]);
+      r[i] = ri;
+      acc = fma((double)ri, (double)ri, acc);
+    }
+  }
+  const double t = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// r.r chunk sums of the FP32 residual, after it was recomputed in FP64
+__global__ void __launch_bounds__(kTreeLanes) k_cg_rr_f(long N, const CgScalars* s,
+                                                        const float* __restrict__ r,
+                                                        double* __restrict__ part) {
+  if (s->done || !s->upd) return;
+  __shared__ double ws[8];
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  double acc = 0.0;
+#pragma unroll 4
+  for (int k = 0; k < kTreePerLane; ++k) {
+    const long i = base + (long)k * kTreeLanes;
+    if (i < N) acc = fma((double)r[i], (double)r[i], acc);
+  }
+  const double t = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// beta, dp and the stopping rule of scf_hartree_cg from r2r (shared by the
+// two folds of the mixed solve)
+__device__ void cg_close_iteration(CgScalars* s, double t, int loop, int ncgres, int ncgmin,
+                                   int ncgmax, double epsvh, double ddx, double ddy, double ddz,
+                                   double vol) {
+  s->r2r = t;
+  double beta = t / s->r1r;
+  if (loop % ncgres == 0) beta = 0.0;
+  s->beta = beta;
+  s->dp = sqrt(t * ddx * ddy * ddz / vol);
+  s->r1r = t;
+  s->iters = loop;
+  bool stop = false;
+  if (loop >= ncgmin) {
+    if (loop >= ncgmax) stop = true;
+    else if (!(s->dp > epsvh)) stop = true;
+  }
+  if (stop) s->done = 1;
+}
+
+// Mixed solve, after the FP32 update: when r.r has dropped by kReliable since
+// the last FP64 residual, or the stopping test would fire, ask for the
+// residual to be recomputed in FP64 (reliable update) and close the
+// iteration after that; otherwise close it now.
+constexpr double kReliable = 1e-2;  // in r.r: a factor 10 in the residual norm
+__global__ void k_cg_fold_beta_f(long nblk, const double* __restrict__ part, CgScalars* s,
+                                 int ncgres, int ncgmin, int ncgmax, double epsvh, double ddx,
+                                 double ddy, double ddz, double vol) {
+  if (s->done) return;
+  __shared__ double ws[8];
+  double acc = 0.0;
+  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + part[k];
+  const double t = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) {
+    const int loop = s->iters + 1;
+    const double dp = sqrt(t * ddx * ddy * ddz / vol);
+    const bool would_stop = loop >= ncgmin && (loop >= ncgmax || !(dp > epsvh));
+    if (t < kReliable * s->r2ref || would_stop) {
+      s->upd = 1;
+      s->r2r = t;
+    } else {
+      s->upd = 0;
+      cg_close_iteration(s, t, loop, ncgres, ncgmin, ncgmax, epsvh, ddx, ddy, ddz, vol);
+    }
+  }
+}
+
+// closes an iteration whose residual was recomputed in FP64
+__global__ void k_cg_fold_upd_f(long nblk, const double* __restrict__ part, CgScalars* s,
+                                int ncgres, int ncgmin, int ncgmax, double epsvh, double ddx,
+                                double ddy, double ddz, double vol) {
+  if (s->done || !s->upd) return;
+  __shared__ double ws[8];
+  double acc = 0.0;
+  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + part[k];
+  const double t = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) {
+    cg_close_iteration(s, t, s->iters + 1, ncgres, ncgmin, ncgmax, epsvh, ddx, ddy, ddz, vol);
+    s->r2ref = t;
+    s->upd = 0;
+  }
+}
+
+// p = r + beta p (FP32)
+__global__ void k_cg_dir_f(long N, const CgScalars* __restrict__ s, const float* __restrict__ r,
+                           float* __restrict__ p) {
+  if (s->done) return;
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  p[i] = fmaf((float)s->beta, p[i], r[i]);
+}
+
+__global__ void k_to_f32x2(long N, const double* __restrict__ a, const double* __restrict__ b,
+                           float* __restrict__ fa, float* __restrict__ fb) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  fa[i] = (float)a[i];
+  fb[i] = (float)b[i];
+}
+
+__global__ void k_cg_ref(CgScalars* s) { s->r2ref = s->r1r; s->upd = 0; }
+
 constexpr size_t hz_smem(int nf) { return sizeof(double) * hz_ring(nf) * hz_plane(nf); }
 constexpr size_t hz2_smem(int nf) { return sizeof(double) * hz2_ring(nf) * hz2_plane(nf); }
 
@@ -530,9 +814,13 @@ int hlap_zmarch_attr(int nfh) {
   return e == cudaSuccess ? RS_OK : cuda_status(e, "k_hlap_zmarch");
 }
 
+// work32: nullptr for the FP64 solve; 3 N floats for the mixed solve (used
+// when nfh and nx are even, which its paired FP32 stencil needs; other grids
+// run the FP64 iteration)
 int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double zmax,
                double epsvh, int ncgmin, int ncgmax, int ncgres, const double* rho, double* vh,
-               double* work, int* iters, double* dp_out, cudaStream_t st) {
+               double* work, int* iters, double* dp_out, cudaStream_t st,
+               float* work32) {
   const long N = (long)nx * ny * nz;
   const long nblk = tree_chunks(N);
   double* b = work;
@@ -592,8 +880,55 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
   // stopping test has fired, so a batch may run past the last iteration.  On
   // a stream other than the legacy one the batch is captured once as a CUDA
   // graph and replayed.
+  const bool mixed = work32 != nullptr && pairs;
+  float *fr = nullptr, *fp = nullptr, *fap = nullptr;
+  if (mixed) {
+    fr = work32;
+    fp = fr + N;
+    fap = fp + N;
+    k_to_f32x2<<<gN, 256, 0, st>>>(N, r, p, fr, fp);
+    k_cg_ref<<<1, 1, 0, st>>>(sc);
+    cudaError_t e = cudaFuncSetAttribute(
+        nfh == 2 ? (const void*)k_hlap_zmarch2f<2>
+                 : (nfh == 4 ? (const void*)k_hlap_zmarch2f<4> : (const void*)k_hlap_zmarch2f<6>),
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(hz2_smem(nfh) / 2));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(
+          nfh == 2 ? (const void*)k_hlap_zmarch2<2, true>
+                   : (nfh == 4 ? (const void*)k_hlap_zmarch2<4, true>
+                               : (const void*)k_hlap_zmarch2<6, true>),
+          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz2_smem(nfh));
+    if (e != cudaSuccess) return cuda_status(e, "mixed Hartree CG kernels");
+  }
+  // one mixed iteration: FP32 A p and update, then (when asked) the FP64
+  // residual b - A vh rounded into r, its r.r, and the closing fold
+  auto iter32 = [&]() {
+    switch (nfh) {
+      case 2: k_hlap_zmarch2f<2><<<gz, HZ2_THREADS, hz2_smem(2) / 2, st>>>(nx, ny, nz, zchunk, hc, fp, fap, sc); break;
+      case 4: k_hlap_zmarch2f<4><<<gz, HZ2_THREADS, hz2_smem(4) / 2, st>>>(nx, ny, nz, zchunk, hc, fp, fap, sc); break;
+      default: k_hlap_zmarch2f<6><<<gz, HZ2_THREADS, hz2_smem(6) / 2, st>>>(nx, ny, nz, zchunk, hc, fp, fap, sc); break;
+    }
+    k_cg_pap_f<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, fp, fap, part, sc);
+    k_cg_fold_alpha<<<1, kTreeLanes, 0, st>>>(nblk, part, sc);
+    k_cg_update_f<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, vh, fp, fap, fr, part);
+    k_cg_fold_beta_f<<<1, kTreeLanes, 0, st>>>(nblk, part, sc, ncgres, ncgmin, lmax, epsvh, ddx,
+                                               ddy, ddz, vol);
+    switch (nfh) {
+      case 2: k_hlap_zmarch2<2, true><<<gz, HZ2_THREADS, hz2_smem(2), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr); break;
+      case 4: k_hlap_zmarch2<4, true><<<gz, HZ2_THREADS, hz2_smem(4), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr); break;
+      default: k_hlap_zmarch2<6, true><<<gz, HZ2_THREADS, hz2_smem(6), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr); break;
+    }
+    k_cg_rr_f<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, fr, part);
+    k_cg_fold_upd_f<<<1, kTreeLanes, 0, st>>>(nblk, part, sc, ncgres, ncgmin, lmax, epsvh, ddx,
+                                              ddy, ddz, vol);
+    k_cg_dir_f<<<gN, 256, 0, st>>>(N, sc, fr, fp);
+  };
   auto batch = [&]() {
     for (int l = 0; l < kCgBatch; ++l) {
+      if (mixed) {
+        iter32();
+        continue;
+      }
       lap(p, ap);
       k_cg_fold_alpha<<<1, kTreeLanes, 0, st>>>(nblk, part, sc);
       k_cg_update_rr<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, vh, p, ap, avhs, b, r, part);
@@ -740,6 +1075,30 @@ extern "C" int rs_interp_c2d(int nx, int ny, int nz, int nf, const double* in, d
   return RS_OK;
 }
 
+extern "C" int rs_hartree_cg_f32(int nx, int ny, int nz, int nfh, double xmax, double ymax,
+                                 double zmax, double epsvh, int ncgmin, int ncgmax, int ncgres,
+                                 const double* rho, double* vh, int* iters, double* dp,
+                                 void* stream) {
+  if (nfh < 1 || nfh > 6 || nx <= 2 * nfh || ny <= 2 * nfh || nz <= 2 * nfh)
+    return rs::fail(RS_EINVAL, "rs_hartree_cg_f32: bad grid or nfh");
+  if (ncgres <= 0 || ncgmax <= 0)
+    return rs::fail(RS_EINVAL, "rs_hartree_cg_f32: bad iteration limits");
+  if ((long)nx * ny * nz > 2147483647L)
+    return rs::fail(RS_EINVAL, "rs_hartree_cg_f32: the dense grid must have fewer than 2^31 points");
+  cudaStream_t st = rs::as_stream(stream);
+  const long N = (long)nx * ny * nz;
+  const long nblk = rs::tree_chunks(N);
+  const size_t bytes64 = sizeof(double) * (5 * N + nblk + 1) + 2 * sizeof(double) * 8;
+  const size_t bytes = bytes64 + sizeof(float) * 3 * N + 16;
+  double* work = nullptr;
+  RS_CUDA(cudaMallocAsync((void**)&work, bytes, st));
+  float* work32 = (float*)(((uintptr_t)work + bytes64 + 15) & ~(uintptr_t)15);
+  int rc = rs::hartree_cg(nx, ny, nz, nfh, xmax, ymax, zmax, epsvh, ncgmin, ncgmax, ncgres, rho,
+                          vh, work, iters, dp, st, work32);
+  cudaFreeAsync(work, st);
+  return rc;
+}
+
 extern "C" int rs_hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax,
                              double zmax, double epsvh, int ncgmin, int ncgmax, int ncgres,
                              const double* rho, double* vh, int* iters, double* dp,
@@ -756,7 +1115,7 @@ extern "C" int rs_hartree_cg(int nx, int ny, int nz, int nfh, double xmax, doubl
   double* work = nullptr;
   RS_CUDA(cudaMallocAsync((void**)&work, bytes, st));
   int rc = rs::hartree_cg(nx, ny, nz, nfh, xmax, ymax, zmax, epsvh, ncgmin, ncgmax, ncgres, rho,
-                          vh, work, iters, dp, st);
+                          vh, work, iters, dp, st, nullptr);
   cudaFreeAsync(work, st);
   if (rc == RS_OK && iters && *iters >= ncgmax && dp && *dp > epsvh) {
     rs::set_error("rs_hartree_cg: ncgmax reached");

@@ -18,7 +18,7 @@
 namespace rs {
 int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double zmax,
                double epsvh, int ncgmin, int ncgmax, int ncgres, const double* rho, double* vh,
-               double* work, int* iters, double* dp_out, cudaStream_t st);
+               double* work, int* iters, double* dp_out, cudaStream_t st, float* work32);
 }
 
 namespace {
@@ -81,5 +81,5 @@ extern "C" int rs_hartree_cg_noalloc(int nx, int ny, int nz, int nfh, double xma
   int rc = scratch_address(&work);
   if (rc != RS_OK) return rc;
   return rs::hartree_cg(nx, ny, nz, nfh, xmax, ymax, zmax, epsvh, ncgmin, ncgmax, ncgres, rho,
-                        vh, work, iters, dp, rs::as_stream(stream));
+                        vh, work, iters, dp, rs::as_stream(stream), nullptr);
 }

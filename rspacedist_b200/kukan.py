@@ -169,13 +169,15 @@ def scf_hartee_laplacian(shape, nfh: int, h, v):
 
 
 def scf_hartree(shape, nfh: int, xmax, rho, vh, epsvh=1e-12, ncgmin=1, ncgmax=800,
-                ncgres=801):
-    """CG Poisson solve; vh (in/out) is the warm start.  Returns (iters, dp)."""
+                ncgres=801, mixed: bool = False):
+    """CG Poisson solve; vh (in/out) is the warm start.  Returns (iters, dp).
+    mixed: FP32 CG vectors with FP64 vh, dots and norms (rs_hartree_cg_f32)."""
     nx, ny, nz = shape
     it = C.c_int(0)
     dp = C.c_double(0)
-    L.call("rs_hartree_cg", nx, ny, nz, nfh, xmax[0], xmax[1], xmax[2], epsvh, ncgmin, ncgmax,
-           ncgres, _ptr(rho), _ptr(vh), C.byref(it), C.byref(dp), _stream())
+    L.call("rs_hartree_cg_f32" if mixed else "rs_hartree_cg", nx, ny, nz, nfh, xmax[0], xmax[1],
+           xmax[2], epsvh, ncgmin, ncgmax, ncgres, _ptr(rho), _ptr(vh), C.byref(it),
+           C.byref(dp), _stream())
     return it.value, dp.value
 
 

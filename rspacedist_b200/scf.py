@@ -247,7 +247,8 @@ def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, z
         mixer.step(rho_o, rho_i, dvol)
         tp = mark("mixing", tp)
         rho_d = K.trans_c2d_smtcharge(shape, 4, rho_i)
-        it, _ = K.scf_hartree(dshape, 4, xmax, rho_d, vh_d, epsvh)
+        it, _ = K.scf_hartree(dshape, 4, xmax, rho_d, vh_d, epsvh,
+                              mixed=dtype == torch.float32)
         tp = mark("hartree", tp)
         vh = K.trans_d2c(shape, 4, vh_d)
         vx_d, _ = K.vxpot_lda_pz(rho_d)

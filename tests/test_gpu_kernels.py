@@ -234,3 +234,27 @@ def test_atomicocc_bit_exact(oracle, cuda, built_lib, si8):
     assert np.array_equal(got, ref)
     diag = [j * (j + 1) // 2 + j for j in range(si8.nprjmx)]
     np.testing.assert_allclose(ref[:, diag], np.einsum("l,lai->ai", f, rp ** 2), rtol=1e-13)
+
+
+def test_hartree_mixed_matches_fp64(cuda, built_lib):
+    """The mixed Hartree CG (FP32 vectors, FP64 dots and vh) solves the same
+    problem: its potential agrees with the FP64 solve to FP32 accuracy."""
+    from rspacedist_b200 import kukan as K
+    n = 48
+    a = 10.26
+    x = (np.arange(n) + 0.5) * (a / n) - a / 2
+    rng = np.random.default_rng(0)
+    rho = np.zeros((n, n, n))
+    for c in rng.uniform(-a / 2, a / 2, (4, 3)):
+        d = [x - c[k] for k in range(3)]
+        d = [di - a * np.round(di / a) for di in d]
+        r2 = d[2][:, None, None] ** 2 + d[1][None, :, None] ** 2 + d[0][None, None, :] ** 2
+        rho += np.exp(-r2 / 2.0) / (2 * np.pi) ** 1.5
+    rho -= rho.mean()
+    xm = (a / 2,) * 3
+    v64 = torch.zeros(n ** 3, dtype=torch.float64, device="cuda")
+    v32 = torch.zeros_like(v64)
+    K.scf_hartree((n, n, n), 4, xm, T(rho.ravel()), v64, 1e-12)
+    it, dp = K.scf_hartree((n, n, n), 4, xm, T(rho.ravel()), v32, 1e-12, mixed=True)
+    err = float((v32 - v64).abs().max() / v64.abs().max())
+    assert err < 2e-6, (err, it, dp)
