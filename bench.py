@@ -491,7 +491,7 @@ def run_gemm_profile(npts):
     print(json.dumps(out), flush=True)
 
 
-def run_hartree_profile(n):
+def run_hartree_profile(n, mixed=False):
     """The Hartree CG Poisson solve (rs_hartree_cg, nfh = 4, epsvh = 1e-12, at
     most 800 iterations) on an n^3 grid of the Si512 cell (a = 41.04 bohr):
     eight normalised Gaussians (sigma = 1 bohr, centres uniform in the cell
@@ -523,10 +523,12 @@ def run_hartree_profile(n):
     torch.cuda.synchronize()
     with ClockSampler(torch.cuda.current_device()) as clk, torch.cuda.stream(side):
         t = time.perf_counter()
-        it, dp = K.scf_hartree((n, n, n), 4, xm, rho_d, vh, 1e-12)
+        it, dp = K.scf_hartree((n, n, n), 4, xm, rho_d, vh, 1e-12, mixed=mixed)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t
-    print(json.dumps({"hartree_profile": {"grid": [n] * 3, "cell_bohr": a}, "iterations": it,
+    print(json.dumps({"hartree_profile": {"grid": [n] * 3, "cell_bohr": a,
+                                          "solve": "mixed (FP32 vectors)" if mixed else "FP64"},
+                      "iterations": it,
                       "dp": dp, "ms": round(dt * 1e3, 2), "clocks": clk.summary(),
                       "us_per_iter": round(dt / it * 1e6, 1),
                       "gbs_at_88_bytes_per_point": round(88 * n ** 3 / (dt / it) / 1e9, 1)}),
@@ -602,6 +604,8 @@ def main():
                     help="time the tensor-core Gram and rotation at 1100 bands x POINTS and exit")
     ap.add_argument("--hartree-profile", type=int, metavar="N",
                     help="time the Hartree CG solve on an N^3 dense grid and exit")
+    ap.add_argument("--mixed", action="store_true",
+                    help="with --hartree-profile: the mixed-precision solve")
     ap.add_argument("--batch-profile", type=int, metavar="CELLS",
                     help="time H*psi of CELLS small cells, per-cell calls vs one batched "
                          "launch, and exit")
@@ -609,7 +613,7 @@ def main():
     if args.batch_profile:
         run_batch_profile(args.batch_profile, 20)
     elif args.hartree_profile:
-        run_hartree_profile(args.hartree_profile)
+        run_hartree_profile(args.hartree_profile, args.mixed)
     elif args.diag_profile:
         run_diag_profile(args.diag_profile)
     elif args.gemm_profile:

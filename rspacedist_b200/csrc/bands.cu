@@ -335,16 +335,21 @@ __global__ void k_pdot_final(long nblk, const double* __restrict__ part, double 
   if (threadIdx.x == 0) out[(long)j * ostride] = scale ? s * dx * dy * dz : s;
 }
 
-// c_j = a_j + d_j b_j, d_j = sign * dp[j*dstride]  (ksdiis_r_01)
-template <class T>
+// c_j = a_j + d_j b_j, d_j = sign * dp[j*dstride]  (ksdiis_r_01); V
+// consecutive values per thread (V divides n)
+template <class T, int V>
 __global__ void k_axpy_b(long n, const T* __restrict__ a, const T* __restrict__ b,
                          const double* __restrict__ dp, long dstride, double sign,
                          T* __restrict__ c) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) * V;
   if (i >= n) return;
   const long o = (long)blockIdx.y * n + i;
   const double d = sign * dp[(long)blockIdx.y * dstride];
-  c[o] = (T)fma(d, (double)b[o], (double)a[o]);
+  const Pack<T, V> av = ldpk<T, V>(a + o), bv = ldpk<T, V>(b + o);
+  Pack<T, V> cv;
+#pragma unroll
+  for (int k = 0; k < V; ++k) cv.v[k] = (T)fma(d, (double)bv.v[k], (double)av.v[k]);
+  stpk<T, V>(c + o, cv);
 }
 
 // ---- fused DIIS passes.  Each forms the trial vectors of ksdiis_r on the
@@ -393,14 +398,14 @@ __global__ void k_diis_dots_a(long n, const T* __restrict__ ps, const T* __restr
 // DIIS matrix sums (ksdiis8f.F90:321-404) with the step lam of band j:
 //   ps.ss, rvv0.rvv0, ps.sph1, rvv0.rvv1, ph1.sph1, rvv1.rvv1 with
 //   ph1 = ps + lam rvre, hph1 = hs + lam avre, sph1 = ss + lam asvre,
-//   rvv1 = hph1 - sval sph1.
+//   rvv1 = hph1 - sval sph1, and the first residual rvv0 = hs - sval ss
+//   formed again as ksdiis_r_01 formed it (so it is never stored).
 template <class T, bool SP>
 __global__ void k_diis_dots_b(long n, const T* __restrict__ ps, const T* __restrict__ rvre,
                               const T* __restrict__ hs, const T* __restrict__ avre,
                               const T* __restrict__ ss, const T* __restrict__ asvre,
-                              const T* __restrict__ rvv0, const Sc* __restrict__ sc,
-                              const double* __restrict__ sval, long nblk,
-                              double* __restrict__ part) {
+                              const Sc* __restrict__ sc, const double* __restrict__ sval,
+                              long nblk, double* __restrict__ part) {
   __shared__ double ws[8];
   const int j = blockIdx.y, nb = gridDim.y;
   const long off = (long)j * n;
@@ -414,9 +419,10 @@ __global__ void k_diis_dots_b(long n, const T* __restrict__ ps, const T* __restr
       const long o = off + i;
       const double p = (double)ps[o];
       const double s = SP ? (double)ss[o] : p;
-      const double v0 = (double)rvv0[o];
+      const double h = (double)hs[o];
+      const double v0 = (double)(T)fma(ev, s, h);
       const T p1 = (T)fma(lam, (double)rvre[o], p);
-      const T h1 = (T)fma(lam, (double)avre[o], (double)hs[o]);
+      const T h1 = (T)fma(lam, (double)avre[o], h);
       const T s1 = SP ? (T)fma(lam, (double)asvre[o], s) : p1;
       const double v1 = (double)(T)fma(ev, (double)s1, (double)h1);
       acc[0] = fma(p, s, acc[0]);
@@ -452,27 +458,33 @@ __global__ void k_dots_final(long nblk, const double* __restrict__ part, double 
 
 // The DIIS combination (ksdiis8f.F90:549-600) of band j with the normalised
 // trial vectors: y1 = tmp * (y + lam dy), new = c1 y1 + c0 y for psi, S psi
-// (with an S metric) and H psi.
-template <class T, bool SP>
+// (with an S metric) and, when upd_h, H psi.  V consecutive values per thread
+// (V divides n).
+template <class T, bool SP, int V>
+__device__ __forceinline__ void diis_comb_vec(long o, T* y, const T* __restrict__ dy, double lam,
+                                              double t, double c0, double c1) {
+  const Pack<T, V> yv = ldpk<T, V>(y + o), dv = ldpk<T, V>(dy + o);
+  Pack<T, V> nv;
+#pragma unroll
+  for (int k = 0; k < V; ++k) {
+    const double a = (double)yv.v[k];
+    const T a1 = (T)((double)(T)fma(lam, (double)dv.v[k], a) * t);
+    nv.v[k] = (T)fma(c1, (double)a1, c0 * a);
+  }
+  stpk<T, V>(y + o, nv);
+}
+template <class T, bool SP, int V>
 __global__ void k_diis_comb(long n, T* ps, const T* __restrict__ rvre, T* hs,
                             const T* __restrict__ avre, T* ss, const T* __restrict__ asvre,
-                            const Sc* __restrict__ sc) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+                            const Sc* __restrict__ sc, int upd_h) {
+  const long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) * V;
   if (i >= n) return;
   const Sc& q = sc[blockIdx.y];
   const double lam = q.lam, t = q.tmp, c0 = q.c[0], c1 = q.c[1];
   const long o = (long)blockIdx.y * n + i;
-  const double p = (double)ps[o];
-  const T p1 = (T)((double)(T)fma(lam, (double)rvre[o], p) * t);
-  ps[o] = (T)fma(c1, (double)p1, c0 * p);
-  if (SP) {
-    const double s = (double)ss[o];
-    const T s1 = (T)((double)(T)fma(lam, (double)asvre[o], s) * t);
-    ss[o] = (T)fma(c1, (double)s1, c0 * s);
-  }
-  const double h = (double)hs[o];
-  const T h1 = (T)((double)(T)fma(lam, (double)avre[o], h) * t);
-  hs[o] = (T)fma(c1, (double)h1, c0 * h);
+  diis_comb_vec<T, SP, V>(o, ps, rvre, lam, t, c0, c1);
+  if (SP) diis_comb_vec<T, SP, V>(o, ss, asvre, lam, t, c0, c1);
+  if (upd_h) diis_comb_vec<T, SP, V>(o, hs, avre, lam, t, c0, c1);
 }
 __global__ void k_diis_comb_rp(long n, double* rps, const double* __restrict__ rpsep,
                                const Sc* __restrict__ sc) {
@@ -854,6 +866,8 @@ static int ksdiis(BandCtx<T>& c, const rs_solver_prm* prm, int l_hsv, double* sv
   double* dres = dval + M + 1;
   double* da1 = dres + M + 1;
   const double a1 = prm->alambda_diis;
+  constexpr int V = 16 / (int)sizeof(T);
+  auto aligned16 = [](const void* p) { return (uintptr_t)p % 16 == 0; };
   if (!rc) {
     cudaMemcpyAsync(dres, resid_h, sizeof(double) * M, cudaMemcpyHostToDevice, c.st);
     cudaMemcpyAsync(da1, &a1, sizeof(double), cudaMemcpyHostToDevice, c.st);
@@ -871,16 +885,22 @@ static int ksdiis(BandCtx<T>& c, const rs_solver_prm* prm, int l_hsv, double* sv
     T* hs = c.band(c.hpsi, b0);                // H phi0, computed afresh each sweep
     double* rps = c.rpb(c.rp, b0);
     const dim3 gv(div_up(N, 256), nb), gr(div_up(nrp > 0 ? nrp : 1, 256), nb);
+    const dim3 gvv(div_up(N / V, 256), nb);
+    // 16-byte vectors when a band is a whole number of them and every band
+    // vector starts on a 16-byte boundary
+    const bool vec = N % V == 0 && aligned16(ps) && aligned16(ss) && aligned16(hs) &&
+                     aligned16(wv);
     const dim3 gd((unsigned)c.nblk, nb);
     const unsigned gs = div_up(nb, 128);
     for (int jiter = 1; jiter + 1 <= prm->ndiismax && !rc; ++jiter) {
       if ((rc = c.apply_h(ps, rps, hs, nb))) break;
       pdot(ps, hs, nb, dval + b0, 1, 1);
-      k_axpy_b<T><<<gv, 256, 0, c.st>>>(N, hs, ss, dval + b0, 1, -1.0, rvv0);
-      if (prm->nprecon_diis) rc = launch_precondition<T>(c.g, rvv0, rvre, nb, c.st);
-      else rc = cudaMemcpyAsync(rvre, rvv0, sizeof(T) * N * nb, cudaMemcpyDeviceToDevice, c.st)
-                    == cudaSuccess ? RS_OK : RS_ECUDA;
-      if (rc) break;
+      // the first residual, smoothed into rvre (or rvre itself without a
+      // preconditioner)
+      T* r0 = prm->nprecon_diis ? rvv0 : rvre;
+      if (vec) k_axpy_b<T, V><<<gvv, 256, 0, c.st>>>(N, hs, ss, dval + b0, 1, -1.0, r0);
+      else k_axpy_b<T, 1><<<gv, 256, 0, c.st>>>(N, hs, ss, dval + b0, 1, -1.0, r0);
+      if (prm->nprecon_diis && (rc = launch_precondition<T>(c.g, rvv0, rvre, nb, c.st))) break;
       if ((rc = c.nl_dot(rvre, rpsep, nb))) break;
       if ((rc = c.apply_h(rvre, rpsep, avre, nb))) break;
       if (sp && (rc = c.apply_s(rvre, rpsep, asvre, nb))) break;
@@ -902,10 +922,10 @@ static int ksdiis(BandCtx<T>& c, const rs_solver_prm* prm, int l_hsv, double* sv
       // the 2x2 DIIS matrices at the step lam, in one pass
       if (sp)
         k_diis_dots_b<T, true><<<gd, kTreeLanes, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre,
-                                                            rvv0, scb, dval + b0, c.nblk, dpart);
+                                                            scb, dval + b0, c.nblk, dpart);
       else
         k_diis_dots_b<T, false><<<gd, kTreeLanes, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre,
-                                                             rvv0, scb, dval + b0, c.nblk, dpart);
+                                                             scb, dval + b0, c.nblk, dpart);
       {
         DotOuts o{};
         double* outs[6] = {&scb->rs[0], &scb->rr[0], &scb->rs[1],
@@ -918,8 +938,19 @@ static int ksdiis(BandCtx<T>& c, const rs_solver_prm* prm, int l_hsv, double* sv
       k_diis_scale_mats_b<<<gs, 128, 0, c.st>>>(nb, scb);
       k_diis_solve_b<<<gs, 128, 0, c.st>>>(nb, scb, prm->eps_eig_diis, dres + b0);
       // combination with the normalised trial vectors (formed again on the fly)
-      if (sp) k_diis_comb<T, true><<<gv, 256, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre, scb);
-      else k_diis_comb<T, false><<<gv, 256, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre, scb);
+      // H phi is recomputed at the top of the next sweep: only the last sweep
+      // leaves the combined H psi
+      const int upd_h = jiter + 2 > prm->ndiismax;
+      if (vec && sp)
+        k_diis_comb<T, true, V><<<gvv, 256, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre, scb, upd_h);
+      else if (vec)
+        k_diis_comb<T, false, V><<<gvv, 256, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre, scb,
+                                                        upd_h);
+      else if (sp)
+        k_diis_comb<T, true, 1><<<gv, 256, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre, scb, upd_h);
+      else
+        k_diis_comb<T, false, 1><<<gv, 256, 0, c.st>>>(N, ps, rvre, hs, avre, ss, asvre, scb,
+                                                       upd_h);
       if (nrp) k_diis_comb_rp<<<gr, 256, 0, c.st>>>(nrp, rps, rpsep, scb);
       e = cudaGetLastError();
       if (e != cudaSuccess) rc = cuda_status(e, "ksdiis");

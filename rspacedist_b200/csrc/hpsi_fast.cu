@@ -288,52 +288,6 @@ __global__ void __launch_bounds__(128) k_nl_rmw_f32(
     if (b < nbb) out[(long)(b0 + b) * N + p] = h[b];
 }
 
-// S psi = psi + sum_e t[atom_e][b] . p_e on every point (nhs = 0 with the
-// overlap matrix sss), NL_BANDS bands per thread: a point's inverse-list
-// entries are read once for 16 bands, psi is read and S psi written once.
-// Same entry order and sums as the per-band gather.
-__global__ void __launch_bounds__(128) k_spsi_f32(
-    const int* __restrict__ inv_off, const int* __restrict__ inv_atom,
-    const float* __restrict__ inv_v, const float* __restrict__ tco, int P, long N, int nb,
-    const float* psi, float* out) {  // psi == out allowed: a thread reads its values first
-  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= N) return;
-  const int b0 = blockIdx.y * NL_BANDS;
-  const int nbb = min(NL_BANDS, nb - b0);
-  const int e0 = __ldg(inv_off + p), e1 = __ldg(inv_off + p + 1);
-  float h[NL_BANDS];
-#pragma unroll
-  for (int b = 0; b < NL_BANDS; ++b) h[b] = b < nbb ? psi[(long)(b0 + b) * N + p] : 0.f;
-  const int nq = P / 4;
-  for (int e = e0; e < e1; ++e) {
-    const int at = __ldg(inv_atom + e);
-    float4 v[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] = k < nq ? ld4(inv_v + (long)e * P + 4 * k) : zero4();
-    const float* tb = tco + ((long)at * nb + b0) * P;
-#pragma unroll
-    for (int b = 0; b < NL_BANDS; ++b) {
-      if (b < nbb) {
-        float s = 0.f;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          if (k < nq) {
-            const float4 t = ld4(tb + (long)b * P + 4 * k);
-            s = fmaf(t.x, v[k].x, s);
-            s = fmaf(t.y, v[k].y, s);
-            s = fmaf(t.z, v[k].z, s);
-            s = fmaf(t.w, v[k].w, s);
-          }
-        }
-        h[b] += s;
-      }
-    }
-  }
-#pragma unroll
-  for (int b = 0; b < NL_BANDS; ++b)
-    if (b < nbb) out[(long)(b0 + b) * N + p] = h[b];
-}
-
 }  // namespace
 
 int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
@@ -390,12 +344,20 @@ int launch_spsi_f32_fast(const rs_geom* g, const double* sss, const double* rp, 
   RS_CUDA(cudaMallocAsync((void**)&t, nt * sizeof(float), st));
   k_tcoef_f32<<<div_up(nt, 256), 256, 0, st>>>(g->natom, g->nprjmx, g->d_nprj, sss, rp,
                                                1.0 / (g->dx * g->dy * g->dz), nb, t);
-  dim3 grid(div_up(g->N, 128), div_up(nb, NL_BANDS));
-  k_spsi_f32<<<grid, 128, 0, st>>>(g->d_inv_off, g->d_inv_atom, g->d_inv_v32, t, g->nprjmx, g->N,
-                                   nb, psi, out);
-  cudaError_t e = cudaGetLastError();
+  // out = psi, then the nonlocal sums added on the points inside a projector
+  // support only: the same entries, sums and order as the per-band gather,
+  // and the other points keep psi unchanged
+  cudaError_t e = cudaSuccess;
+  if (out != psi)
+    e = cudaMemcpyAsync(out, psi, sizeof(float) * g->N * nb, cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess && g->n_cov > 0) {
+    dim3 g2(div_up(g->n_cov, 128), div_up(nb, NL_BANDS));
+    k_nl_rmw_f32<<<g2, 128, 0, st>>>(g->d_cov, g->d_cov_off, g->n_cov, g->d_inv_atom,
+                                      g->d_inv_v32, t, g->nprjmx, g->N, nb, out);
+    e = cudaGetLastError();
+  }
   cudaFreeAsync(t, st);
-  if (e != cudaSuccess) return cuda_status(e, "k_spsi_f32");
+  if (e != cudaSuccess) return cuda_status(e, "S psi (k_nl_rmw_f32)");
   return RS_OK;
 }
 

@@ -84,6 +84,20 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 
 inline unsigned div_up(long a, long b) { return (unsigned)((a + b - 1) / b); }
 
+// V consecutive values of T moved as one aligned vector access
+template <class T, int V>
+struct alignas(sizeof(T) * V) Pack {
+  T v[V];
+};
+template <class T, int V>
+__device__ __forceinline__ Pack<T, V> ldpk(const T* p) {
+  return *reinterpret_cast<const Pack<T, V>*>(p);
+}
+template <class T, int V>
+__device__ __forceinline__ void stpk(T* p, const Pack<T, V>& x) {
+  *reinterpret_cast<Pack<T, V>*>(p) = x;
+}
+
 void fd_coefs(int nf, double a[9]);
 
 }  // namespace rs

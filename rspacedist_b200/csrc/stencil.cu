@@ -66,6 +66,112 @@ __global__ void k_precondition(int nx, int ny, int nz, const T* __restrict__ in,
   }
 }
 
+// Plane-marching form of k_precondition for grids whose x-rows split into
+// 16-byte vectors (V points of T).  A CTA owns TY whole x-rows of one band
+// and walks a run of z planes.  Each plane, with one halo row on either side
+// in y, is copied into a shared ring with 16-byte cp.async, kPzAhead planes
+// ahead of the plane being smoothed, so HBM latency hides behind the copies
+// in flight and every value crosses HBM once per band (the halo rows come
+// from L2, loaded by the neighbouring tiles).  A thread smooths V points of
+// one row from the ring: the same seven fmas in the same order as
+// k_precondition.
+constexpr int kPzAhead = 2;
+constexpr int kPzRing = kPzAhead + 4;  // planes z-1..z+1, the ones in flight, the one issued
+constexpr int kPzThreads = 256;
+constexpr int kPzZChunk = 32;
+
+__device__ __forceinline__ void pz_cp16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void pz_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void pz_wait_ahead() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(kPzAhead) : "memory");
+}
+
+template <class T>
+using PzVec = Pack<T, 16 / (int)sizeof(T)>;
+
+template <class T>
+__global__ void __launch_bounds__(kPzThreads) k_precondition_zm(int nx, int ny, int nz, int ty_rows,
+                                                                int nty, int zc,
+                                                                const T* __restrict__ in,
+                                                                T* __restrict__ out) {
+  constexpr int V = 16 / (int)sizeof(T);
+  extern __shared__ __align__(16) unsigned char pz_smem[];
+  T* ring = reinterpret_cast<T*>(pz_smem);  // [kPzRing][ty_rows + 2][nx]
+  const int nxv = nx / V;
+  const int rows = ty_rows + 2;
+  const long slot = (long)rows * nx;
+  const int tid = threadIdx.x;
+  const int tx = tid % nxv, ty = tid / nxv;  // rows past ny in the last tile stay idle
+  const int ytile = blockIdx.x % nty, zt = blockIdx.x / nty;
+  const int y0 = ytile * ty_rows;
+  const int z0 = zt * zc, z1 = min(nz, z0 + zc);
+  const long plane = (long)nx * ny;
+  const T* v = in + (long)blockIdx.y * plane * nz;
+  T* o = out + (long)blockIdx.y * plane * nz;
+  const int nchunk = rows * nxv;
+  // copy plane zz (wrapped) with its halo rows into its ring slot, one group
+  auto issue = [&](int zz) {
+    const int zw = zz < 0 ? zz + nz : (zz >= nz ? zz - nz : zz);
+    T* dst = ring + (long)((zz - z0 + 1 + kPzRing) % kPzRing) * slot;
+    const T* src = v + (long)zw * plane;
+    for (int c = tid; c < nchunk; c += blockDim.x) {
+      const int r = c / nxv, cx = c - r * nxv;
+      int yr = y0 - 1 + r;
+      yr = yr < 0 ? yr + ny : (yr >= ny ? yr - ny : yr);
+      pz_cp16(dst + (long)r * nx + cx * V, src + (long)yr * nx + cx * V);
+    }
+    pz_commit();
+  };
+  // planes z0-1 .. z0+1+kPzAhead (the last one needed is z1)
+  for (int zz = z0 - 1; zz <= z0 + 1 + kPzAhead; ++zz) {
+    if (zz <= z1) issue(zz);
+    else pz_commit();
+  }
+  const T c = (T)(1.0 / 12.0), h = (T)0.5;
+  const int iy = y0 + ty;
+  const bool active = ty < ty_rows && iy < ny;
+  const int xm = tx == 0 ? nx - 1 : tx * V - 1;
+  const int xp = tx == nxv - 1 ? 0 : tx * V + V;
+  for (int z = z0; z < z1; ++z) {
+    pz_wait_ahead();
+    __syncthreads();
+    // the slot of plane z+2+kPzAhead last held plane z-2, read before the barrier
+    if (z + 2 + kPzAhead <= z1) issue(z + 2 + kPzAhead);
+    else pz_commit();
+    if (active) {
+      const T* sm = ring + (long)((z - z0 + kPzRing) % kPzRing) * slot;   // plane z-1
+      const T* s0 = ring + (long)((z - z0 + 1) % kPzRing) * slot;         // plane z
+      const T* sp = ring + (long)((z - z0 + 2) % kPzRing) * slot;         // plane z+1
+      const int r = ty + 1;
+      PzVec<T> a0 = *reinterpret_cast<const PzVec<T>*>(s0 + (long)r * nx + tx * V);
+      PzVec<T> aym = *reinterpret_cast<const PzVec<T>*>(s0 + (long)(r - 1) * nx + tx * V);
+      PzVec<T> ayp = *reinterpret_cast<const PzVec<T>*>(s0 + (long)(r + 1) * nx + tx * V);
+      PzVec<T> azm = *reinterpret_cast<const PzVec<T>*>(sm + (long)r * nx + tx * V);
+      PzVec<T> azp = *reinterpret_cast<const PzVec<T>*>(sp + (long)r * nx + tx * V);
+      const T left = s0[(long)r * nx + xm], right = s0[(long)r * nx + xp];
+      PzVec<T> res;
+#pragma unroll
+      for (int k = 0; k < V; ++k) {
+        const T xl = k == 0 ? left : a0.v[k - 1];
+        const T xr = k == V - 1 ? right : a0.v[k + 1];
+        T t = c * xl;
+        t = fma(c, aym.v[k], t);
+        t = fma(c, azm.v[k], t);
+        t = fma(h, a0.v[k], t);
+        t = fma(c, azp.v[k], t);
+        t = fma(c, ayp.v[k], t);
+        t = fma(c, xr, t);
+        res.v[k] = t;
+      }
+      *reinterpret_cast<PzVec<T>*>(o + (long)z * plane + (long)iy * nx + tx * V) = res;
+    }
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // scf_hartee_laplacian (scf_hartree8f.F90:949-1004): the x pass starts from
 // the first product; diagonal = hadx+hady+hadz with had = acfdh(0)/(d*d)*(-1/2).
 __global__ void k_hartree_lap(int nx, int ny, int nz, int nf, HartreeCoefs c,
@@ -164,6 +270,28 @@ int launch_kslaplacian(const rs_geom* g, const T* psi, const T* veff, T* out, in
 template <class T>
 int launch_precondition(const rs_geom* g, const T* in, T* out, int nb, cudaStream_t st) {
   if (nb <= 0) return RS_OK;
+  if (nb > 65535) return fail(RS_EINVAL, "precondition: nb > 65535");
+  constexpr int V = 16 / (int)sizeof(T);
+  const int nxv = g->nx / V;
+  const bool aligned = ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0);
+  if (g->nx % V == 0 && nxv >= 1 && nxv <= kPzThreads && aligned && in != out) {
+    const int tyr = std::max(1, std::min(g->ny, kPzThreads / nxv));
+    const int nty = (g->ny + tyr - 1) / tyr;
+    // z runs of up to kPzZChunk planes, shorter when few bands leave SMs idle
+    int zc = std::min(g->nz, kPzZChunk);
+    while (zc > 4 && (long)nty * div_up(g->nz, zc) * nb < 148L * 8) zc = (zc + 1) / 2;
+    const int nzc = (g->nz + zc - 1) / zc;
+    const size_t smem = sizeof(T) * (size_t)kPzRing * (tyr + 2) * g->nx;
+    if (smem <= 200 * 1024 && (long)nty * nzc < (1L << 31)) {
+      RS_CUDA(cudaFuncSetAttribute(k_precondition_zm<T>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      dim3 grid((unsigned)(nty * nzc), nb);
+      k_precondition_zm<T><<<grid, nxv * tyr, smem, st>>>(g->nx, g->ny, g->nz, tyr, nty, zc, in,
+                                                           out);
+      RS_LAUNCH_CHECK("k_precondition_zm");
+      return RS_OK;
+    }
+  }
   const long nrow = (long)g->ny * g->nz;
   const int thr = g->nx >= 128 ? 128 : (g->nx + 31) / 32 * 32;
   dim3 grid((unsigned)div_up(nrow, kPrecRows), nb);
