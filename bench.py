@@ -516,7 +516,7 @@ def run_hartree_profile(n, mixed=False):
     rho_d = torch.tensor(rho.ravel(), device="cuda")
     vh = torch.zeros_like(rho_d)
     xm = (a / 2,) * 3
-    K.scf_hartree((n, n, n), 4, xm, rho_d, vh, 1e-12, ncgmax=50)
+    K.scf_hartree((n, n, n), 4, xm, rho_d, vh, 1e-12, ncgmax=50, mixed=mixed)
     torch.cuda.synchronize()
     vh.zero_()
     side = torch.cuda.Stream()  # a real stream: the solve replays its batches as a graph

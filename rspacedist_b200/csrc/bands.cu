@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "reduce.cuh"
@@ -526,15 +527,15 @@ __global__ void k_diis_solve_b(int nb, Sc* sc, double eps_eig, double* __restric
   if (j < nb) diis_solve(sc + j, eps_eig, resid + j);
 }
 
-// dst band dband[k] = src band sband[k] for k < K (bands of n values)
-template <class T>
-__global__ void k_move_bands(long n, int K, const int* __restrict__ sband, const T* __restrict__ src,
+// dst band dband[k] = src band sband[k] for k = blockIdx.y (bands of n
+// values, V consecutive values per thread, V divides n)
+template <class T, int V>
+__global__ void k_move_bands(long n, const int* __restrict__ sband, const T* __restrict__ src,
                              const int* __restrict__ dband, T* __restrict__ dst) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n * K) return;
-  const int k = (int)(i / n);
-  const long e = i % n;
-  dst[(long)dband[k] * n + e] = src[(long)sband[k] * n + e];
+  const long e = ((long)blockIdx.x * blockDim.x + threadIdx.x) * V;
+  if (e >= n) return;
+  const int k = blockIdx.y;
+  stpk<T, V>(dst + (long)dband[k] * n + e, ldpk<T, V>(src + (long)sband[k] * n + e));
 }
 
 }  // namespace
@@ -1050,18 +1051,37 @@ static int reorder(BandCtx<T>& c, double* sval_h, double* resid_h) {
   const int* from = dmv;
   const int* to = dmv + K;
   const int* slot = dmv + 2 * K;
+  // gather the moving bands into tmp, then scatter them to their ranks, in
+  // launches of at most 65535 bands
+  auto move = [&](auto* a, long n, bool vec) {
+    using U = std::remove_pointer_t<decltype(a)>;
+    constexpr int V = 16 / (int)sizeof(U);
+    U* b = (U*)tmp;
+    for (int k0 = 0; k0 < K; k0 += 65535) {
+      const int kc = std::min(65535, K - k0);
+      if (vec) {
+        const dim3 grid(div_up(n / V, 256), kc);
+        k_move_bands<U, V><<<grid, 256, 0, c.st>>>(n, from + k0, a, slot + k0, b);
+      } else {
+        const dim3 grid(div_up(n, 256), kc);
+        k_move_bands<U, 1><<<grid, 256, 0, c.st>>>(n, from + k0, a, slot + k0, b);
+      }
+    }
+    for (int k0 = 0; k0 < K; k0 += 65535) {
+      const int kc = std::min(65535, K - k0);
+      if (vec) {
+        const dim3 grid(div_up(n / V, 256), kc);
+        k_move_bands<U, V><<<grid, 256, 0, c.st>>>(n, slot + k0, b, to + k0, a);
+      } else {
+        const dim3 grid(div_up(n, 256), kc);
+        k_move_bands<U, 1><<<grid, 256, 0, c.st>>>(n, slot + k0, b, to + k0, a);
+      }
+    }
+  };
   T* arrs[2] = {c.psi, c.sep() ? c.spsi : nullptr};
-  for (T* a : arrs) {
-    if (!a) continue;
-    k_move_bands<T><<<div_up(N * K, 256), 256, 0, c.st>>>(N, K, from, a, slot, (T*)tmp);
-    k_move_bands<T><<<div_up(N * K, 256), 256, 0, c.st>>>(N, K, slot, (T*)tmp, to, a);
-  }
-  if (nrp) {
-    k_move_bands<double><<<div_up((long)nrp * K, 256), 256, 0, c.st>>>(nrp, K, from, c.rp, slot,
-                                                                        (double*)tmp);
-    k_move_bands<double><<<div_up((long)nrp * K, 256), 256, 0, c.st>>>(nrp, K, slot,
-                                                                        (double*)tmp, to, c.rp);
-  }
+  for (T* a : arrs)
+    if (a) move(a, N, N % (16 / (long)sizeof(T)) == 0 && (uintptr_t)a % 16 == 0);
+  if (nrp) move(c.rp, (long)nrp, false);
   cudaFreeAsync(dmv, c.st);
   cudaFreeAsync(tmp, c.st);
   cudaError_t e = cudaStreamSynchronize(c.st);

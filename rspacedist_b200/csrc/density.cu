@@ -523,15 +523,18 @@ __global__ void k_cg_dir(long N, const CgScalars* __restrict__ s, const double* 
 // ---------------------------------------------------------------- mixed CG
 // The Hartree CG of the mixed path: the same iteration as hartree_cg (kukan's
 // recurrences, restart, stopping rule, device-side folds and graph batches),
-// with the vectors p, A p, r, A x and b in FP32 and the solution vh, every dot
-// product and every residual norm in FP64.  The A p stencil is the paired
-// z-march in FP32.
+// with the vectors p, A p and r in FP32 and the solution vh, every dot
+// product and every residual norm in FP64.  Between two FP64 residuals the
+// solution change dvh accumulates in FP32 and is then added into vh.  The A p
+// stencil is the paired z-march in FP32 and also sums p.Ap, one partial per
+// CTA.
 template <int NF>
 __global__ void __launch_bounds__(HZ2_THREADS, 1) k_hlap_zmarch2f(int nx, int ny, int nz,
                                                                   int zchunk, HartreeCoefs c,
                                                                   const float* __restrict__ p,
                                                                   float* __restrict__ ap,
-                                                                  const CgScalars* __restrict__ s) {
+                                                                  const CgScalars* __restrict__ s,
+                                                                  double* __restrict__ part) {
   static_assert(NF % 2 == 0, "float2 path needs an even halo");
   if (s->done) return;
   constexpr int HX = HZ2_TX + 2 * NF, HY = HZ2_TY + 2 * NF, PL = HX * HY, RING = hz2_ring(NF);
@@ -582,6 +585,7 @@ __global__ void __launch_bounds__(HZ2_THREADS, 1) k_hlap_zmarch2f(int nx, int ny
     cp_commit_hz();
   };
   float2 q[2 * NF + 1];
+  double pacc = 0.0;  // p . A p over this thread's points
 #pragma unroll
   for (int k = 0; k < NF; ++k)
     q[k] = __ldg(reinterpret_cast<const float2*>(p + (long)wrapz(zs - NF + k) * plane + own));
@@ -640,72 +644,113 @@ __global__ void __launch_bounds__(HZ2_THREADS, 1) k_hlap_zmarch2f(int nx, int ny
       a0 = fmaf(cz[m], q[NF + m].x, a0);
       a1 = fmaf(cz[m], q[NF + m].y, a1);
     }
-    if (active) *reinterpret_cast<float2*>(ap + (long)z * plane + own) = make_float2(a0, a1);
+    if (active) {
+      *reinterpret_cast<float2*>(ap + (long)z * plane + own) = make_float2(a0, a1);
+      pacc = fma((double)q[NF].x, (double)a0, pacc);
+      pacc = fma((double)q[NF].y, (double)a1, pacc);
+    }
 #pragma unroll
     for (int k = 0; k < 2 * NF; ++k) q[k] = q[k + 1];
   }
   cp_wait_hz<0>();
-}
-
-__global__ void __launch_bounds__(kTreeLanes) k_cg_pap_f(long N, const float* __restrict__ p,
-                                                         const float* __restrict__ ap,
-                                                         double* __restrict__ part,
-                                                         const CgScalars* __restrict__ s) {
-  if (s->done) return;
-  __shared__ double ws[8];
-  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
-  double acc = 0.0;
-#pragma unroll 4
-  for (int k = 0; k < kTreePerLane; ++k) {
-    const long i = base + (long)k * kTreeLanes;
-    if (i < N) acc = fma((double)p[i], (double)ap[i], acc);
+  // this CTA's share of p.Ap, summed in a fixed order (warps, then lanes)
+  __shared__ double ws[HZ2_THREADS / 32];
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) pacc = pacc + __shfl_down_sync(0xffffffffu, pacc, off);
+  if ((tid & 31) == 0) ws[tid >> 5] = pacc;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < HZ2_THREADS / 32; ++w) t = t + ws[w];
+    part[blockIdx.x] = t;
   }
-  const double t = tree_fold256(acc, ws);
-  if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-// vh += alpha p (FP64), r -= alpha A p (FP32), r.r chunk sums (FP64)
-__global__ void __launch_bounds__(kTreeLanes) k_cg_update_f(long N, const CgScalars* s,
-                                                            double* __restrict__ vh,
+// alpha = r.r / p.Ap from the stencil's per-CTA partials (every block folds
+// them in the same order), then dvh += alpha p and r -= alpha A p (FP32, the
+// same alpha) and the r.r sum of this 4096-point chunk (FP64).  V consecutive
+// values per lane (V divides N).  dvh, the change of the solution since the
+// last FP64 residual, is added into vh (FP64) by k_cg_fold_dvh before each
+// FP64 residual.
+template <int V>
+__global__ void __launch_bounds__(kTreeLanes) k_cg_update_f(long N, CgScalars* s, long npap,
+                                                            const double* __restrict__ pap_part,
+                                                            float* __restrict__ dvh,
                                                             const float* __restrict__ p,
                                                             const float* __restrict__ ap,
                                                             float* __restrict__ r,
                                                             double* __restrict__ part) {
   if (s->done) return;
   __shared__ double ws[8];
-  const double alph = s->alph;
-  const float alf = (float)alph;
-  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  __shared__ double alph_s;
+  double q = 0.0;
+  for (long k = threadIdx.x; k < npap; k += kTreeLanes) q = q + pap_part[k];
+  q = tree_fold256(q, ws);
+  if (threadIdx.x == 0) {
+    alph_s = s->r1r / q;
+    if (blockIdx.x == 0) {
+      s->pap = q;
+      s->alph = alph_s;
+    }
+  }
+  __syncthreads();
+  const float alf = (float)alph_s;
+  const long base = (long)blockIdx.x * kTreeChunk + (long)threadIdx.x * V;
   double acc = 0.0;
-#pragma unroll 4
-  for (int k = 0; k < kTreePerLane; ++k) {
-    const long i = base + (long)k * kTreeLanes;
+#pragma unroll
+  for (int k = 0; k < kTreePerLane / V; ++k) {
+    const long i = base + (long)k * kTreeLanes * V;
     if (i < N) {
-      vh[i] = fma(alph, (double)p[i], vh[i]);
-      const float ri = fmaf(-alf, ap[i], r[i]);
-      r[i] = ri;
-      acc = fma((double)ri, (double)ri, acc);
+      Pack<float, V> dv = ldpk<float, V>(dvh + i), rv = ldpk<float, V>(r + i);
+      const Pack<float, V> pv = ldpk<float, V>(p + i), av = ldpk<float, V>(ap + i);
+#pragma unroll
+      for (int c = 0; c < V; ++c) {
+        dv.v[c] = fmaf(alf, pv.v[c], dv.v[c]);
+        rv.v[c] = fmaf(-alf, av.v[c], rv.v[c]);
+        acc = fma((double)rv.v[c], (double)rv.v[c], acc);
+      }
+      stpk<float, V>(dvh + i, dv);
+      stpk<float, V>(r + i, rv);
     }
   }
   const double t = tree_fold256(acc, ws);
   if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
+// blocks of the kernels that only run at an FP64 residual (and return at once
+// otherwise): a grid-stride loop over a few waves keeps the idle launches short
+constexpr unsigned kGatedBlocks = 148 * 8;
+
+// vh += dvh (FP64), dvh = 0, when an FP64 residual follows
+__global__ void k_cg_fold_dvh(long N, const CgScalars* __restrict__ s, float* __restrict__ dvh,
+                              double* __restrict__ vh) {
+  if (s->done || !s->upd) return;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (long)gridDim.x * blockDim.x) {
+    vh[i] = vh[i] + (double)dvh[i];
+    dvh[i] = 0.f;
+  }
+}
+
 // r.r chunk sums of the FP32 residual, after it was recomputed in FP64
-__global__ void __launch_bounds__(kTreeLanes) k_cg_rr_f(long N, const CgScalars* s,
+// (blocks stride over the 4096-point chunks)
+__global__ void __launch_bounds__(kTreeLanes) k_cg_rr_f(long N, long nblk, const CgScalars* s,
                                                         const float* __restrict__ r,
                                                         double* __restrict__ part) {
   if (s->done || !s->upd) return;
   __shared__ double ws[8];
-  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
-  double acc = 0.0;
+  for (long cb = blockIdx.x; cb < nblk; cb += gridDim.x) {
+    const long base = cb * kTreeChunk + threadIdx.x;
+    double acc = 0.0;
 #pragma unroll 4
-  for (int k = 0; k < kTreePerLane; ++k) {
-    const long i = base + (long)k * kTreeLanes;
-    if (i < N) acc = fma((double)r[i], (double)r[i], acc);
+    for (int k = 0; k < kTreePerLane; ++k) {
+      const long i = base + (long)k * kTreeLanes;
+      if (i < N) acc = fma((double)r[i], (double)r[i], acc);
+    }
+    const double t = tree_fold256(acc, ws);
+    if (threadIdx.x == 0) part[cb] = t;
   }
-  const double t = tree_fold256(acc, ws);
-  if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
 // beta, dp and the stopping rule of scf_hartree_cg from r2r (shared by the
@@ -771,13 +816,19 @@ __global__ void k_cg_fold_upd_f(long nblk, const double* __restrict__ part, CgSc
   }
 }
 
-// p = r + beta p (FP32)
+// p = r + beta p (FP32), V consecutive values per thread (V divides N)
+template <int V>
 __global__ void k_cg_dir_f(long N, const CgScalars* __restrict__ s, const float* __restrict__ r,
                            float* __restrict__ p) {
   if (s->done) return;
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) * V;
   if (i >= N) return;
-  p[i] = fmaf((float)s->beta, p[i], r[i]);
+  const float beta = (float)s->beta;
+  const Pack<float, V> rv = ldpk<float, V>(r + i);
+  Pack<float, V> pv = ldpk<float, V>(p + i);
+#pragma unroll
+  for (int k = 0; k < V; ++k) pv.v[k] = fmaf(beta, pv.v[k], rv.v[k]);
+  stpk<float, V>(p + i, pv);
 }
 
 __global__ void k_to_f32x2(long N, const double* __restrict__ a, const double* __restrict__ b,
@@ -814,7 +865,14 @@ int hlap_zmarch_attr(int nfh) {
   return e == cudaSuccess ? RS_OK : cuda_status(e, "k_hlap_zmarch");
 }
 
-// work32: nullptr for the FP64 solve; 3 N floats for the mixed solve (used
+bool hartree_ap_f32_ok(int nx, int ny, int nz, int nfh);
+unsigned hartree_ap_f32_ctas(int nx, int ny, int nz);
+int hartree_ap_f32_attr();
+int launch_hartree_ap_f32(int nx, int ny, int nz, const double* cx, const double* cy,
+                          const double* cz, double diag, const float* p, float* ap,
+                          const int* done, double* part, cudaStream_t st);
+
+// work32: nullptr for the FP64 solve; 4 N floats for the mixed solve (used
 // when nfh and nx are even, which its paired FP32 stencil needs; other grids
 // run the FP64 iteration)
 int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double zmax,
@@ -881,11 +939,17 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
   // a stream other than the legacy one the batch is captured once as a CUDA
   // graph and replayed.
   const bool mixed = work32 != nullptr && pairs;
-  float *fr = nullptr, *fp = nullptr, *fap = nullptr;
+  // nfh = 4 grids with x in whole 16-byte vectors take the 4 x 2 point z-march
+  // of H psi for A p; the others the paired Hartree z-march
+  const bool wide_ap = mixed && hartree_ap_f32_ok(nx, ny, nz, nfh);
+  const unsigned nap = wide_ap ? hartree_ap_f32_ctas(nx, ny, nz) : gz;
+  float *fr = nullptr, *fp = nullptr, *fap = nullptr, *fdv = nullptr;
   if (mixed) {
     fr = work32;
     fp = fr + N;
     fap = fp + N;
+    fdv = fap + N;
+    RS_CUDA(cudaMemsetAsync(fdv, 0, sizeof(float) * N, st));
     k_to_f32x2<<<gN, 256, 0, st>>>(N, r, p, fr, fp);
     k_cg_ref<<<1, 1, 0, st>>>(sc);
     cudaError_t e = cudaFuncSetAttribute(
@@ -899,29 +963,40 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
                                : (const void*)k_hlap_zmarch2<6, true>),
           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hz2_smem(nfh));
     if (e != cudaSuccess) return cuda_status(e, "mixed Hartree CG kernels");
+    if (wide_ap && (rc = hartree_ap_f32_attr())) return rc;
   }
   // one mixed iteration: FP32 A p and update, then (when asked) the FP64
   // residual b - A vh rounded into r, its r.r, and the closing fold
   auto iter32 = [&]() {
-    switch (nfh) {
-      case 2: k_hlap_zmarch2f<2><<<gz, HZ2_THREADS, hz2_smem(2) / 2, st>>>(nx, ny, nz, zchunk, hc, fp, fap, sc); break;
-      case 4: k_hlap_zmarch2f<4><<<gz, HZ2_THREADS, hz2_smem(4) / 2, st>>>(nx, ny, nz, zchunk, hc, fp, fap, sc); break;
-      default: k_hlap_zmarch2f<6><<<gz, HZ2_THREADS, hz2_smem(6) / 2, st>>>(nx, ny, nz, zchunk, hc, fp, fap, sc); break;
+    if (wide_ap)
+      launch_hartree_ap_f32(nx, ny, nz, hc.cx, hc.cy, hc.cz, hc.diag, fp, fap, &sc->done, ap, st);
+    else switch (nfh) {
+      case 2: k_hlap_zmarch2f<2><<<gz, HZ2_THREADS, hz2_smem(2) / 2, st>>>(nx, ny, nz, zchunk, hc, fp, fap, sc, ap); break;
+      case 4: k_hlap_zmarch2f<4><<<gz, HZ2_THREADS, hz2_smem(4) / 2, st>>>(nx, ny, nz, zchunk, hc, fp, fap, sc, ap); break;
+      default: k_hlap_zmarch2f<6><<<gz, HZ2_THREADS, hz2_smem(6) / 2, st>>>(nx, ny, nz, zchunk, hc, fp, fap, sc, ap); break;
     }
-    k_cg_pap_f<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, fp, fap, part, sc);
-    k_cg_fold_alpha<<<1, kTreeLanes, 0, st>>>(nblk, part, sc);
-    k_cg_update_f<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, vh, fp, fap, fr, part);
+    // p.Ap: one partial per stencil CTA (in the FP64 A p array, which the
+    // mixed iteration leaves unused), folded by every block of the update
+    if (N % 4 == 0)
+      k_cg_update_f<4><<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, (long)nap, ap, fdv, fp, fap,
+                                                              fr, part);
+    else
+      k_cg_update_f<1><<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, (long)nap, ap, fdv, fp, fap,
+                                                              fr, part);
     k_cg_fold_beta_f<<<1, kTreeLanes, 0, st>>>(nblk, part, sc, ncgres, ncgmin, lmax, epsvh, ddx,
                                                ddy, ddz, vol);
+    k_cg_fold_dvh<<<std::min(gN, kGatedBlocks), 256, 0, st>>>(N, sc, fdv, vh);
     switch (nfh) {
       case 2: k_hlap_zmarch2<2, true><<<gz, HZ2_THREADS, hz2_smem(2), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr); break;
       case 4: k_hlap_zmarch2<4, true><<<gz, HZ2_THREADS, hz2_smem(4), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr); break;
       default: k_hlap_zmarch2<6, true><<<gz, HZ2_THREADS, hz2_smem(6), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr); break;
     }
-    k_cg_rr_f<<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, fr, part);
+    k_cg_rr_f<<<std::min((unsigned)nblk, kGatedBlocks), kTreeLanes, 0, st>>>(N, nblk, sc, fr,
+                                                                              part);
     k_cg_fold_upd_f<<<1, kTreeLanes, 0, st>>>(nblk, part, sc, ncgres, ncgmin, lmax, epsvh, ddx,
                                               ddy, ddz, vol);
-    k_cg_dir_f<<<gN, 256, 0, st>>>(N, sc, fr, fp);
+    if (N % 4 == 0) k_cg_dir_f<4><<<div_up(N / 4, 256), 256, 0, st>>>(N, sc, fr, fp);
+    else k_cg_dir_f<1><<<gN, 256, 0, st>>>(N, sc, fr, fp);
   };
   auto batch = [&]() {
     for (int l = 0; l < kCgBatch; ++l) {
@@ -1089,7 +1164,7 @@ extern "C" int rs_hartree_cg_f32(int nx, int ny, int nz, int nfh, double xmax, d
   const long N = (long)nx * ny * nz;
   const long nblk = rs::tree_chunks(N);
   const size_t bytes64 = sizeof(double) * (5 * N + nblk + 1) + 2 * sizeof(double) * 8;
-  const size_t bytes = bytes64 + sizeof(float) * 3 * N + 16;
+  const size_t bytes = bytes64 + sizeof(float) * 4 * N + 16;
   double* work = nullptr;
   RS_CUDA(cudaMallocAsync((void**)&work, bytes, st));
   float* work32 = (float*)(((uintptr_t)work + bytes64 + 15) & ~(uintptr_t)15);

@@ -42,6 +42,10 @@ struct StArgs {
   const float* psi;
   float* out;
   const float* veff;
+  // Hartree form only: skip the launch when *done is set, and write this
+  // CTA's share of psi . out to part[blockIdx.x]
+  const int* done;
+  double* part;
 };
 
 __device__ __forceinline__ int wrap_once(int i, int n) {
@@ -73,7 +77,11 @@ __device__ __forceinline__ void cp_wait() {
 constexpr int RING = 8;    // staged planes (halo'd) in shared memory
 constexpr int AHEAD = 3;   // planes in flight beyond the queue's newest plane
 
+// HARTREE: the Hartree operator of the mixed CG, A p with diagonal c0 and
+// no veff, plus the p . A p partial of the CTA (one band).
+template <bool HARTREE>
 __global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
+  if (HARTREE && *a.done) return;
   extern __shared__ __align__(16) float smem_raw[];
   float (*pl)[HY][HX] = reinterpret_cast<float (*)[HY][HX]>(smem_raw);  // [RING][HY][HX]
   const int tid = threadIdx.x;
@@ -146,9 +154,12 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
     q[k][0] = *reinterpret_cast<const float4*>(&sl[ly][lx]);
     q[k][1] = *reinterpret_cast<const float4*>(&sl[ly + 1][lx]);
   }
-  float4 vreg[2];
-  vreg[0] = active ? ld4(a.veff + (long)zs * plane + own0) : zero4();
-  vreg[1] = active ? ld4(a.veff + (long)zs * plane + own1) : zero4();
+  float4 vreg[2] = {zero4(), zero4()};
+  if (!HARTREE && active) {
+    vreg[0] = ld4(a.veff + (long)zs * plane + own0);
+    vreg[1] = ld4(a.veff + (long)zs * plane + own1);
+  }
+  double pacc = 0.0;  // Hartree form: p . A p over this thread's points
 
   for (int z = zs; z < ze; ++z) {
     stage(z + 4 + AHEAD);   // reuses the slot of plane z-1 (freed by the last sync)
@@ -160,7 +171,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
       q[8][1] = *reinterpret_cast<const float4*>(&nw[ly + 1][lx]);
     }
     const float4 vcur[2] = {vreg[0], vreg[1]};
-    if (active && z + 1 < ze) {
+    if (!HARTREE && active && z + 1 < ze) {
       vreg[0] = ld4(a.veff + (long)(z + 1) * plane + own0);
       vreg[1] = ld4(a.veff + (long)(z + 1) * plane + own1);
     }
@@ -179,7 +190,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
           s = fmaf(a.cx[3], xv[i + 1], s);
           s = fmaf(a.cx[2], xv[i + 2], s);
           s = fmaf(a.cx[1], xv[i + 3], s);
-          s = fmaf(a.c0 + vv[i], xv[i + 4], s);
+          s = fmaf(HARTREE ? a.c0 : a.c0 + vv[i], xv[i + 4], s);
           s = fmaf(a.cx[1], xv[i + 5], s);
           s = fmaf(a.cx[2], xv[i + 6], s);
           s = fmaf(a.cx[3], xv[i + 7], s);
@@ -206,6 +217,12 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
         for (int m = 1; m <= 4; ++m) fma4(a.cz[m], q[4 + m][rr], acc);
         *reinterpret_cast<float4*>(out + (long)z * plane + (rr ? own1 : own0)) =
             make_float4(acc[0], acc[1], acc[2], acc[3]);
+        if (HARTREE) {
+          pacc = fma((double)C.x, (double)acc[0], pacc);
+          pacc = fma((double)C.y, (double)acc[1], pacc);
+          pacc = fma((double)C.z, (double)acc[2], pacc);
+          pacc = fma((double)C.w, (double)acc[3], pacc);
+        }
       }
     }
 #pragma unroll
@@ -216,6 +233,20 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
     __syncthreads();
   }
   cp_wait<0>();
+  if (HARTREE) {
+    // the CTA's sum in a fixed order: lanes of a warp, then the warps
+    __shared__ double ws[NTHREADS / 32];
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) pacc = pacc + __shfl_down_sync(0xffffffffu, pacc, off);
+    if ((tid & 31) == 0) ws[tid >> 5] = pacc;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+#pragma unroll
+      for (int k = 0; k < NTHREADS / 32; ++k) t = t + ws[k];
+      a.part[blockIdx.x] = t;
+    }
+  }
 }
 
 // t coefficients in atom-major order t[a][b][i] = (sum_j rp[b][a][j] m[a][i][j]) / dV
@@ -311,9 +342,11 @@ int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
   const int nzc = (g->nz + a.zchunk - 1) / a.zchunk;
   dim3 grid(a.ntx * a.nty * nzc, nb);
   const size_t smem = sizeof(float) * RING * HY * HX;
-  RS_CUDA(cudaFuncSetAttribute(k_stencil_f32_zmarch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem));
-  k_stencil_f32_zmarch<<<grid, NTHREADS, smem, st>>>(a);
+  a.done = nullptr;
+  a.part = nullptr;
+  RS_CUDA(cudaFuncSetAttribute(k_stencil_f32_zmarch<false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_stencil_f32_zmarch<false><<<grid, NTHREADS, smem, st>>>(a);
   RS_LAUNCH_CHECK("k_stencil_f32_zmarch");
   if (g->natom == 0 || g->n_cov == 0) return RS_OK;
   const long nt = (long)nb * g->natom * g->nprjmx;
@@ -327,6 +360,45 @@ int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
   cudaError_t e = cudaGetLastError();
   cudaFreeAsync(t, st);
   if (e != cudaSuccess) return cuda_status(e, "k_nl_rmw_f32");
+  return RS_OK;
+}
+
+// A p of the mixed Hartree CG (nfh = 4) by the H psi z-march: coefficients
+// cx, cy, cz [1..4] and diag from hartree_coefs, runs of 32 z planes (so one
+// grid fills the GPU), one p.Ap partial per CTA in part[0, *nparts).  The
+// launch returns at once when *done is set.
+bool hartree_ap_f32_ok(int nx, int ny, int nz, int nfh) {
+  return nfh == 4 && nx % 4 == 0 && ny % 2 == 0 && nx >= 8 && ny >= 8 && nz >= 8;
+}
+unsigned hartree_ap_f32_ctas(int nx, int ny, int nz) {
+  const int zchunk = nz <= 48 ? nz : 32;
+  return (unsigned)(((nx + TX - 1) / TX) * ((ny + TY - 1) / TY) * ((nz + zchunk - 1) / zchunk));
+}
+// shared-memory limit of the Hartree form; call before any stream capture
+int hartree_ap_f32_attr() {
+  RS_CUDA(cudaFuncSetAttribute(k_stencil_f32_zmarch<true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(sizeof(float) * RING * HY * HX)));
+  return RS_OK;
+}
+int launch_hartree_ap_f32(int nx, int ny, int nz, const double* cx, const double* cy,
+                          const double* cz, double diag, const float* p, float* ap,
+                          const int* done, double* part, cudaStream_t st) {
+  StArgs a;
+  a.nx = nx; a.ny = ny; a.nz = nz;
+  a.zchunk = nz <= 48 ? nz : 32;
+  a.ntx = (nx + TX - 1) / TX;
+  a.nty = (ny + TY - 1) / TY;
+  a.cx[0] = a.cy[0] = a.cz[0] = 0.f;
+  for (int m = 1; m < 5; ++m) {
+    a.cx[m] = (float)cx[m]; a.cy[m] = (float)cy[m]; a.cz[m] = (float)cz[m];
+  }
+  a.c0 = (float)diag;
+  a.psi = p; a.out = ap; a.veff = nullptr;
+  a.done = done; a.part = part;
+  const size_t smem = sizeof(float) * RING * HY * HX;
+  k_stencil_f32_zmarch<true><<<hartree_ap_f32_ctas(nx, ny, nz), NTHREADS, smem, st>>>(a);
+  RS_LAUNCH_CHECK("k_stencil_f32_zmarch (Hartree)");
   return RS_OK;
 }
 

@@ -50,6 +50,9 @@ constexpr int JB = 32;
 constexpr int JB2 = 2 * JB;
 constexpr int JLD = JB2 + 1;  // padded smem row
 constexpr int kBjThreads = 256;
+// the subproblem sweep is latency-bound (63 dependent rounds, two barriers
+// each): one rotation pair of S and two entries of Q per thread and round
+constexpr int kBjSolveThreads = 1024;
 
 __device__ __forceinline__ int bj_index(int I, int J, int k) {
   return k < JB ? I * JB + k : J * JB + (k - JB);
@@ -70,7 +73,7 @@ __device__ __forceinline__ Rot bj_params(const double (*S)[JLD], int p, int q) {
   return o;
 }
 
-__global__ void __launch_bounds__(kBjThreads) k_bjac_solve(double* __restrict__ A, int np,
+__global__ void __launch_bounds__(kBjSolveThreads) k_bjac_solve(double* __restrict__ A, int np,
                                                            int nbe, int round,
                                                            double* __restrict__ Qbuf) {
   extern __shared__ double bj_sm[];
@@ -80,7 +83,7 @@ __global__ void __launch_bounds__(kBjThreads) k_bjac_solve(double* __restrict__ 
   const int tid = threadIdx.x;
   int I, J;
   rr_pair(round, blockIdx.x, nbe, &I, &J);
-  for (int e = tid; e < JB2 * JB2; e += kBjThreads) {
+  for (int e = tid; e < JB2 * JB2; e += kBjSolveThreads) {
     const int r = e / JB2, c = e % JB2;
     S[r][c] = A[(long)bj_index(I, J, r) * np + bj_index(I, J, c)];
     Q[r][c] = r == c ? 1.0 : 0.0;
@@ -94,7 +97,7 @@ __global__ void __launch_bounds__(kBjThreads) k_bjac_solve(double* __restrict__ 
     }
     __syncthreads();
     // S <- J^T S J on the 2x2 blocks of every two rotations
-    for (int k = tid; k < JB * JB; k += kBjThreads) {
+    for (int k = tid; k < JB * JB; k += kBjSolveThreads) {
       const Rot P = rot[k % JB], R = rot[k / JB];
       const double apr = S[P.p][R.p], aps = S[P.p][R.q];
       const double aqr = S[P.q][R.p], aqs = S[P.q][R.q];
@@ -106,7 +109,7 @@ __global__ void __launch_bounds__(kBjThreads) k_bjac_solve(double* __restrict__ 
       S[P.q][R.q] = R.s * rqr + R.c * rqs;
     }
     // Q <- Q J
-    for (int k = tid; k < JB * JB2; k += kBjThreads) {
+    for (int k = tid; k < JB * JB2; k += kBjSolveThreads) {
       const Rot R = rot[k / JB2];
       const int i = k % JB2;
       const double qp = Q[i][R.p], qq = Q[i][R.q];
@@ -116,7 +119,7 @@ __global__ void __launch_bounds__(kBjThreads) k_bjac_solve(double* __restrict__ 
     __syncthreads();
   }
   double* Qo = Qbuf + (long)blockIdx.x * JB2 * JB2;
-  for (int e = tid; e < JB2 * JB2; e += kBjThreads) {
+  for (int e = tid; e < JB2 * JB2; e += kBjSolveThreads) {
     const int r = e / JB2, c = e % JB2;
     A[(long)bj_index(I, J, r) * np + bj_index(I, J, c)] = S[r][c];
     Qo[e] = Q[r][c];  // row-major Q[r][c]
@@ -434,7 +437,7 @@ int syev_jacobi(int n, double* A, double* w, double* Z, int max_sweeps, cudaStre
     if (e != cudaSuccess) { rc = cuda_status(e, "syev_jacobi"); break; }
     if (h[0] == 0.0 || h[0] <= 1e-30 * h[1]) break;
     for (int r = 0; r < nbe - 1; ++r) {
-      k_bjac_solve<<<npair, kBjThreads, ssm, st>>>(Ap, np, nbe, r, Qb);
+      k_bjac_solve<<<npair, kBjSolveThreads, ssm, st>>>(Ap, np, nbe, r, Qb);
       k_bjac_update<<<nupd, kBjThreads, usm, st>>>(Ap, V, np, nbe, r, Qb);
     }
     e = cudaGetLastError();
