@@ -442,6 +442,45 @@ def run_diag_profile(dtype_name):
                       "bands": NB, "grid": [GRID] * 3}), flush=True)
 
 
+def run_proj_profile(npmesh, sample):
+    """Projector-table generation (rs_projector_tables: Fourier-filtered
+    projectors on the npmesh fine mesh and the double-grid contraction of
+    pseudocalc_07) for the 512 atoms of the Si512 cell: one warm call, then
+    three timed calls on the wall clock (host lists in, host vnlocp out), and
+    the oracle on `sample` atoms scaled to 512.  Prints one JSON line with the
+    largest difference from the oracle over the sampled atoms."""
+    import torch
+    from oracle import oracle as O
+    from rspacedist_b200 import projectors as PR
+    cell = make_cell()
+    PR.projector_tables(cell, npmesh=npmesh)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(3):
+        t = time.perf_counter()
+        v = PR.projector_tables(cell, npmesh=npmesh)
+        ts.append(time.perf_counter() - t)
+    ds = cell.ds
+    coef, nqct, nqmx = PR.bessel_coefs(ds, cell.h)
+    col, ym = PR.channel_table(ds)
+    L = cell.num_list
+    sl = lambda a: np.ascontiguousarray(a[:sample * L])
+    lists = dict(natx=cell.natxyz[0][:sample], naty=cell.natxyz[1][:sample],
+                 natz=cell.natxyz[2][:sample], natinf=cell.natinf[:sample],
+                 lstx=sl(cell.lstxyz[0]), lsty=sl(cell.lstxyz[1]), lstz=sl(cell.lstxyz[2]))
+    t = time.perf_counter()
+    ref = O.projector_tables(cell.atoms[:sample], lists, cell.nmax, cell.h, cell.npmax, 4, npmesh,
+                             L, col, ym, coef, nqct, nqmx, ds["rcut"], PR.PSFTRAD, PR.PSCTOFF,
+                             PR.EPS, PR.NFILTYP, PR.FILPP, O.dg_weights(4, npmesh))
+    tc = (time.perf_counter() - t) * cell.natom / sample
+    err = float(np.abs(v[:sample] - ref).max() / np.abs(ref).max())
+    print(json.dumps({"proj_profile": {"atoms": cell.natom, "projectors": len(col), "npmesh": npmesh,
+                                       "nqct": nqct, "num_list": L},
+                      "gpu_s": [round(x, 4) for x in ts],
+                      "oracle_s_scaled": round(tc, 2), "oracle_sample_atoms": sample,
+                      "oracle_threads": 1, "max_rel_diff": err}), flush=True)
+
+
 def run_gemm_profile(npts):
     """The subspace contractions of the Rayleigh-Ritz step at the Si512 band
     count: Psi^T H Psi (rs_gram_f32, 1100 x 1100 over npts points) and the
@@ -606,11 +645,15 @@ def main():
                     help="time the Hartree CG solve on an N^3 dense grid and exit")
     ap.add_argument("--mixed", action="store_true",
                     help="with --hartree-profile: the mixed-precision solve")
+    ap.add_argument("--proj-profile", type=int, metavar="NPMESH",
+                    help="time the projector-table generation of the Si512 cell and exit")
     ap.add_argument("--batch-profile", type=int, metavar="CELLS",
                     help="time H*psi of CELLS small cells, per-cell calls vs one batched "
                          "launch, and exit")
     args = ap.parse_args()
-    if args.batch_profile:
+    if args.proj_profile:
+        run_proj_profile(args.proj_profile, 4)
+    elif args.batch_profile:
         run_batch_profile(args.batch_profile, 20)
     elif args.hartree_profile:
         run_hartree_profile(args.hartree_profile, args.mixed)

@@ -46,6 +46,31 @@ int rs_sphere_lists(int natom, const double* atx, const double* aty, const doubl
                     int num_list, int* natx, int* naty, int* natz, int* natinf, int* lst,
                     int* lstx, int* lsty, int* lstz);
 
+/* Double-grid weights of pseudocalc_01a (pseudocalc8f.F90:343-629):
+ * w[j + nfdg*npmesh] = wxyz(j), j = -nfdg*npmesh .. nfdg*npmesh-1 (host). */
+int rs_double_grid_weights(int nfdg, int npmesh, double* w);
+
+/* Projector tables of one species on the GPU: replaces pseudocalc_07
+ * (pseudocalc8f.F90:2515-3702).  Inputs are host arrays: atom positions
+ * atx/aty/atz and coarse indices natx/naty/natz, natinf and the list offsets
+ * lstx/lsty/lstz (natom*num_list) from rs_sphere_lists; per projector la the
+ * coefficient column prj_col[la] (1..6: the tmpspd1..6 radial channels s, s',
+ * p, p', d, d') and the real harmonic prj_m[la] (1..9: ylm01..ylm09);
+ * coef(0:nqmx, 0:7) column-major (Fourier-Bessel coefficients of
+ * filterpseudopotentials), nqct of them used; rcut = radial(nradct), psftrad,
+ * psctoff, eps, nfiltyp (1: Fermi filter with width filpp) and wxyz from
+ * rs_double_grid_weights.  Output: vnlocp(num_list, nprj, natom) (host),
+ * zero past natinf.  The fine mesh is npmesh points per coarse spacing. */
+int rs_projector_tables(int natom, int nprj, int num_list, int nxmax, int nymax, int nzmax,
+                        double dx, double dy, double dz, int npxmax, int npymax, int npzmax,
+                        int nfdg, int npmesh, const double* atx, const double* aty,
+                        const double* atz, const int* natx, const int* naty, const int* natz,
+                        const int* natinf, const int* lstx, const int* lsty, const int* lstz,
+                        const int* prj_col, const int* prj_m, int nqct, int nqmx,
+                        const double* coef, double rcut, double psftrad, double psctoff,
+                        double eps, int nfiltyp, double filpp, const double* wxyz,
+                        double* vnlocp, void* stream);
+
 /* Uploads the grid, the sphere lists and vnlocp (host, vnlocp(num_list,
  * nprjmx,natom) layout) and builds the point-major inverse lists used by the
  * fused H*psi.  Stands for the geometry arguments kukan threads through

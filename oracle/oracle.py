@@ -390,3 +390,32 @@ def force_nl(sysk, M, psi, sval, occ):
     lib().orc_force_nl(C.byref(s), M, _d(_f64(psi)), _d(_f64(sval)), _d(_f64(occ)), _d(fx),
                        _d(fy), _d(fz))
     return np.stack([fx, fy, fz], axis=1)
+
+
+def dg_weights(nfdg, npmesh):
+    """wxyz of pseudocalc_01a, index j + nfdg*npmesh."""
+    w = np.zeros(2 * nfdg * npmesh)
+    lib().orc_dg_weights(nfdg, npmesh, _d(w))
+    return w
+
+
+def projector_tables(atoms, lists, nmax, h, npmax, nfdg, npmesh, num_list, prj_col, prj_m,
+                     coef, nqct, nqmx, rcut, psftrad, psctoff, eps, nfiltyp, filpp, wxyz):
+    """vnlocp (natom, nprj, num_list) of pseudocalc_07 for one species; lists
+    is the dict returned by sphere_lists (natx.., natinf, lstx..)."""
+    atoms = _f64(atoms).reshape(-1, 3)
+    A = atoms.shape[0]
+    ax, ay, az = (np.ascontiguousarray(atoms[:, k]) for k in range(3))
+    ii = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    col, ym = ii(prj_col), ii(prj_m)
+    P = len(col)
+    v = np.zeros((A, P, num_list))
+    keep = [ii(lists[k]) for k in ("natx", "naty", "natz", "natinf", "lstx", "lsty", "lstz")]
+    st = lib().orc_projector_tables(
+        A, P, num_list, nmax[0], nmax[1], nmax[2], C.c_double(h[0]), C.c_double(h[1]),
+        C.c_double(h[2]), npmax[0], npmax[1], npmax[2], nfdg, npmesh, _d(ax), _d(ay), _d(az),
+        *[_i(k) for k in keep], _i(col), _i(ym), nqct, nqmx, _d(_f64(coef)), C.c_double(rcut),
+        C.c_double(psftrad), C.c_double(psctoff), C.c_double(eps), nfiltyp, C.c_double(filpp),
+        _d(_f64(wxyz)), _d(v))
+    assert st == 0, "orc_projector_tables: out of memory"
+    return v

@@ -104,6 +104,22 @@ int orc_sphere_lists(int natom, const double* atx, const double* aty, const doub
                      int num_list, int* natx, int* naty, int* natz, int* natinf, int* lst,
                      int* lstx, int* lsty, int* lstz);
 
+/* ---- projector tables (pseudocalc_01a, pseudocalc_07) ---- */
+/* w[j + nfdg*npmesh], j = -nfdg*npmesh .. nfdg*npmesh-1 (wxyz) */
+void orc_dg_weights(int nfdg, int npmesh, double* w);
+/* One species: v[(a*nprj + la)*num_list + ii] (vnlocp), lists lstx/y/z[a*num_list + ii]
+ * as offsets from (natx, naty, natz); projector la uses coefficient column
+ * prj_col[la] (1..6: s, s', p, p', d, d') of coef[c*(nqmx+1) + iq] and the real
+ * harmonic ylm0<prj_m[la]> (1..9).  Returns 1 when out of memory. */
+int orc_projector_tables(int natom, int nprj, int num_list, int nxmax, int nymax, int nzmax,
+                         double dx, double dy, double dz, int npxmax, int npymax, int npzmax,
+                         int nfdg, int npmesh, const double* atx, const double* aty,
+                         const double* atz, const int* natx, const int* naty, const int* natz,
+                         const int* natinf, const int* lstx, const int* lsty, const int* lstz,
+                         const int* prj_col, const int* prj_m, int nqct, int nqmx,
+                         const double* coef, double rcut, double psftrad, double psctoff,
+                         double eps, int nfiltyp, double filpp, const double* wxyz, double* v);
+
 /* ---- eigen / subspace ---- */
 int orc_jacobi_eig(int n, double* a, double* w, double* z);
 void orc_reorder_rank(int m, const double* sval, int* rank);

@@ -95,6 +95,10 @@ SIGNATURES = {
     "rs_dot_f64": [_l, _p, _p, _p, _p],
     "rs_dot_f32": [_l, _p, _p, _p, _p],
     "rs_atomicocc": [_p, _p, _p, _i, _p, _p],
+    "rs_double_grid_weights": [_i, _i, _dp],
+    "rs_projector_tables": [_i, _i, _i, _i, _i, _i, _d, _d, _d, _i, _i, _i, _i, _i, _dp, _dp,
+                            _dp, _ip, _ip, _ip, _ip, _ip, _ip, _ip, _ip, _ip, _i, _i, _dp, _d,
+                            _d, _d, _d, _i, _d, _dp, _dp, _p],
     "rs_hartree_cg_f32": [_i, _i, _i, _i, _d, _d, _d, _d, _i, _i, _i, _p, _p, _ip, _dp, _p],
     "rs_hpsi_batch_create": [C.POINTER(_p), _i, C.POINTER(_p), _ip],
     "rs_hpsi_batch_set_f32": [_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p), C.POINTER(_p),
