@@ -345,18 +345,21 @@ __global__ void k_axpy_b(long n, const T* __restrict__ a, const T* __restrict__ 
   const long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) * V;
   if (i >= n) return;
   const long o = (long)blockIdx.y * n + i;
-  const double d = sign * dp[(long)blockIdx.y * dstride];
+  const T d = (T)(sign * dp[(long)blockIdx.y * dstride]);
   const Pack<T, V> av = ldpk<T, V>(a + o), bv = ldpk<T, V>(b + o);
   Pack<T, V> cv;
 #pragma unroll
-  for (int k = 0; k < V; ++k) cv.v[k] = (T)fma(d, (double)bv.v[k], (double)av.v[k]);
+  for (int k = 0; k < V; ++k) cv.v[k] = fma(d, bv.v[k], av.v[k]);
   stpk<T, V>(c + o, cv);
 }
 
 // ---- fused DIIS passes.  Each forms the trial vectors of ksdiis_r on the
-// fly, rounded to T exactly as the stored vectors were, and accumulates every
-// dot product it needs in the fixed tree order, so each band sees the same
-// values as with the vectors stored.  part layout: [dot][band][chunk].
+// fly, with the same T-precision formula in every pass (the step, eigenvalue
+// and combination coefficients rounded to T once; for T = double the Fortran
+// statement's FMA), and accumulates every dot product it needs in FP64 in the
+// fixed tree order, so each band sees the same values as with the vectors
+// stored.  The FP32 path so forms its vectors in FP32 arithmetic, which keeps
+// the passes clear of FP32<->FP64 conversions.  part layout: [dot][band][chunk].
 //
 // Trial-step sums (ksdiis8f.F90:285-300) with a1 = alambda_diis:
 //   rvre.hs, rvre.ss, ph1.hph1, ph1.sph1 with ph1 = ps + a1 rvre,
@@ -370,7 +373,7 @@ __global__ void k_diis_dots_a(long n, const T* __restrict__ ps, const T* __restr
   __shared__ double ws[8];
   const int j = blockIdx.y, nb = gridDim.y;
   const long off = (long)j * n;
-  const double a1 = *a1p;
+  const T a1 = (T)*a1p;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
 #pragma unroll 4
@@ -378,11 +381,12 @@ __global__ void k_diis_dots_a(long n, const T* __restrict__ ps, const T* __restr
     const long i = base + (long)k * kTreeLanes;
     if (i < n) {
       const long o = off + i;
-      const double r = (double)rvre[o], h = (double)hs[o], p = (double)ps[o];
-      const double s = SP ? (double)ss[o] : p;
-      const T p1 = (T)fma(a1, r, p);
-      const T h1 = (T)fma(a1, (double)avre[o], h);
-      const T s1 = SP ? (T)fma(a1, (double)asvre[o], s) : p1;
+      const T rt = rvre[o], ht = hs[o], pt = ps[o];
+      const T st = SP ? ss[o] : pt;
+      const T p1 = fma(a1, rt, pt);
+      const T h1 = fma(a1, avre[o], ht);
+      const T s1 = SP ? fma(a1, asvre[o], st) : p1;
+      const double r = (double)rt, h = (double)ht, s = (double)st;
       acc[0] = fma(r, h, acc[0]);
       acc[1] = fma(r, s, acc[1]);
       acc[2] = fma((double)p1, (double)h1, acc[2]);
@@ -410,7 +414,7 @@ __global__ void k_diis_dots_b(long n, const T* __restrict__ ps, const T* __restr
   __shared__ double ws[8];
   const int j = blockIdx.y, nb = gridDim.y;
   const long off = (long)j * n;
-  const double lam = sc[j].lam, ev = -1.0 * sval[j];
+  const T lam = (T)sc[j].lam, ev = (T)(-1.0 * sval[j]);
   double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
 #pragma unroll 4
@@ -418,14 +422,15 @@ __global__ void k_diis_dots_b(long n, const T* __restrict__ ps, const T* __restr
     const long i = base + (long)k * kTreeLanes;
     if (i < n) {
       const long o = off + i;
-      const double p = (double)ps[o];
-      const double s = SP ? (double)ss[o] : p;
-      const double h = (double)hs[o];
-      const double v0 = (double)(T)fma(ev, s, h);
-      const T p1 = (T)fma(lam, (double)rvre[o], p);
-      const T h1 = (T)fma(lam, (double)avre[o], h);
-      const T s1 = SP ? (T)fma(lam, (double)asvre[o], s) : p1;
-      const double v1 = (double)(T)fma(ev, (double)s1, (double)h1);
+      const T pt = ps[o];
+      const T st = SP ? ss[o] : pt;
+      const T ht = hs[o];
+      const double p = (double)pt, s = (double)st;
+      const double v0 = (double)fma(ev, st, ht);
+      const T p1 = fma(lam, rvre[o], pt);
+      const T h1 = fma(lam, avre[o], ht);
+      const T s1 = SP ? fma(lam, asvre[o], st) : p1;
+      const double v1 = (double)fma(ev, s1, h1);
       acc[0] = fma(p, s, acc[0]);
       acc[1] = fma(v0, v0, acc[1]);
       acc[2] = fma(p, (double)s1, acc[2]);
@@ -465,12 +470,13 @@ template <class T, bool SP, int V>
 __device__ __forceinline__ void diis_comb_vec(long o, T* y, const T* __restrict__ dy, double lam,
                                               double t, double c0, double c1) {
   const Pack<T, V> yv = ldpk<T, V>(y + o), dv = ldpk<T, V>(dy + o);
+  const T lt = (T)lam, tt = (T)t, c0t = (T)c0, c1t = (T)c1;
   Pack<T, V> nv;
 #pragma unroll
   for (int k = 0; k < V; ++k) {
-    const double a = (double)yv.v[k];
-    const T a1 = (T)((double)(T)fma(lam, (double)dv.v[k], a) * t);
-    nv.v[k] = (T)fma(c1, (double)a1, c0 * a);
+    const T a = yv.v[k];
+    const T a1 = fma(lt, dv.v[k], a) * tt;
+    nv.v[k] = fma(c1t, a1, c0t * a);
   }
   stpk<T, V>(y + o, nv);
 }

@@ -58,15 +58,22 @@ __device__ __forceinline__ int bj_index(int I, int J, int k) {
   return k < JB ? I * JB + k : J * JB + (k - JB);
 }
 
-// rotation (c, s) zeroing S[p][q] (same formula as the scalar sweep)
+// rotation (c, s) zeroing S[p][q]: the smaller root t of t^2 + 2 theta t - 1 = 0,
+// theta = (aqq - app) / (2 apq), written as t = sign(theta) 2|apq| / (|d| +
+// sqrt(d^2 + 4 apq^2)) with d = aqq - app, and c = 1/sqrt(1 + t^2).  The
+// sign convention is the scalar sweep's (theta = +-0 counts as positive); one
+// division, one square root and one reciprocal square root per rotation,
+// since these dependent long-latency steps set the pace of the 63 rounds.
 __device__ __forceinline__ Rot bj_params(const double (*S)[JLD], int p, int q) {
   Rot o{p, q, 1.0, 0.0};
   const double apq = S[p][q];
   if (apq != 0.0) {
     const double app = S[p][p], aqq = S[q][q];
-    const double theta = (aqq - app) / (2.0 * apq);
-    const double tt = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-    const double c = 1.0 / sqrt(tt * tt + 1.0);
+    const double d = aqq - app;
+    const double a2 = 2.0 * fabs(apq);
+    const double sgn = (d == 0.0 || (d > 0.0) == (apq > 0.0)) ? 1.0 : -1.0;
+    const double tt = sgn * a2 / (fabs(d) + sqrt(d * d + a2 * a2));
+    const double c = rsqrt(tt * tt + 1.0);
     o.c = c;
     o.s = tt * c;
   }
