@@ -385,13 +385,26 @@ __global__ void k_gram_reduce(const double* __restrict__ part, int nsplit, int m
 }
 
 // ------------------------------------------------------------------ rotation
-// Y[j][p] = sum_k X[k][p] Z(k, j), output tiles of 128 points x 128 bands.
-// X and Z arrive pre-split and pre-tiled (k_tile_x, k_tile_z), so a stage is
-// two 32 KB bulk copies: X hi | lo (MN-major) and Z hi | lo (K-major).  Each
-// CTA walks tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (band tile
-// fastest, so the CTAs that share an X block run together and read it from
-// HBM once); the producer and the MMA warp run ahead into the next tile
-// while the drain warps finish the last one.  Drained sums add up in FP32.
+// Y[j][p] = sum_k X[k][p] Z(k, j).  The contraction is bound by operand
+// delivery from L2 (about 9.5 TB/s into all SMs at 48 flop per byte), so a
+// CTA computes two 128 x 128 output tiles at once: one 128-point block of X
+// against two 128-band blocks of Z.  A stage is three 32 KB bulk copies,
+// X hi | lo (MN-major) and the two Z hi | lo (K-major), fed to 6 MMAs per
+// K step, 64 flop per byte.  Each CTA walks tile pairs t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... (band pair fastest, so the CTAs sharing an X
+// block run together and read it from HBM once); an odd last band tile
+// runs alone.  Two TMEM buffers, each two accumulators of 128 columns: the
+// MMA warp fills one while the drain warps fold the other into FP32
+// registers (DGRP stages per accumulator, as in the Gram), so the producer
+// and the MMA warp run ahead into the next pair while the last one drains.
+constexpr int RSTAGES = 2;
+constexpr int RSTAGE_BYTES = 6 * OPB;
+constexpr size_t ROT_SMEM = (size_t)RSTAGES * RSTAGE_BYTES + 1024;
+
+struct RotBars {
+  uint64_t full[RSTAGES], empty[RSTAGES], tfull[2], tempty[2];
+};
+
 __device__ __forceinline__ void drain_f32(uint32_t taddr, float* acc) {
 #pragma unroll
   for (int c = 0; c < 64; c += 16) {
@@ -405,20 +418,27 @@ __device__ __forceinline__ void drain_f32(uint32_t taddr, float* acc) {
 
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_rotate_tf32x3(const char* __restrict__ xt, const char* __restrict__ zt, long npts, int nkb,
-                    int nout, long ntiles, float* __restrict__ Y, long ldy) {
+                    int nout, int ntn, long ntiles, float* __restrict__ Y, long ldy) {
   extern __shared__ __align__(1024) char smem_dyn[];
   char* smem = (char*)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) PipeBars bar;
+  __shared__ __align__(8) RotBars bar;
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int ntn = (nout + GN - 1) / GN;
+  const int npr = (ntn + 1) / 2;  // band-tile pairs
   const int ngrp = (nkb + DGRP - 1) / DGRP;
   const long mytiles = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
-  if (warp == 2) tmem_alloc(&tmem_base, TM_BUFS * GN);
+  if (warp == 2) tmem_alloc(&tmem_base, 4 * GN);
   if (tid == 0) {
-    pipe_init(bar, NDRAIN);
+    for (int q = 0; q < RSTAGES; ++q) {
+      mbar_init(&bar.full[q], 1);
+      mbar_init(&bar.empty[q], 1);
+    }
+    for (int q = 0; q < 2; ++q) {
+      mbar_init(&bar.tfull[q], 1);
+      mbar_init(&bar.tempty[q], NDRAIN);
+    }
     abort_flag = 0;
     fence_mbar_init();
   }
@@ -437,21 +457,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       for (; c < nstage && !bad; ++c) {
         const long t = blockIdx.x + (c / nkb) * gridDim.x;
         const int kb = (int)(c % nkb);
-        const long pt = t / ntn;
-        const int jt = (int)(t % ntn);
-        const int s = (int)(c % STAGES);
-        if (c >= STAGES &&
-            !mbar_wait_or_abort(&bar.empty[s], (int)(c / STAGES - 1) & 1, &abort_flag)) {
+        const long pt = t / npr;
+        const int j1 = 2 * (int)(t % npr);
+        const bool two = j1 + 1 < ntn;
+        const int s = (int)(c % RSTAGES);
+        if (c >= RSTAGES &&
+            !mbar_wait_or_abort(&bar.empty[s], (int)(c / RSTAGES - 1) & 1, &abort_flag)) {
           bad = true;
           break;
         }
-        char* st = smem + s * STAGE_BYTES;
-        mbar_arrive_expect_tx(&bar.full[s], 4 * OPB);
+        char* st = smem + s * RSTAGE_BYTES;
+        mbar_arrive_expect_tx(&bar.full[s], (two ? 6 : 4) * OPB);
         bulk_load(st, xt + (pt * nkb + kb) * (2L * OPB), 2 * OPB, &bar.full[s]);
-        bulk_load(st + 2 * OPB, zt + ((long)jt * nkb + kb) * (2L * OPB), 2 * OPB, &bar.full[s]);
+        bulk_load(st + 2 * OPB, zt + ((long)j1 * nkb + kb) * (2L * OPB), 2 * OPB, &bar.full[s]);
+        if (two)
+          bulk_load(st + 4 * OPB, zt + ((long)(j1 + 1) * nkb + kb) * (2L * OPB), 2 * OPB,
+                    &bar.full[s]);
       }
-      for (long j = max(0L, c - STAGES); j < c; ++j)
-        if (!mbar_wait(&bar.full[j % STAGES], (int)(j / STAGES) & 1)) bad = true;
+      for (long j = max(0L, c - RSTAGES); j < c; ++j)
+        if (!mbar_wait(&bar.full[j % RSTAGES], (int)(j / RSTAGES) & 1)) bad = true;
       if (bad) abort_flag = 1;
     }
   } else if (warp == 1) {
@@ -460,26 +484,32 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       constexpr uint32_t idesc = idesc_tf32(GM, GN, 1, 0);
       long c = 0;
       for (; c < nstage; ++c) {
+        const long t = blockIdx.x + (c / nkb) * gridDim.x;
+        const bool two = 2 * (int)(t % npr) + 1 < ntn;
         const int kb = (int)(c % nkb);
-        const long G = (c / nkb) * ngrp + kb / DGRP;  // accumulator group, over all tiles
-        const int tb = (int)(G % TM_BUFS), s = (int)(c % STAGES);
-        if (kb % DGRP == 0 && G >= TM_BUFS &&
-            !mbar_wait_or_abort(&bar.tempty[tb], (int)(G / TM_BUFS - 1) & 1, &abort_flag)) {
+        const long G = (c / nkb) * ngrp + kb / DGRP;  // accumulator group, over all pairs
+        const int tb = (int)(G & 1), s = (int)(c % RSTAGES);
+        if (kb % DGRP == 0 && G >= 2 &&
+            !mbar_wait_or_abort(&bar.tempty[tb], (int)(G / 2 - 1) & 1, &abort_flag)) {
           bad = true;
           break;
         }
-        if (!mbar_wait_or_abort(&bar.full[s], (int)(c / STAGES) & 1, &abort_flag)) {
+        if (!mbar_wait_or_abort(&bar.full[s], (int)(c / RSTAGES) & 1, &abort_flag)) {
           bad = true;
           break;
         }
         tc_fence_after();
-        const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
-        issue_stage<true>(tmem + tb * GN, sa, sa + OPB, sa + 2 * OPB, sa + 3 * OPB, idesc,
-                          kb % DGRP == 0);
+        const uint32_t sa = smem_u32(smem + s * RSTAGE_BYTES);
+        const bool first = kb % DGRP == 0;
+        issue_stage<true>(tmem + (2 * tb) * GN, sa, sa + OPB, sa + 2 * OPB, sa + 3 * OPB, idesc,
+                          first);
+        if (two)
+          issue_stage<true>(tmem + (2 * tb + 1) * GN, sa, sa + OPB, sa + 4 * OPB, sa + 5 * OPB,
+                            idesc, first);
         mma_commit(&bar.empty[s]);
         if (kb % DGRP == DGRP - 1 || kb == nkb - 1) mma_commit(&bar.tfull[tb]);
       }
-      if (c > 0 && !mbar_wait(&bar.empty[(c - 1) % STAGES], (int)((c - 1) / STAGES) & 1))
+      if (c > 0 && !mbar_wait(&bar.empty[(c - 1) % RSTAGES], (int)((c - 1) / RSTAGES) & 1))
         bad = true;
       if (bad) abort_flag = 1;
     }
@@ -490,24 +520,32 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     long G = 0;
     for (long i = 0; i < mytiles && !bad; ++i) {
       const long t = blockIdx.x + i * gridDim.x;
-      const long p = (t / ntn) * GM + dq * 32 + (tid & 31);
-      const int j0 = (int)(t % ntn) * GN + dh * 64;
-      float acc[64];
+      const long p = (t / npr) * GM + dq * 32 + (tid & 31);
+      const int j1 = 2 * (int)(t % npr);
+      const bool two = j1 + 1 < ntn;
+      float acc1[64], acc2[64];
 #pragma unroll
-      for (int k = 0; k < 64; ++k) acc[k] = 0.f;
+      for (int k = 0; k < 64; ++k) acc1[k] = acc2[k] = 0.f;
       for (int g = 0; g < ngrp; ++g, ++G) {
-        const int tb = (int)(G % TM_BUFS);
-        const bool ok = mbar_wait_or_abort(&bar.tfull[tb], (int)(G / TM_BUFS) & 1, &abort_flag);
+        const int tb = (int)(G & 1);
+        const bool ok = mbar_wait_or_abort(&bar.tfull[tb], (int)(G / 2) & 1, &abort_flag);
         if (__any_sync(0xffffffffu, !ok)) { bad = true; break; }
         tc_fence_after();
-        drain_f32(tmem + tb * GN + dh * 64 + dlane, acc);
+        drain_f32(tmem + (2 * tb) * GN + dh * 64 + dlane, acc1);
+        if (two) drain_f32(tmem + (2 * tb + 1) * GN + dh * 64 + dlane, acc2);
         tc_fence_before();
         mbar_arrive(&bar.tempty[tb]);
       }
       if (!bad && p < npts) {
+        const int b1 = j1 * GN + dh * 64, b2 = b1 + GN;
 #pragma unroll
         for (int k = 0; k < 64; ++k)
-          if (j0 + k < nout) Y[(long)(j0 + k) * ldy + p] = acc[k];
+          if (b1 + k < nout) Y[(long)(b1 + k) * ldy + p] = acc1[k];
+        if (two) {
+#pragma unroll
+          for (int k = 0; k < 64; ++k)
+            if (b2 + k < nout) Y[(long)(b2 + k) * ldy + p] = acc2[k];
+        }
       }
     }
   }
@@ -516,7 +554,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   if (bad || abort_flag) {
     if (tid == 64) atomicExch(&g_tc_error, 1);
   }
-  if (warp == 2) tmem_dealloc(tmem, TM_BUFS * GN);
+  if (warp == 2) tmem_dealloc(tmem, 4 * GN);
 }
 
 
@@ -621,15 +659,15 @@ int rotate_f32(long npts, int kin, int nout, const float* X, long ldx, const dou
   k_tile_x<<<(unsigned)(npt * nkb), 256, 0, st>>>(X, ldx, npts, kin, nkb, xt);
   k_tile_z<<<(unsigned)(ntn * nkb), 256, 0, st>>>(Z, ldz, kin, nout, nkb, zt);
   cudaError_t e = cudaFuncSetAttribute(k_rotate_tf32x3,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROT_SMEM);
   if (e == cudaSuccess) {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const long ntiles = npt * ntn;
+    const long ntiles = npt * ((ntn + 1) / 2);  // (point tile, band-tile pair)
     const long nblk = min(ntiles, (long)nsm);
-    k_rotate_tf32x3<<<(unsigned)nblk, TC_THREADS, TC_SMEM, st>>>(xt, zt, npts, nkb, nout, ntiles,
-                                                                 Y, ldy);
+    k_rotate_tf32x3<<<(unsigned)nblk, TC_THREADS, ROT_SMEM, st>>>(xt, zt, npts, nkb, nout, ntn,
+                                                                  ntiles, Y, ldy);
     e = cudaGetLastError();
   }
   cudaFreeAsync(xt, st);

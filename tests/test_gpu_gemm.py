@@ -36,7 +36,8 @@ def test_gram_f32_tensor_cores(built_lib, cuda, m, n, K, sym):
 
 
 @pytest.mark.parametrize("npts,kin,nout", [(4096, 20, 20), (65536, 160, 160),
-                                           (12288, 300, 270)])
+                                           (12288, 300, 270), (8192, 70, 513),
+                                           (4100, 33, 129)])
 def test_rotate_f32_tensor_cores(built_lib, cuda, npts, kin, nout):
     from rspacedist_b200 import lib
     rng = np.random.default_rng(npts + kin)
