@@ -319,6 +319,61 @@ __global__ void __launch_bounds__(128) k_nl_rmw_f32(
     if (b < nbb) out[(long)(b0 + b) * N + p] = h[b];
 }
 
+// S psi = psi + sum_e t[atom_e][b] . p_e in one pass over the grid: a thread
+// owns 4 consecutive points (one 16-byte vector per band) and SP_BANDS bands,
+// reads psi once, adds the projector sums of the points that lie inside a
+// support (the entries of the inverse list, in its order, each sum an FMA
+// chain over the projectors as in k_nl_rmw_f32) and writes S psi once.  psi
+// == out is allowed: a thread reads its values before writing them.
+constexpr int SP_BANDS = 8;
+__global__ void __launch_bounds__(128) k_spsi_f32_fused(
+    long N, int nb, const float* psi, float* out, const int* __restrict__ inv_off,
+    const int* __restrict__ inv_atom, const float* __restrict__ inv_v,
+    const float* __restrict__ tco, int P) {
+  const long p0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (p0 >= N) return;
+  const int b0 = blockIdx.y * SP_BANDS;
+  const int nbb = min(SP_BANDS, nb - b0);
+  float4 h[SP_BANDS];
+#pragma unroll
+  for (int b = 0; b < SP_BANDS; ++b)
+    h[b] = b < nbb ? ld4(psi + (long)(b0 + b) * N + p0) : zero4();
+  const int4 o4 = __ldg(reinterpret_cast<const int4*>(inv_off + p0));
+  const int o[5] = {o4.x, o4.y, o4.z, o4.w, __ldg(inv_off + p0 + 4)};
+  const int nq = P / 4;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    for (int e = o[k]; e < o[k + 1]; ++e) {
+      const int at = __ldg(inv_atom + e);
+      float4 v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v[q] = q < nq ? ld4(inv_v + (long)e * P + 4 * q) : zero4();
+      const float* tb = tco + ((long)at * nb + b0) * P;
+#pragma unroll
+      for (int b = 0; b < SP_BANDS; ++b) {
+        if (b < nbb) {
+          float sum = 0.f;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            if (q < nq) {
+              const float4 t = ld4(tb + (long)b * P + 4 * q);
+              sum = fmaf(t.x, v[q].x, sum);
+              sum = fmaf(t.y, v[q].y, sum);
+              sum = fmaf(t.z, v[q].z, sum);
+              sum = fmaf(t.w, v[q].w, sum);
+            }
+          }
+          float* hk = k == 0 ? &h[b].x : (k == 1 ? &h[b].y : (k == 2 ? &h[b].z : &h[b].w));
+          *hk += sum;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < SP_BANDS; ++b)
+    if (b < nbb) *reinterpret_cast<float4*>(out + (long)(b0 + b) * N + p0) = h[b];
+}
+
 }  // namespace
 
 int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
@@ -416,10 +471,20 @@ int launch_spsi_f32_fast(const rs_geom* g, const double* sss, const double* rp, 
   RS_CUDA(cudaMallocAsync((void**)&t, nt * sizeof(float), st));
   k_tcoef_f32<<<div_up(nt, 256), 256, 0, st>>>(g->natom, g->nprjmx, g->d_nprj, sss, rp,
                                                1.0 / (g->dx * g->dy * g->dz), nb, t);
-  // out = psi, then the nonlocal sums added on the points inside a projector
-  // support only: the same entries, sums and order as the per-band gather,
-  // and the other points keep psi unchanged
   cudaError_t e = cudaSuccess;
+  const bool vec = g->N % 4 == 0 && ((uintptr_t)psi | (uintptr_t)out) % 16 == 0 &&
+                   nb <= 65535 * SP_BANDS;
+  if (vec) {
+    dim3 grid(div_up(g->N / 4, 128), div_up(nb, SP_BANDS));
+    k_spsi_f32_fused<<<grid, 128, 0, st>>>(g->N, nb, psi, out, g->d_inv_off, g->d_inv_atom,
+                                            g->d_inv_v32, t, g->nprjmx);
+    e = cudaGetLastError();
+    cudaFreeAsync(t, st);
+    if (e != cudaSuccess) return cuda_status(e, "k_spsi_f32_fused");
+    return RS_OK;
+  }
+  // otherwise out = psi, then the nonlocal sums added on the points inside a
+  // projector support only (the same entries, sums and order)
   if (out != psi)
     e = cudaMemcpyAsync(out, psi, sizeof(float) * g->N * nb, cudaMemcpyDeviceToDevice, st);
   if (e == cudaSuccess && g->n_cov > 0) {

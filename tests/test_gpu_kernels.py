@@ -108,6 +108,26 @@ def test_hpsi_f32(setup, oracle, nb):
     np.testing.assert_allclose(sout.cpu().numpy(), sref, atol=F32_RTOL * np.abs(sref).max())
 
 
+@pytest.mark.parametrize("nb", [1, 8, 13])
+def test_spsi_f32_one_pass_matches_two_pass(setup, nb):
+    """The one-pass FP32 S psi (16-byte vectors) and the copy + covered-point
+    pass used for unaligned bands give the same bits, also in place."""
+    from rspacedist_b200 import kukan as K, system as S
+    cell, g, veff, _ = setup
+    psi = torch.tensor(S.random_bands(cell, nb, 7), dtype=torch.float32, device="cuda")
+    rp = K.nonlocaloperation_01(g, psi)
+    sss = T(cell.sss)
+    fused = K.spsi(g, sss, rp, psi)
+    big = torch.zeros(nb * cell.N + 1, dtype=torch.float32, device="cuda")
+    shifted = big[1:].view(nb, cell.N)  # 4 bytes off a 16-byte boundary
+    shifted.copy_(psi)
+    two_pass = K.spsi(g, sss, rp, shifted)
+    assert torch.equal(fused, two_pass)
+    inplace = psi.clone()
+    K.spsi(g, sss, rp, inplace, out=inplace)
+    assert torch.equal(fused, inplace)
+
+
 def test_hpsi_host_matches_device(setup):
     from rspacedist_b200 import kukan as K, system as S
     cell, g, veff, _ = setup
