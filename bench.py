@@ -460,6 +460,20 @@ def run_proj_profile(npmesh, sample):
         t = time.perf_counter()
         v = PR.projector_tables(cell, npmesh=npmesh)
         ts.append(time.perf_counter() - t)
+    # the same tables left in device memory, timed with CUDA events on the
+    # launching stream (list upload and kernels; no copy back)
+    vd = torch.empty(v.shape, dtype=torch.float64, device="cuda")
+    PR.projector_tables(cell, npmesh=npmesh, out=vd)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tds = []
+    for _ in range(3):
+        e0.record()
+        PR.projector_tables(cell, npmesh=npmesh, out=vd)
+        e1.record()
+        torch.cuda.synchronize()
+        tds.append(e0.elapsed_time(e1) / 1e3)
+    assert np.array_equal(vd.cpu().numpy(), v)
     ds = cell.ds
     coef, nqct, nqmx = PR.bessel_coefs(ds, cell.h)
     col, ym = PR.channel_table(ds)
@@ -477,6 +491,7 @@ def run_proj_profile(npmesh, sample):
     print(json.dumps({"proj_profile": {"atoms": cell.natom, "projectors": len(col), "npmesh": npmesh,
                                        "nqct": nqct, "num_list": L},
                       "gpu_s": [round(x, 4) for x in ts],
+                      "gpu_device_out_s": [round(x, 4) for x in tds],
                       "oracle_s_scaled": round(tc, 2), "oracle_sample_atoms": sample,
                       "oracle_threads": 1, "max_rel_diff": err}), flush=True)
 

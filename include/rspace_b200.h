@@ -59,8 +59,10 @@ int rs_double_grid_weights(int nfdg, int npmesh, double* w);
  * coef(0:nqmx, 0:7) column-major (Fourier-Bessel coefficients of
  * filterpseudopotentials), nqct of them used; rcut = radial(nradct), psftrad,
  * psctoff, eps, nfiltyp (1: Fermi filter with width filpp) and wxyz from
- * rs_double_grid_weights.  Output: vnlocp(num_list, nprj, natom) (host),
- * zero past natinf.  The fine mesh is npmesh points per coarse spacing. */
+ * rs_double_grid_weights.  Output: vnlocp(num_list, nprj, natom), zero past
+ * natinf, in host memory (returns when it is written) or device memory
+ * (written in stream order).  The fine mesh is npmesh points per coarse
+ * spacing. */
 int rs_projector_tables(int natom, int nprj, int num_list, int nxmax, int nymax, int nzmax,
                         double dx, double dy, double dz, int npxmax, int npymax, int npzmax,
                         int nfdg, int npmesh, const double* atx, const double* aty,

@@ -298,7 +298,13 @@ extern "C" int rs_projector_tables(
   const size_t bytes_atoms = sizeof(double) * 3 * natom + sizeof(int) * 4 * natom;
   const size_t bytes_lists = sizeof(int) * 3 * (size_t)natom * num_list;
   const size_t bytes_c = sizeof(double) * (size_t)(nqmx + 1) * 8 + sizeof(double) * nw;
-  const size_t bytes_v = sizeof(double) * (size_t)natom * nprj * num_list;
+  // vnlocp in device memory is written in place, in stream order; host
+  // memory gets a copy at the end
+  cudaPointerAttributes pa;
+  const bool dev_out = cudaPointerGetAttributes(&pa, vnlocp) == cudaSuccess &&
+                       (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
+  cudaGetLastError();
+  const size_t bytes_v = dev_out ? 0 : sizeof(double) * (size_t)natom * nprj * num_list;
   const size_t bytes_w = sizeof(double) * (size_t)B * per_atom;
   char* buf = nullptr;
   const size_t total = bytes_atoms + bytes_lists + bytes_c + bytes_v + bytes_w + 5 * 256;
@@ -314,7 +320,7 @@ extern "C" int rs_projector_tables(
   int* d_lst = (int*)take(bytes_lists);
   double* d_coef = (double*)take(bytes_c);
   double* d_w = d_coef + (size_t)(nqmx + 1) * 8;
-  double* d_v = (double*)take(bytes_v);
+  double* d_v = dev_out ? vnlocp : (double*)take(bytes_v);
   double* d_work = (double*)take(bytes_w);
   int rc = RS_OK;
   cudaError_t e = cudaSuccess;
@@ -367,8 +373,9 @@ extern "C" int rs_projector_tables(
     e = cudaGetLastError();
     if (e != cudaSuccess) rc = cuda_status(e, "rs_projector_tables: kernels");
   }
-  if (rc == RS_OK) {
-    e = cudaMemcpyAsync(vnlocp, d_v, bytes_v, cudaMemcpyDeviceToHost, st);
+  if (rc == RS_OK && !dev_out) {
+    e = cudaMemcpyAsync(vnlocp, d_v, sizeof(double) * (size_t)natom * nprj * num_list,
+                        cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = cuda_status(e, "rs_projector_tables: download");
   }

@@ -83,8 +83,10 @@ def double_grid_weights(nfdg: int, npmesh: int) -> np.ndarray:
 
 def projector_tables(cell: Cell, npmesh: int = NPMESH, nfdg: int = 4, psftrad: float = PSFTRAD,
                      psctoff: float = PSCTOFF, nfiltyp: int = NFILTYP, filpp: float = FILPP,
-                     eps: float = EPS, stream=None) -> np.ndarray:
-    """vnlocp of the cell, shape (natom, nprj, num_list), from the GPU."""
+                     eps: float = EPS, stream=None, out=None):
+    """vnlocp of the cell, shape (natom, nprj, num_list), from the GPU: a
+    numpy array, or ``out`` (a contiguous FP64 CUDA tensor of that shape,
+    written in stream order) when given."""
     ds = cell.ds
     coef, nqct, nqmx = bessel_coefs(ds, cell.h, psftrad)
     col, ym = channel_table(ds)
@@ -95,12 +97,13 @@ def projector_tables(cell: Cell, npmesh: int = NPMESH, nfdg: int = 4, psftrad: f
     lx, ly, lz = (np.ascontiguousarray(a, dtype=np.int32) for a in cell.lstxyz)
     nat = [np.ascontiguousarray(a, dtype=np.int32) for a in cell.natxyz]
     natinf = np.ascontiguousarray(cell.natinf, dtype=np.int32)
-    v = np.zeros((A, P, L))
+    v = np.zeros((A, P, L)) if out is None else out
     dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    vp = dp(v) if out is None else C.cast(C.c_void_p(out.data_ptr()), C.POINTER(C.c_double))
     ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
     _lib.call("rs_projector_tables", A, P, L, cell.nmax[0], cell.nmax[1], cell.nmax[2],
               cell.h[0], cell.h[1], cell.h[2], cell.npmax[0], cell.npmax[1], cell.npmax[2], nfdg,
               npmesh, dp(ax), dp(ay), dp(az), ip(nat[0]), ip(nat[1]), ip(nat[2]), ip(natinf),
               ip(lx), ip(ly), ip(lz), ip(col), ip(ym), nqct, nqmx, dp(coef), ds["rcut"], psftrad,
-              psctoff, eps, nfiltyp, filpp, dp(w), dp(v), stream)
+              psctoff, eps, nfiltyp, filpp, dp(w), vp, stream)
     return v

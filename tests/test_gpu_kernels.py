@@ -151,6 +151,34 @@ def test_precondition(setup, oracle):
     np.testing.assert_allclose(o32, ref, atol=1e-6 * np.abs(ref).max())
 
 
+def _grid_only_geometry(shape, h=0.3):
+    """A geometry without atoms, for the grid kernels on arbitrary shapes."""
+    import types
+    from rspacedist_b200 import kukan as K
+    N = int(np.prod(shape))
+    e = types.SimpleNamespace(shape=tuple(shape), h=(h, h, h), natom=0, nprjmx=4, num_list=1,
+                              nprj=np.zeros(1, np.int32), natinf=np.zeros(1, np.int32),
+                              lst=np.zeros(1, np.int32), vnlocp=np.zeros(1), N=N)
+    return K.Geometry(e)
+
+
+@pytest.mark.parametrize("shape", [(12, 10, 10), (20, 9, 11), (18, 10, 9), (16, 16, 40),
+                                   (10, 12, 64)])
+def test_precondition_shapes(cuda, oracle, shape):
+    """The plane-marching preconditioner (rows in 16-byte vectors, partial y
+    tiles and z runs) and the row-wise form it falls back to give the
+    oracle's bits in FP64 on grids of every parity."""
+    from rspacedist_b200 import kukan as K
+    g = _grid_only_geometry(shape)
+    nx, ny, nz = shape
+    psi = np.random.default_rng(nx * ny + nz).standard_normal((3, nx * ny * nz))
+    ref = oracle.precondition(shape, psi)
+    out = K.ksprecondition(g, T(psi))
+    assert np.array_equal(out.cpu().numpy(), ref)
+    o32 = K.ksprecondition(g, T(psi, torch.float32)).cpu().numpy()
+    np.testing.assert_allclose(o32, ref, atol=1e-6 * np.abs(ref).max())
+
+
 def test_density(setup, oracle):
     from rspacedist_b200 import kukan as K
     cell, g, veff, psi = setup
@@ -254,6 +282,30 @@ def test_atomicocc_bit_exact(oracle, cuda, built_lib, si8):
     assert np.array_equal(got, ref)
     diag = [j * (j + 1) // 2 + j for j in range(si8.nprjmx)]
     np.testing.assert_allclose(ref[:, diag], np.einsum("l,lai->ai", f, rp ** 2), rtol=1e-13)
+
+
+@pytest.mark.parametrize("shape", [(40, 48, 56), (42, 44, 40)])
+def test_hartree_mixed_anisotropic(cuda, built_lib, shape):
+    """Mixed Hartree CG on box grids: (40, 48, 56) takes the 4 x 2-point A p
+    z-march with a partial z run, (42, 44, 40) the paired Hartree z-march."""
+    from rspacedist_b200 import kukan as K
+    nx, ny, nz = shape
+    hh = 0.22
+    axes = [(np.arange(n) + 0.5) * hh - n * hh / 2 for n in (nx, ny, nz)]
+    rho = np.zeros((nz, ny, nx))
+    rng = np.random.default_rng(nx)
+    for c in rng.uniform(-1.5, 1.5, (3, 3)):
+        d = [axes[k] - c[k] for k in range(3)]
+        r2 = d[2][:, None, None] ** 2 + d[1][None, :, None] ** 2 + d[0][None, None, :] ** 2
+        rho += np.exp(-r2 / 1.5)
+    rho -= rho.mean()
+    xm = tuple(n * hh / 2 for n in (nx, ny, nz))
+    v64 = torch.zeros(rho.size, dtype=torch.float64, device="cuda")
+    v32 = torch.zeros_like(v64)
+    K.scf_hartree(shape, 4, xm, T(rho.ravel()), v64, 1e-12)
+    it, dp = K.scf_hartree(shape, 4, xm, T(rho.ravel()), v32, 1e-12, mixed=True)
+    err = float((v32 - v64).abs().max() / v64.abs().max())
+    assert err < 2e-6, (err, it, dp)
 
 
 def test_hartree_mixed_matches_fp64(cuda, built_lib):

@@ -135,3 +135,8 @@ def test_projector_tables_gpu_match_oracle(oracle, cuda, which, npmesh):
     got = PR.projector_tables(cell, npmesh=npmesh)
     np.testing.assert_allclose(got, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
     assert np.abs(ref).max() > 0
+    import torch
+    dev = torch.full(got.shape, np.nan, dtype=torch.float64, device="cuda")
+    PR.projector_tables(cell, npmesh=npmesh, out=dev)
+    torch.cuda.synchronize()
+    assert np.array_equal(dev.cpu().numpy(), got)
