@@ -101,11 +101,13 @@ def scf_occupation(sval, tnumele: float, tf: float = 3.0e-3, tfmin: float = -3.0
     sval = np.asarray(sval, dtype=np.float64)
 
     def count(ferm):
-        f = np.array([fermidis(fwght, e, tf, ferm) for e in sval])
-        s = 0.0
-        for v in f:
-            s = s + v
-        return f, s
+        # fermidis of every band at once (the same formula and clipping), and
+        # the electron count summed left to right as the Fortran loop does
+        acoef = (sval - ferm) / tf
+        inside = np.abs(acoef) < 1.0e2
+        f = np.where(inside, 1.0 / (np.exp(np.where(inside, acoef, 0.0)) + 1.0),
+                     np.where(acoef > 0.0, 0.0, 1.0)) * fwght
+        return f, float(np.cumsum(f)[-1]) if f.size else 0.0
 
     ferm1, ferm3 = tfmax, tfmin
     _, n1 = count(ferm1)
