@@ -174,7 +174,8 @@ int rs_gram_f64(int m, int n, long K, const double* A, long lda, const double* B
 /* Y(dev) = X Z: band j of Y = sum_k Z(k,j) * band k of X, Z FP64 column-major
  * (kin x nout, ldz) -- the Psi <- Psi Z updates of rayleighritz_r
  * (rayleigh-ritz8f.F90:96-119).  FP32: tcgen05 3xTF32 with X read
- * MN-major; npts and ldx multiples of 4.  Y must not alias X. */
+ * MN-major; npts and ldx multiples of 4.  FP32: Y may alias X (X is packed
+ * into tensor-core blocks before Y is written); FP64: Y must not alias X. */
 int rs_rotate_f32(long npts, int kin, int nout, const float* X, long ldx, const double* Z,
                   long ldz, float* Y, long ldy, void* stream);
 int rs_rotate_f64(long npts, int kin, int nout, const double* X, long ldx, const double* Z,

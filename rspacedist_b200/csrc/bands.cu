@@ -544,6 +544,15 @@ __global__ void k_move_bands(long n, const int* __restrict__ sband, const T* __r
   stpk<T, V>(dst + (long)dband[k] * n + e, ldpk<T, V>(src + (long)sband[k] * n + e));
 }
 
+// A(i, j) = A(j, i) for i < j (column-major M x M): the upper triangle
+// becomes the mirror of the lower one
+__global__ void k_mirror_lower(int M, double* A) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)M * M) return;
+  const int i = (int)(idx % M), j = (int)(idx / M);
+  if (i < j) A[(long)j * M + i] = A[(long)i * M + j];
+}
+
 }  // namespace
 
 // ============================================================ the solver
@@ -699,25 +708,30 @@ struct BandCtx {
     return rc;
   }
 
-  // Psi <- Psi Z, S Psi <- S Psi Z, <p|Psi> <- <p|Psi> Z (Z FP64 M x M)
+  // Psi <- Psi Z, S Psi <- S Psi Z, <p|Psi> <- <p|Psi> Z (Z FP64 M x M).
+  // The FP32 rotation packs its operand into tensor-core blocks before the
+  // product reads anything, so it writes the result over Psi in place; the
+  // FP64 product (a library GEMM) goes through a work array.
   int rotate_all(const double* Z) {
     int rc = RS_OK;
-    T* tmp = nullptr;
-    RS_CUDA(cudaMallocAsync((void**)&tmp, sizeof(T) * (size_t)N * M, st));
     T* arrs[2] = {psi, sep() ? spsi : nullptr};
-    for (T* a : arrs) {
-      if (!a || rc) continue;
-      if constexpr (sizeof(T) == 4)
-        rc = rotate_f32(N, M, M, (const float*)a, N, Z, M, (float*)tmp, N, st);
-      else
+    if constexpr (sizeof(T) == 4) {
+      for (T* a : arrs)
+        if (a && !rc) rc = rotate_f32(N, M, M, (const float*)a, N, Z, M, (float*)a, N, st);
+    } else {
+      T* tmp = nullptr;
+      RS_CUDA(cudaMallocAsync((void**)&tmp, sizeof(T) * (size_t)N * M, st));
+      for (T* a : arrs) {
+        if (!a || rc) continue;
         rc = rotate_f64(N, M, M, (const double*)a, N, Z, M, (double*)tmp, N, st);
-      if (!rc) {
-        cudaError_t e = cudaMemcpyAsync(a, tmp, sizeof(T) * (size_t)N * M,
-                                        cudaMemcpyDeviceToDevice, st);
-        if (e != cudaSuccess) rc = cuda_status(e, "rotate copy");
+        if (!rc) {
+          cudaError_t e = cudaMemcpyAsync(a, tmp, sizeof(T) * (size_t)N * M,
+                                          cudaMemcpyDeviceToDevice, st);
+          if (e != cudaSuccess) rc = cuda_status(e, "rotate copy");
+        }
       }
+      cudaFreeAsync(tmp, st);
     }
-    cudaFreeAsync(tmp, st);
     if (rc || nrp == 0) return rc;
     double* tr = nullptr;
     RS_CUDA(cudaMallocAsync((void**)&tr, sizeof(double) * (size_t)nrp * M, st));
@@ -1003,12 +1017,7 @@ static int rayleighritz(BandCtx<T>& c, int l_rrb, double* sval_h) {
     rc = gram_f64(M, M, c.N, (const double*)c.psi, c.N, (const double*)c.hpsi, c.N, dv, A, M, c.st);
   // dsyev('v','l') reads the lower triangle: mirror it
   if (!rc) {
-    std::vector<double> h((size_t)M * M);
-    cudaMemcpyAsync(h.data(), A, sizeof(double) * M * M, cudaMemcpyDeviceToHost, c.st);
-    cudaStreamSynchronize(c.st);
-    for (int j = 0; j < M; ++j)
-      for (int i = 0; i < j; ++i) h[(size_t)j * M + i] = h[(size_t)i * M + j];
-    cudaMemcpyAsync(A, h.data(), sizeof(double) * M * M, cudaMemcpyHostToDevice, c.st);
+    k_mirror_lower<<<div_up((long)M * M, 256), 256, 0, c.st>>>(M, A);
     rc = syev_jacobi(M, A, w, Z, 60, c.st, nullptr);
   }
   if (!rc) rc = c.rotate_all(Z);

@@ -641,6 +641,8 @@ int gram_f32(int m, int n, long K, const float* A, long lda, const float* B, lon
   return check_tc_error(st);
 }
 
+// Y may be X (same layout, nout <= kin): X is read only by the packing pass,
+// which completes before the product writes Y.
 int rotate_f32(long npts, int kin, int nout, const float* X, long ldx, const double* Z, long ldz,
                float* Y, long ldy, cudaStream_t st) {
   if (npts <= 0 || nout <= 0) return RS_OK;

@@ -18,7 +18,6 @@
 #include <math.h>
 
 #include <algorithm>
-#include <vector>
 
 #include "rs_common.cuh"
 
@@ -142,11 +141,13 @@ __global__ void __launch_bounds__(256) k_proj_fine(ProjArgs a, int a0,
   }
 }
 
-// one contraction pass: out[p][i2][i1][o0] = sum_j in[p][i2'][...] w(j) along
-// one axis.  Shapes are given as (n0, n1, n2) of the output with the input's
-// strides; the tap index of output coordinate t is t * npmesh - (npmesh-1)/2 + j
-// on the contracted axis (input coordinates are offset by the input's lower
-// bound).  axis: 0 = x (contiguous), 1 = y, 2 = z.
+// One contraction pass of the double grid along one axis (0 = x, the
+// contiguous one; 1 = y; 2 = z).  Output element (c0, c1, c2) of plane p
+// (atom x projector), coordinates from the output's lower bounds lo0..lo2, is
+//     sum_{j = js..je} in[p][... c_axis -> t*npmesh - (npmesh-1)/2 + j ...] w(j)
+// with t = c_axis; the two other coordinates index the input directly (their
+// lower bounds equal the output's), the contracted one from the input's lower
+// bound ilo.  The sum runs in the order of the Fortran loop over j.
 struct DgPass {
   int n0, n1, n2;           // output extents (x, y, z order)
   int lo0, lo1, lo2;        // output lower bounds (-n/2 + 1)
