@@ -272,9 +272,11 @@ __global__ void __launch_bounds__(HZ2_THREADS, 1) k_hlap_zmarch2(int nx, int ny,
                                                                  double* __restrict__ ap,
                                                                  const CgScalars* __restrict__ s,
                                                                  const double* __restrict__ b = nullptr,
-                                                                 float* __restrict__ out32 = nullptr) {
+                                                                 float* __restrict__ out32 = nullptr,
+                                                                 double* __restrict__ rpart = nullptr) {
   static_assert(NF % 2 == 0, "double2 path needs an even halo");
   if (s->done || (RES && !s->upd)) return;
+  double racc = 0.0;  // RES: r.r of this thread's FP32 residual values
   constexpr int HX = HZ2_TX + 2 * NF, HY = HZ2_TY + 2 * NF, PL = HX * HY, RING = hz2_ring(NF);
   constexpr int PL2 = PL / 2, NST = (PL2 + HZ2_THREADS - 1) / HZ2_THREADS;
   extern __shared__ double2 hz2_sm[];  // [RING][HY][HX / 2]
@@ -377,7 +379,10 @@ __global__ void __launch_bounds__(HZ2_THREADS, 1) k_hlap_zmarch2(int nx, int ny,
       const long o = (long)z * plane + own;
       if (RES) {
         const double2 bb = *reinterpret_cast<const double2*>(b + o);
-        *reinterpret_cast<float2*>(out32 + o) = make_float2((float)(bb.x - a0), (float)(bb.y - a1));
+        const float2 r = make_float2((float)(bb.x - a0), (float)(bb.y - a1));
+        *reinterpret_cast<float2*>(out32 + o) = r;
+        racc = fma((double)r.x, (double)r.x, racc);
+        racc = fma((double)r.y, (double)r.y, racc);
       } else {
         *reinterpret_cast<double2*>(ap + o) = make_double2(a0, a1);
       }
@@ -386,6 +391,20 @@ __global__ void __launch_bounds__(HZ2_THREADS, 1) k_hlap_zmarch2(int nx, int ny,
     for (int k = 0; k < 2 * NF; ++k) q[k] = q[k + 1];
   }
   cp_wait_hz<0>();
+  if (RES) {
+    // this CTA's share of r.r, summed in a fixed order (lanes, then warps)
+    __shared__ double rws[HZ2_THREADS / 32];
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) racc = racc + __shfl_down_sync(0xffffffffu, racc, off);
+    if ((tid & 31) == 0) rws[tid >> 5] = racc;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < HZ2_THREADS / 32; ++w) t = t + rws[w];
+      rpart[blockIdx.x] = t;
+    }
+  }
 }
 
 // chunk sums of p.ap in the reduction tree's order, from the stored ap
@@ -733,26 +752,6 @@ __global__ void k_cg_fold_dvh(long N, const CgScalars* __restrict__ s, float* __
   }
 }
 
-// r.r chunk sums of the FP32 residual, after it was recomputed in FP64
-// (blocks stride over the 4096-point chunks)
-__global__ void __launch_bounds__(kTreeLanes) k_cg_rr_f(long N, long nblk, const CgScalars* s,
-                                                        const float* __restrict__ r,
-                                                        double* __restrict__ part) {
-  if (s->done || !s->upd) return;
-  __shared__ double ws[8];
-  for (long cb = blockIdx.x; cb < nblk; cb += gridDim.x) {
-    const long base = cb * kTreeChunk + threadIdx.x;
-    double acc = 0.0;
-#pragma unroll 4
-    for (int k = 0; k < kTreePerLane; ++k) {
-      const long i = base + (long)k * kTreeLanes;
-      if (i < N) acc = fma((double)r[i], (double)r[i], acc);
-    }
-    const double t = tree_fold256(acc, ws);
-    if (threadIdx.x == 0) part[cb] = t;
-  }
-}
-
 // beta, dp and the stopping rule of scf_hartree_cg from r2r (shared by the
 // two folds of the mixed solve)
 __device__ void cg_close_iteration(CgScalars* s, double t, int loop, int ncgres, int ncgmin,
@@ -986,15 +985,15 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
     k_cg_fold_beta_f<<<1, kTreeLanes, 0, st>>>(nblk, part, sc, ncgres, ncgmin, lmax, epsvh, ddx,
                                                ddy, ddz, vol);
     k_cg_fold_dvh<<<std::min(gN, kGatedBlocks), 256, 0, st>>>(N, sc, fdv, vh);
+    // the FP64 residual rounded into r, with its r.r partials per CTA (in the
+    // FP64 A p array too: the update has consumed the p.Ap partials by now)
     switch (nfh) {
-      case 2: k_hlap_zmarch2<2, true><<<gz, HZ2_THREADS, hz2_smem(2), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr); break;
-      case 4: k_hlap_zmarch2<4, true><<<gz, HZ2_THREADS, hz2_smem(4), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr); break;
-      default: k_hlap_zmarch2<6, true><<<gz, HZ2_THREADS, hz2_smem(6), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr); break;
+      case 2: k_hlap_zmarch2<2, true><<<gz, HZ2_THREADS, hz2_smem(2), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr, ap); break;
+      case 4: k_hlap_zmarch2<4, true><<<gz, HZ2_THREADS, hz2_smem(4), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr, ap); break;
+      default: k_hlap_zmarch2<6, true><<<gz, HZ2_THREADS, hz2_smem(6), st>>>(nx, ny, nz, zchunk, hc, vh, nullptr, sc, b, fr, ap); break;
     }
-    k_cg_rr_f<<<std::min((unsigned)nblk, kGatedBlocks), kTreeLanes, 0, st>>>(N, nblk, sc, fr,
-                                                                              part);
-    k_cg_fold_upd_f<<<1, kTreeLanes, 0, st>>>(nblk, part, sc, ncgres, ncgmin, lmax, epsvh, ddx,
-                                              ddy, ddz, vol);
+    k_cg_fold_upd_f<<<1, kTreeLanes, 0, st>>>((long)gz, ap, sc, ncgres, ncgmin, lmax, epsvh,
+                                              ddx, ddy, ddz, vol);
     if (N % 4 == 0) k_cg_dir_f<4><<<div_up(N / 4, 256), 256, 0, st>>>(N, sc, fr, fp);
     else k_cg_dir_f<1><<<gN, 256, 0, st>>>(N, sc, fr, fp);
   };

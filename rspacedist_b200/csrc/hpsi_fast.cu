@@ -319,17 +319,52 @@ __global__ void __launch_bounds__(128) k_nl_rmw_f32(
     if (b < nbb) out[(long)(b0 + b) * N + p] = h[b];
 }
 
-// S psi = psi + sum_e t[atom_e][b] . p_e in one pass over the grid: a thread
-// owns 4 consecutive points (one 16-byte vector per band) and SP_BANDS bands,
-// reads psi once, adds the projector sums of the points that lie inside a
-// support (the entries of the inverse list, in its order, each sum an FMA
-// chain over the projectors as in k_nl_rmw_f32) and writes S psi once.  psi
-// == out is allowed: a thread reads its values before writing them.
+// S psi in two passes.  k_entry_sums: s[b][e] = sum_j t[atom_e][b][j] p_e[j]
+// for every inverse-list entry e, one FMA chain in projector order (the sum
+// k_nl_rmw_f32 adds per entry); a thread owns one entry and NL_BANDS bands,
+// lanes of a warp mostly share the atom, so the t loads are broadcasts.
+__global__ void __launch_bounds__(128) k_entry_sums(long nent, const int* __restrict__ inv_atom,
+                                                    const float* __restrict__ inv_v,
+                                                    const float* __restrict__ tco, int P, int nb,
+                                                    float* __restrict__ s) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nent) return;
+  const int b0 = blockIdx.y * NL_BANDS;
+  const int nbb = min(NL_BANDS, nb - b0);
+  const int at = __ldg(inv_atom + e);
+  const int nq = P / 4;
+  float4 v[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = q < nq ? ld4(inv_v + e * P + 4 * q) : zero4();
+  const float* tb = tco + ((long)at * nb + b0) * P;
+#pragma unroll
+  for (int b = 0; b < NL_BANDS; ++b) {
+    if (b < nbb) {
+      float sum = 0.f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (q < nq) {
+          const float4 t = ld4(tb + (long)b * P + 4 * q);
+          sum = fmaf(t.x, v[q].x, sum);
+          sum = fmaf(t.y, v[q].y, sum);
+          sum = fmaf(t.z, v[q].z, sum);
+          sum = fmaf(t.w, v[q].w, sum);
+        }
+      }
+      s[(long)(b0 + b) * nent + e] = sum;
+    }
+  }
+}
+
+// k_spsi_apply: S psi = psi + the entry sums of each point, added in the
+// inverse-list order (so the same additions as k_nl_rmw_f32).  A thread owns
+// 4 consecutive points (one 16-byte vector per band) and SP_BANDS bands,
+// reads psi and writes S psi once; psi == out is allowed (a thread reads its
+// values before writing them).
 constexpr int SP_BANDS = 8;
-__global__ void __launch_bounds__(128) k_spsi_f32_fused(
-    long N, int nb, const float* psi, float* out, const int* __restrict__ inv_off,
-    const int* __restrict__ inv_atom, const float* __restrict__ inv_v,
-    const float* __restrict__ tco, int P) {
+__global__ void __launch_bounds__(128) k_spsi_apply(long N, int nb, long nent, const float* psi,
+                                                    float* out, const int* __restrict__ inv_off,
+                                                    const float* __restrict__ s) {
   const long p0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
   if (p0 >= N) return;
   const int b0 = blockIdx.y * SP_BANDS;
@@ -340,31 +375,17 @@ __global__ void __launch_bounds__(128) k_spsi_f32_fused(
     h[b] = b < nbb ? ld4(psi + (long)(b0 + b) * N + p0) : zero4();
   const int4 o4 = __ldg(reinterpret_cast<const int4*>(inv_off + p0));
   const int o[5] = {o4.x, o4.y, o4.z, o4.w, __ldg(inv_off + p0 + 4)};
-  const int nq = P / 4;
+  if (o[4] > o[0]) {
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    for (int e = o[k]; e < o[k + 1]; ++e) {
-      const int at = __ldg(inv_atom + e);
-      float4 v[4];
+    for (int k = 0; k < 4; ++k) {
+      for (int e = o[k]; e < o[k + 1]; ++e) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) v[q] = q < nq ? ld4(inv_v + (long)e * P + 4 * q) : zero4();
-      const float* tb = tco + ((long)at * nb + b0) * P;
-#pragma unroll
-      for (int b = 0; b < SP_BANDS; ++b) {
-        if (b < nbb) {
-          float sum = 0.f;
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            if (q < nq) {
-              const float4 t = ld4(tb + (long)b * P + 4 * q);
-              sum = fmaf(t.x, v[q].x, sum);
-              sum = fmaf(t.y, v[q].y, sum);
-              sum = fmaf(t.z, v[q].z, sum);
-              sum = fmaf(t.w, v[q].w, sum);
-            }
+        for (int b = 0; b < SP_BANDS; ++b) {
+          if (b < nbb) {
+            const float v = __ldg(s + (long)(b0 + b) * nent + e);
+            float* hk = k == 0 ? &h[b].x : (k == 1 ? &h[b].y : (k == 2 ? &h[b].z : &h[b].w));
+            *hk += v;
           }
-          float* hk = k == 0 ? &h[b].x : (k == 1 ? &h[b].y : (k == 2 ? &h[b].z : &h[b].w));
-          *hk += sum;
         }
       }
     }
@@ -475,12 +496,24 @@ int launch_spsi_f32_fast(const rs_geom* g, const double* sss, const double* rp, 
   const bool vec = g->N % 4 == 0 && ((uintptr_t)psi | (uintptr_t)out) % 16 == 0 &&
                    nb <= 65535 * SP_BANDS;
   if (vec) {
-    dim3 grid(div_up(g->N / 4, 128), div_up(nb, SP_BANDS));
-    k_spsi_f32_fused<<<grid, 128, 0, st>>>(g->N, nb, psi, out, g->d_inv_off, g->d_inv_atom,
-                                            g->d_inv_v32, t, g->nprjmx);
-    e = cudaGetLastError();
+    const long ne = g->n_inv;
+    float* sums = nullptr;
+    if (ne > 0) {
+      e = cudaMallocAsync((void**)&sums, sizeof(float) * (size_t)ne * nb, st);
+      if (e == cudaSuccess) {
+        dim3 g1(div_up(ne, 128), div_up(nb, NL_BANDS));
+        k_entry_sums<<<g1, 128, 0, st>>>(ne, g->d_inv_atom, g->d_inv_v32, t, g->nprjmx, nb, sums);
+      }
+    }
+    if (e == cudaSuccess) {
+      dim3 g2(div_up(g->N / 4, 128), div_up(nb, SP_BANDS));
+      k_spsi_apply<<<g2, 128, 0, st>>>(g->N, nb, ne > 0 ? ne : 1, psi, out, g->d_inv_off,
+                                        sums);
+      e = cudaGetLastError();
+    }
+    if (sums) cudaFreeAsync(sums, st);
     cudaFreeAsync(t, st);
-    if (e != cudaSuccess) return cuda_status(e, "k_spsi_f32_fused");
+    if (e != cudaSuccess) return cuda_status(e, "S psi (k_entry_sums, k_spsi_apply)");
     return RS_OK;
   }
   // otherwise out = psi, then the nonlocal sums added on the points inside a

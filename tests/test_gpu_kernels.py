@@ -109,9 +109,10 @@ def test_hpsi_f32(setup, oracle, nb):
 
 
 @pytest.mark.parametrize("nb", [1, 8, 13])
-def test_spsi_f32_one_pass_matches_two_pass(setup, nb):
-    """The one-pass FP32 S psi (16-byte vectors) and the copy + covered-point
-    pass used for unaligned bands give the same bits, also in place."""
+def test_spsi_f32_vector_path_matches_rmw_path(setup, nb):
+    """The FP32 S psi of aligned bands (per-entry sums, then one 16-byte
+    vector pass over the grid) and the copy + covered-point pass used for
+    unaligned bands give the same bits, also in place."""
     from rspacedist_b200 import kukan as K, system as S
     cell, g, veff, _ = setup
     psi = torch.tensor(S.random_bands(cell, nb, 7), dtype=torch.float32, device="cuda")
