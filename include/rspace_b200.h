@@ -166,7 +166,9 @@ int rs_hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, dou
  * (orthogonalization8f.F90:225-228).  FP32 operands run on tcgen05 tensor
  * cores with the 3xTF32 split and FP32 accumulation over K chunks of 16384,
  * chunks summed in FP64; sym=1 (A==B, m==n) computes one triangle and
- * mirrors it.  K, lda, ldb multiples of 4. */
+ * mirrors it; sym=2 (m==n, A and B distinct, a product known to be
+ * symmetric such as Psi^T H Psi) computes the lower triangle C(i,j), i >= j,
+ * and mirrors it into the upper one.  K, lda, ldb multiples of 4. */
 int rs_gram_f32(int m, int n, long K, const float* A, long lda, const float* B, long ldb,
                 double alpha, double* C, long ldc, int sym, void* stream);
 int rs_gram_f64(int m, int n, long K, const double* A, long lda, const double* B, long ldb,

@@ -698,8 +698,10 @@ struct BandCtx {
     W = G + (size_t)M * M;
     const double dv = dx * dy * dz;
     if constexpr (sizeof(T) == 4)
+      // the Cholesky reads the lower triangle only: with S psi != psi the
+      // product is computed for the lower tile pairs and mirrored
       rc = gram_f32(M, M, N, (const float*)psi, N, (const float*)spsi, N, dv, G, M,
-                    spsi == psi, st);
+                    spsi == psi ? 1 : 2, st);
     else
       rc = gram_f64(M, M, N, (const double*)psi, N, (const double*)spsi, N, dv, G, M, st);
     if (!rc) rc = chol_inv_t(M, G, W, st);
@@ -1012,7 +1014,8 @@ static int rayleighritz(BandCtx<T>& c, int l_rrb, double* sval_h) {
   w = Z + (size_t)M * M;
   const double dv = c.dx * c.dy * c.dz;
   if constexpr (sizeof(T) == 4)
-    rc = gram_f32(M, M, c.N, (const float*)c.psi, c.N, (const float*)c.hpsi, c.N, dv, A, M, 0, c.st);
+    rc = gram_f32(M, M, c.N, (const float*)c.psi, c.N, (const float*)c.hpsi, c.N, dv, A, M, 2,
+                  c.st);  // lower tile pairs: dsyev('v','l') reads the lower triangle
   else
     rc = gram_f64(M, M, c.N, (const double*)c.psi, c.N, (const double*)c.hpsi, c.N, dv, A, M, c.st);
   // dsyev('v','l') reads the lower triangle: mirror it

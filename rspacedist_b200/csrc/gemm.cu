@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(GRAM_THREADS, 1)
       jt = pr / tn;
     }
   }
-  const bool same = sym && it == jt;
+  const bool same = sym == 1 && it == jt;  // one block serves both operands
   const int kb0 = blockIdx.y * kbc;
   const int nst = max(0, min(nkb, kb0 + kbc) - kb0);
   const int ngrp = (nst + DGRP - 1) / DGRP;
@@ -597,7 +597,11 @@ int gram_f32(int m, int n, long K, const float* A, long lda, const float* B, lon
     return fail(RS_EINVAL, "rs_gram_f32: K, lda, ldb must be multiples of 4, A/B 16-byte aligned");
   if (K <= 0 || lda < K || ldb < K)
     return fail(RS_EINVAL, "rs_gram_f32: K must be positive and at most lda, ldb");
-  if (sym && (m != n || A != B || lda != ldb)) sym = 0;
+  // sym 1: A == B, one triangle, diagonal blocks loaded once; sym 2: the
+  // lower-triangle tile pairs of a product known to be symmetric (A != B)
+  if (sym == 1 && (m != n || A != B || lda != ldb)) sym = 0;
+  if (sym == 2 && m != n) sym = 0;
+  const bool shared = sym == 1;
   keep_pool_memory();
   const int tm = (m + GM - 1) / GM, tn = (n + GN - 1) / GN;
   const int npairs = sym ? tm * (tm + 1) / 2 : tm * tn;
@@ -609,7 +613,8 @@ int gram_f32(int m, int n, long K, const float* A, long lda, const float* B, lon
   const int ns = (int)gram_splits(npairs, piece);
   const int kbc = (nkb + ns - 1) / ns;
   const int nsplit = (int)npieces * ns;
-  const size_t abytes = (size_t)tm * nkb * 2 * OPB, bbytes = sym ? 0 : (size_t)tn * nkb * 2 * OPB;
+  const size_t abytes = (size_t)tm * nkb * 2 * OPB,
+               bbytes = shared ? 0 : (size_t)tn * nkb * 2 * OPB;
   char* at = nullptr;
   double* part = nullptr;
   RS_CUDA(cudaMallocAsync((void**)&at, abytes + bbytes, st));
@@ -618,13 +623,13 @@ int gram_f32(int m, int n, long K, const float* A, long lda, const float* B, lon
     cudaFreeAsync(at, st);
     return cuda_status(e, "rs_gram_f32: work arrays");
   }
-  char* bt = sym ? at : at + abytes;
+  char* bt = shared ? at : at + abytes;
   e = cudaFuncSetAttribute(k_gram_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)TC_SMEM);
   for (long pc = 0; pc < npieces && e == cudaSuccess; ++pc) {
     const long k0 = pc * piece;
     k_tile_rows<<<(unsigned)(tm * nkb), 256, 0, st>>>(A, lda, m, k0, K, nkb, at);
-    if (!sym) k_tile_rows<<<(unsigned)(tn * nkb), 256, 0, st>>>(B, ldb, n, k0, K, nkb, bt);
+    if (!shared) k_tile_rows<<<(unsigned)(tn * nkb), 256, 0, st>>>(B, ldb, n, k0, K, nkb, bt);
     dim3 grid(npairs, ns);
     k_gram_tf32x3<<<grid, GRAM_THREADS, TC_SMEM, st>>>(at, bt, nkb, kbc, sym, tm, (int)pc * ns,
                                                        nsplit, part);

@@ -35,6 +35,30 @@ def test_gram_f32_tensor_cores(built_lib, cuda, m, n, K, sym):
     assert err < 2e-6, err
 
 
+@pytest.mark.parametrize("m,K", [(20, 32768), (257, 20004), (300, 50000)])
+def test_gram_f32_lower_triangle(built_lib, cuda, m, K):
+    """sym=2: the lower triangle of A B^T for distinct A, B (a product known to
+    be symmetric), mirrored into the upper one.  The K splits follow the
+    number of tile pairs, so the lower triangle agrees with the full product
+    to rounding, not bit for bit."""
+    from rspacedist_b200 import lib
+    rng = np.random.default_rng(m + K)
+    A = rng.standard_normal((m, K)).astype(np.float32)
+    B = rng.standard_normal((m, K)).astype(np.float32)
+    ref = A.astype(np.float64) @ B.astype(np.float64).T
+    dA, dB = torch.tensor(A, device="cuda"), torch.tensor(B, device="cuda")
+    full = torch.zeros((m, m), dtype=torch.float64, device="cuda")
+    low = torch.zeros_like(full)
+    lib.call("rs_gram_f32", m, m, K, _p(dA), K, _p(dB), K, 1.0, _p(full), m, 0, _s())
+    lib.call("rs_gram_f32", m, m, K, _p(dA), K, _p(dB), K, 1.0, _p(low), m, 2, _s())
+    f, lo = full.cpu().numpy().T, low.cpu().numpy().T  # C(i, j) at [i, j]
+    il = np.tril_indices(m)
+    assert np.array_equal(lo, lo.T)
+    scale = np.abs(ref).max()
+    assert np.abs(lo[il] - ref[il]).max() < 2e-6 * scale
+    assert np.abs(lo[il] - f[il]).max() < 2e-6 * scale
+
+
 @pytest.mark.parametrize("npts,kin,nout", [(4096, 20, 20), (65536, 160, 160),
                                            (12288, 300, 270), (8192, 70, 513),
                                            (4100, 33, 129)])
