@@ -712,14 +712,19 @@ struct BandCtx {
 
   // Psi <- Psi Z, S Psi <- S Psi Z, <p|Psi> <- <p|Psi> Z (Z FP64 M x M).
   // The FP32 rotation packs its operand into tensor-core blocks before the
-  // product reads anything, so it writes the result over Psi in place; the
-  // FP64 product (a library GEMM) goes through a work array.
+  // product reads anything, so it writes the result over Psi in place.  On
+  // the FP32 path S Psi Z is formed as S (Psi Z) from the rotated Psi and
+  // <p|Psi> Z (S is linear; one S pass costs a sixth of a rotation); the
+  // FP64 path rotates S Psi, its product (a library GEMM) through a work
+  // array.
   int rotate_all(const double* Z) {
     int rc = RS_OK;
     T* arrs[2] = {psi, sep() ? spsi : nullptr};
     if constexpr (sizeof(T) == 4) {
-      for (T* a : arrs)
-        if (a && !rc) rc = rotate_f32(N, M, M, (const float*)a, N, Z, M, (float*)a, N, st);
+      rc = rotate_f32(N, M, M, (const float*)psi, N, Z, M, (float*)psi, N, st);
+      if (!rc && nrp > 0) rc = rotate_rp(Z);
+      if (!rc && sep()) rc = apply_s(psi, rp, spsi, M);
+      return rc;
     } else {
       T* tmp = nullptr;
       RS_CUDA(cudaMallocAsync((void**)&tmp, sizeof(T) * (size_t)N * M, st));
@@ -735,9 +740,13 @@ struct BandCtx {
       cudaFreeAsync(tmp, st);
     }
     if (rc || nrp == 0) return rc;
+    return rotate_rp(Z);
+  }
+  // <p|Psi> <- <p|Psi> Z (FP64)
+  int rotate_rp(const double* Z) {
     double* tr = nullptr;
     RS_CUDA(cudaMallocAsync((void**)&tr, sizeof(double) * (size_t)nrp * M, st));
-    rc = rotate_f64(nrp, M, M, rp, nrp, Z, M, tr, nrp, st);
+    int rc = rotate_f64(nrp, M, M, rp, nrp, Z, M, tr, nrp, st);
     if (!rc) RS_CUDA(cudaMemcpyAsync(rp, tr, sizeof(double) * (size_t)nrp * M,
                                      cudaMemcpyDeviceToDevice, st));
     cudaFreeAsync(tr, st);
