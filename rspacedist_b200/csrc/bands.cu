@@ -38,6 +38,8 @@ int gram_f32(int m, int n, long K, const float* A, long lda, const float* B, lon
              double alpha, double* C, long ldc, int sym, cudaStream_t st);
 int gram_f64(int m, int n, long K, const double* A, long lda, const double* B, long ldb,
              double alpha, double* C, long ldc, cudaStream_t st);
+int gram_f64_beta(int m, int n, long K, const double* A, long lda, const double* B, long ldb,
+                  double alpha, double beta, double* C, long ldc, cudaStream_t st);
 int rotate_f32(long npts, int kin, int nout, const float* X, long ldx, const double* Z, long ldz,
                float* Y, long ldy, cudaStream_t st);
 int rotate_f64(long npts, int kin, int nout, const double* X, long ldx, const double* Z, long ldz,
@@ -544,6 +546,25 @@ __global__ void k_move_bands(long n, const int* __restrict__ sband, const T* __r
   stpk<T, V>(dst + (long)dband[k] * n + e, ldpk<T, V>(src + (long)sband[k] * n + e));
 }
 
+// T[b][a][i] = sum_j S_a(i, j) <p_j|psi_b> with S_a(i, j) = m[(a*P + i)*P + j]
+// (the projector sums of S psi before the 1/dV, in the order of k_tcoef_f32)
+__global__ void k_s_rp(int M, int natom, int P, const int* __restrict__ nprj,
+                       const double* __restrict__ m, const double* __restrict__ rp,
+                       double* __restrict__ T) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)M * natom * P) return;
+  const int i = (int)(idx % P);
+  const long ba = idx / P;
+  const int a = (int)(ba % natom);
+  const int pa = nprj[a];
+  const double* r = rp + ba * P;
+  const double* s = m + ((long)a * P + i) * P;
+  double acc = 0.0;
+  if (i < pa)
+    for (int j = 0; j < pa; ++j) acc = fma(r[j], s[j], acc);
+  T[idx] = acc;
+}
+
 // A(i, j) = A(j, i) for i < j (column-major M x M): the upper triangle
 // becomes the mirror of the lower one
 __global__ void k_mirror_lower(int M, double* A) {
@@ -689,21 +710,40 @@ struct BandCtx {
   // Psi <- Psi L^-T, S Psi and <p|Psi> likewise.
   int ortho_all(bool cmpt) {
     int rc;
+    // FP32 with an S metric: dV Psi^T S Psi = dV Psi^T Psi + <p|Psi>^T S <p|Psi>
+    // (the nonlocal part of S psi is sum_a |p> S_a <p|psi> / dV), so the Gram
+    // needs <p|Psi> but not S Psi, which rotate_all forms afterwards
+    const bool split = sizeof(T) == 4 && sep() && nrp > 0;
     if (cmpt) {
       if ((rc = nl_dot(psi, rp, M))) return rc;
-      if (sep() && (rc = apply_s(psi, rp, spsi, M))) return rc;
+      if (sep() && !split && (rc = apply_s(psi, rp, spsi, M))) return rc;
     }
     double *G = nullptr, *W = nullptr;
     RS_CUDA(cudaMallocAsync((void**)&G, sizeof(double) * 2 * (size_t)M * M, st));
     W = G + (size_t)M * M;
     const double dv = dx * dy * dz;
-    if constexpr (sizeof(T) == 4)
-      // the Cholesky reads the lower triangle only: with S psi != psi the
-      // product is computed for the lower tile pairs and mirrored
-      rc = gram_f32(M, M, N, (const float*)psi, N, (const float*)spsi, N, dv, G, M,
-                    spsi == psi ? 1 : 2, st);
-    else
+    if constexpr (sizeof(T) == 4) {
+      // the Cholesky reads the lower triangle only: one triangle of tile pairs
+      if (split) {
+        rc = gram_f32(M, M, N, (const float*)psi, N, (const float*)psi, N, dv, G, M, 1, st);
+        double* Ts = nullptr;
+        if (!rc) {
+          cudaError_t e = cudaMallocAsync((void**)&Ts, sizeof(double) * (size_t)nrp * M, st);
+          if (e != cudaSuccess) rc = cuda_status(e, "ortho_all: S <p|psi>");
+        }
+        if (!rc) {
+          k_s_rp<<<div_up((long)nrp * M, 256), 256, 0, st>>>(M, g->natom, g->nprjmx, g->d_nprj,
+                                                              sss, rp, Ts);
+          rc = gram_f64_beta(M, M, nrp, rp, nrp, Ts, nrp, 1.0, 1.0, G, M, st);
+        }
+        if (Ts) cudaFreeAsync(Ts, st);
+      } else {
+        rc = gram_f32(M, M, N, (const float*)psi, N, (const float*)spsi, N, dv, G, M,
+                      spsi == psi ? 1 : 2, st);
+      }
+    } else {
       rc = gram_f64(M, M, N, (const double*)psi, N, (const double*)spsi, N, dv, G, M, st);
+    }
     if (!rc) rc = chol_inv_t(M, G, W, st);
     if (!rc) rc = rotate_all(W);
     cudaFreeAsync(G, st);

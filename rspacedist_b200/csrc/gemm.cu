@@ -706,9 +706,18 @@ int cublas_status(cublasStatus_t s, const char* what) {
   return fail(RS_ECUDA, std::string(what) + ": cuBLAS status " + std::to_string((int)s));
 }
 
+int gram_f64_beta(int m, int n, long K, const double* A, long lda, const double* B, long ldb,
+                  double alpha, double beta, double* C, long ldc, cudaStream_t st);
+
 // C[i + j*ldc] = alpha sum_k A[i*lda + k] B[j*ldb + k]  (C = alpha A B^T)
 int gram_f64(int m, int n, long K, const double* A, long lda, const double* B, long ldb,
              double alpha, double* C, long ldc, cudaStream_t st) {
+  return gram_f64_beta(m, n, K, A, lda, B, ldb, alpha, 0.0, C, ldc, st);
+}
+
+// C = alpha A^T B + beta C (the same operand layout as gram_f64)
+int gram_f64_beta(int m, int n, long K, const double* A, long lda, const double* B, long ldb,
+                  double alpha, double beta, double* C, long ldc, cudaStream_t st) {
   if (m <= 0 || n <= 0) return RS_OK;
   if (K > INT32_MAX || lda > INT32_MAX || ldb > INT32_MAX)
     return fail(RS_EINVAL, "rs_gram_f64: K and leading dimensions must fit in 32 bits");
@@ -716,7 +725,6 @@ int gram_f64(int m, int n, long K, const double* A, long lda, const double* B, l
   cublasHandle_t h = cublas_handle();
   if (!h) return fail(RS_ECUDA, "rs_gram_f64: cublasCreate failed");
   int rc = cublas_status(cublasSetStream(h, st), "rs_gram_f64");
-  const double beta = 0.0;
   if (!rc)
     rc = cublas_status(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, m, n, (int)K, &alpha, A,
                                    (int)lda, B, (int)ldb, &beta, C, (int)ldc),
