@@ -370,6 +370,44 @@ int rs_hpsi_batch_info(const rs_hpsi_batch* plan, int* threads_per_cta, int* ban
                        int* ctas_per_sm);
 int rs_hpsi_batch_destroy(rs_hpsi_batch* plan);
 
+/* ---- device-resident state handle (the drop-in surface of scf_diag and
+ * scf_charge: kukan8f.F90:466-487, 605-622, 647-662) --------------------- */
+/* One cell and one k-point/spin: psi, S psi, H psi (M x N, precision 32 =
+ * the mixed path or 64 = the plain FP64 path), <p|psi> (FP64), veff, D and S
+ * stay on the GPU between calls; host memory is read at upload and written
+ * only for results (sval, residual_states, rho, psi for checkpoints).  All
+ * work runs on the stream given to rs_create; every call returns when its
+ * results are in place.  A state is used from one host thread.
+ *   rs_create: grid (dx, dy, dz spacings), band count, precision;
+ *   rs_upload_geometry: as rs_geom_create, plus D (natom*nprjmx^2, required
+ *     with atoms) and S (same size, NULL for S = 1), host arrays;
+ *   rs_set_potential: veff (host, FP64, N), stored in the state's precision;
+ *   rs_upload_bands: psi (host, M x N in the state's precision); S psi starts
+ *     as a copy, H psi and <p|psi> as zeros (kukan's state before its first
+ *     orthogonalisation);
+ *   rs_orthogonalize: rs_orthogonalize_* on the state;
+ *   rs_hpsi: H psi of all bands from psi and <p|psi>;
+ *   rs_diag_step: rs_scf_diag_* on the state; sval, resid host (M, in/out);
+ *   rs_density: rho (host, N) = sum_b occ_b psi_b^2 with occ host (M);
+ *   rs_download_bands: psi to host;
+ *   rs_state_arrays: the device pointers, for the other entry points. */
+typedef struct rs_state rs_state;
+int rs_create(rs_state** s, int precision, int nx, int ny, int nz, int nf, double dx, double dy,
+              double dz, int nbands, void* stream);
+int rs_upload_geometry(rs_state* s, int natom, int nprjmx, int num_list, const int* nprj,
+                       const int* natinf, const int* lst, const double* vnlocp,
+                       const double* dij, const double* sss);
+int rs_set_potential(rs_state* s, const double* veff);
+int rs_upload_bands(rs_state* s, const void* psi);
+int rs_orthogonalize(rs_state* s, int cmpt);
+int rs_hpsi(rs_state* s);
+int rs_diag_step(rs_state* s, const rs_solver_prm* prm, int iscf, double* sval, double* resid,
+                 int* ksconv, int* ksitmax);
+int rs_density(rs_state* s, const double* occ, double* rho);
+int rs_download_bands(rs_state* s, void* psi);
+int rs_state_arrays(rs_state* s, void** psi, void** spsi, void** hpsi, double** rp, void** veff);
+int rs_destroy(rs_state* s);
+
 /* ---- fixed-tree reductions (shared order with the oracle) --------------- */
 /* out(dev, 1 double) = sum_i a_i b_i in the documented block tree. */
 int rs_dot_f64(long n, const double* a, const double* b, double* out, void* stream);

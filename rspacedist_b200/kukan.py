@@ -353,6 +353,79 @@ class Bands:
         return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+class State:
+    """The device-resident state handle (rs_create ... rs_destroy): psi, S psi,
+    H psi, <p|psi>, veff, D and S of one cell live in the library; numpy
+    arrays go in and come out."""
+
+    def __init__(self, cell: Cell, nbands: int, precision: int = 32, nf: int = 4):
+        self.cell, self.M, self.prec = cell, nbands, precision
+        self.dtype = np.float32 if precision == 32 else np.float64
+        h = C.c_void_p()
+        L.call("rs_create", C.byref(h), precision, cell.shape[0], cell.shape[1], cell.shape[2],
+               nf, cell.h[0], cell.h[1], cell.h[2], nbands, _stream())
+        self.handle = h
+        self.sval = np.zeros(nbands)
+        self.resid = np.zeros(nbands)
+        ip = lambda a: np.ascontiguousarray(a, np.int32)
+        dp = lambda a: np.ascontiguousarray(a, np.float64)
+        self._keep = [ip(cell.nprj), ip(cell.natinf), ip(cell.lst), dp(cell.vnlocp),
+                      dp(cell.dij), dp(cell.sss) if cell.sss is not None else None]
+        nprj, natinf, lst, v, dij, sss = self._keep
+        P = C.POINTER
+        L.call("rs_upload_geometry", h, cell.natom, cell.nprjmx, cell.num_list,
+               nprj.ctypes.data_as(P(C.c_int)), natinf.ctypes.data_as(P(C.c_int)),
+               lst.ctypes.data_as(P(C.c_int)), v.ctypes.data_as(P(C.c_double)),
+               dij.ctypes.data_as(P(C.c_double)),
+               sss.ctypes.data_as(P(C.c_double)) if sss is not None else None)
+
+    def _d(self, a):
+        return a.ctypes.data_as(C.POINTER(C.c_double))
+
+    def set_potential(self, veff):
+        v = np.ascontiguousarray(veff, np.float64)
+        L.call("rs_set_potential", self.handle, self._d(v))
+
+    def upload_bands(self, psi):
+        p = np.ascontiguousarray(psi, self.dtype)
+        L.call("rs_upload_bands", self.handle, p.ctypes.data_as(C.c_void_p))
+
+    def download_bands(self):
+        out = np.empty((self.M, self.cell.N), self.dtype)
+        L.call("rs_download_bands", self.handle, out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def orthogonalize(self, cmpt: int = 1):
+        L.call("rs_orthogonalize", self.handle, cmpt)
+
+    def hpsi(self):
+        L.call("rs_hpsi", self.handle)
+
+    def diag_step(self, iscf: int, prm=None):
+        prm = prm or L.solver_prm()
+        conv, itm = C.c_int(0), C.c_int(0)
+        L.call("rs_diag_step", self.handle, C.byref(prm), iscf, self._d(self.sval),
+               self._d(self.resid), C.byref(conv), C.byref(itm))
+        return bool(conv.value), itm.value
+
+    def density(self, occ):
+        o = np.ascontiguousarray(occ, np.float64)
+        rho = np.empty(self.cell.N)
+        L.call("rs_density", self.handle, self._d(o), self._d(rho))
+        return rho
+
+    def close(self):
+        if self.handle:
+            L.call("rs_destroy", self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def orthogonalization(b: Bands, cmpt: int = 1):
     """orthogonalization_r_01, all bands (Cholesky-QR in the S metric)."""
     L.call("rs_orthogonalize_" + b.suffix, b.g.handle, _ptr(b.sss), b.M, _ptr(b.psi),

@@ -96,6 +96,18 @@ SIGNATURES = {
     "rs_dot_f32": [_l, _p, _p, _p, _p],
     "rs_atomicocc": [_p, _p, _p, _i, _p, _p],
     "rs_double_grid_weights": [_i, _i, _dp],
+    "rs_create": [C.POINTER(_p), _i, _i, _i, _i, _i, _d, _d, _d, _i, _p],
+    "rs_upload_geometry": [_p, _i, _i, _i, _ip, _ip, _ip, _dp, _dp, _dp],
+    "rs_set_potential": [_p, _dp],
+    "rs_upload_bands": [_p, _p],
+    "rs_orthogonalize": [_p, _i],
+    "rs_hpsi": [_p],
+    "rs_diag_step": [_p, _sp, _i, _dp, _dp, _ip, _ip],
+    "rs_density": [_p, _dp, _dp],
+    "rs_download_bands": [_p, _p],
+    "rs_state_arrays": [_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p), C.POINTER(_dp),
+                        C.POINTER(_p)],
+    "rs_destroy": [_p],
     "rs_projector_tables": [_i, _i, _i, _i, _i, _i, _d, _d, _d, _i, _i, _i, _i, _i, _dp, _dp,
                             _dp, _ip, _ip, _ip, _ip, _ip, _ip, _ip, _ip, _ip, _i, _i, _dp, _d,
                             _d, _d, _d, _i, _d, _dp, _dp, _p],
