@@ -30,7 +30,8 @@ int launch_gather(const rs_geom* g, const double* mat, const double* rp, const T
                   const T* veff, T* out, int nb, cudaStream_t st);
 int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
                          const double* rp, const float* psi, float* hpsi, int nb,
-                         cudaStream_t st);
+                         cudaStream_t st, bool local_only = false);
+bool hpsi_f32_fast_ok(const rs_geom* g, int nb);
 bool spsi_f32_fast_ok(const rs_geom* g);
 int launch_spsi_f32_fast(const rs_geom* g, const double* sss, const double* rp, const float* psi,
                          float* out, int nb, cudaStream_t st);
@@ -1056,16 +1057,40 @@ static int rayleighritz(BandCtx<T>& c, int l_rrb, double* sval_h) {
   c.dx = c.g->dx; c.dy = c.g->dy; c.dz = c.g->dz;
   const int M = c.M;
   int rc = RS_OK;
-  if (l_rrb && (rc = c.apply_h(c.psi, c.rp, c.hpsi, M))) return rc;
+  // FP32 with projectors, H psi recomputed here: dV Psi^T H Psi = dV Psi^T
+  // (-1/2 lap + veff) Psi + <p|Psi>^T D <p|Psi>, so only the local part is
+  // applied (hpsi is work space on exit)
+  bool split = false;
+  if constexpr (sizeof(T) == 4)
+    split = l_rrb && c.nrp > 0 && c.g->natom > 0 && hpsi_f32_fast_ok(c.g, M);
+  if (l_rrb) {
+    if (split)
+      rc = launch_hpsi_f32_fast(c.g, (const float*)c.veff, c.dij, c.rp, (const float*)c.psi,
+                                (float*)c.hpsi, M, c.st, true);
+    else
+      rc = c.apply_h(c.psi, c.rp, c.hpsi, M);
+    if (rc) return rc;
+  }
   double *A = nullptr, *w = nullptr, *Z = nullptr;
   RS_CUDA(cudaMallocAsync((void**)&A, sizeof(double) * ((size_t)2 * M * M + M), c.st));
   Z = A + (size_t)M * M;
   w = Z + (size_t)M * M;
   const double dv = c.dx * c.dy * c.dz;
-  if constexpr (sizeof(T) == 4)
+  if constexpr (sizeof(T) == 4) {
     rc = gram_f32(M, M, c.N, (const float*)c.psi, c.N, (const float*)c.hpsi, c.N, dv, A, M, 2,
                   c.st);  // lower tile pairs: dsyev('v','l') reads the lower triangle
-  else
+    if (!rc && split) {
+      double* Td = nullptr;
+      cudaError_t e = cudaMallocAsync((void**)&Td, sizeof(double) * (size_t)c.nrp * M, c.st);
+      if (e != cudaSuccess) rc = cuda_status(e, "rayleighritz: D <p|psi>");
+      if (!rc) {
+        k_s_rp<<<div_up((long)c.nrp * M, 256), 256, 0, c.st>>>(M, c.g->natom, c.g->nprjmx,
+                                                              c.g->d_nprj, c.dij, c.rp, Td);
+        rc = gram_f64_beta(M, M, c.nrp, c.rp, c.nrp, Td, c.nrp, 1.0, 1.0, A, M, c.st);
+      }
+      if (Td) cudaFreeAsync(Td, c.st);
+    }
+  } else
     rc = gram_f64(M, M, c.N, (const double*)c.psi, c.N, (const double*)c.hpsi, c.N, dv, A, M, c.st);
   // dsyev('v','l') reads the lower triangle: mirror it
   if (!rc) {

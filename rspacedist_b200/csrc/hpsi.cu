@@ -9,7 +9,7 @@ int launch_gather(const rs_geom* g, const double* mat, const double* rp, const T
                   const T* veff, T* out, int nb, cudaStream_t st);
 int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
                          const double* rp, const float* psi, float* hpsi, int nb,
-                         cudaStream_t st);
+                         cudaStream_t st, bool local_only = false);
 }  // namespace rs
 
 extern "C" int rs_hpsi_f32(const rs_geom* g, const float* veff, const double* dij,

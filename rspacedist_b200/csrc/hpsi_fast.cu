@@ -397,14 +397,25 @@ __global__ void __launch_bounds__(128) k_spsi_apply(long N, int nb, long nent, c
 
 }  // namespace
 
-int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
-                         const double* rp, const float* psi, float* hpsi, int nb,
-                         cudaStream_t st) {
-  if (nb <= 0) return RS_OK;
+// true when launch_hpsi_f32_fast takes the z-march (and can stop after its
+// local part) for nb bands
+bool hpsi_f32_fast_ok(const rs_geom* g, int nb) {
   const bool shape_ok = g->nf == 4 && g->nx % 4 == 0 && g->ny % 2 == 0 && g->nx >= 8 &&
                         g->ny >= 8 && g->nz >= 8 && nb <= 65535;
   const bool proj_ok = g->nprjmx % 4 == 0 && g->nprjmx <= 16;
-  if (!shape_ok || !proj_ok) return launch_gather<float, 1>(g, dij, rp, psi, veff, hpsi, nb, st);
+  return shape_ok && proj_ok;
+}
+
+// local_only: (-1/2 lap + veff) psi alone, without the nonlocal term (only
+// where hpsi_f32_fast_ok holds)
+int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
+                         const double* rp, const float* psi, float* hpsi, int nb,
+                         cudaStream_t st, bool local_only) {
+  if (nb <= 0) return RS_OK;
+  if (!hpsi_f32_fast_ok(g, nb)) {
+    if (local_only) return fail(RS_EINVAL, "H psi: local part alone needs the z-march shape");
+    return launch_gather<float, 1>(g, dij, rp, psi, veff, hpsi, nb, st);
+  }
   StArgs a;
   a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
   a.zchunk = g->nz <= 160 ? g->nz : 64;
@@ -424,7 +435,7 @@ int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_stencil_f32_zmarch<false><<<grid, NTHREADS, smem, st>>>(a);
   RS_LAUNCH_CHECK("k_stencil_f32_zmarch");
-  if (g->natom == 0 || g->n_cov == 0) return RS_OK;
+  if (local_only || g->natom == 0 || g->n_cov == 0) return RS_OK;
   const long nt = (long)nb * g->natom * g->nprjmx;
   float* t = nullptr;
   RS_CUDA(cudaMallocAsync((void**)&t, nt * sizeof(float), st));
