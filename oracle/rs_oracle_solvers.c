@@ -4,7 +4,7 @@
  * RMM-DIIS, state reordering and the nonlocal force.  TEST INFRASTRUCTURE
  * (see rs_oracle.c).  Dense products use orc_tree_dot per matrix element;
  * the BLAS calls of the reference have no defined summation order, so parity
- * on these routines is judged within a tolerance, not bit for bit.
+ * on these routines is checked within a tolerance, not bit for bit.
  */
 #include <math.h>
 #include <pthread.h>
