@@ -145,8 +145,11 @@ class Cell:
         return np.full(self.natom, self.nprjmx, np.int32)
 
 
-def make_cell(A, n, atoms, ds, with_s=True) -> Cell:
-    """A: cell edge(s) in bohr, n: grid points per axis (even), atoms (natom,3)."""
+def make_cell(A, n, atoms, ds, with_s=True, filtered: bool = False, npmesh: int = 2) -> Cell:
+    """A: cell edge(s) in bohr, n: grid points per axis (even), atoms (natom,3).
+    filtered: the projector tables of pseudocalc_07 (Fourier-filtered radial
+    functions on the npmesh double grid, built on the GPU by
+    rs_projector_tables) in place of the directly sampled ones."""
     A = np.broadcast_to(np.asarray(A, float), (3,))
     n = np.broadcast_to(np.asarray(n, int), (3,))
     if np.any(n % 2):
@@ -158,6 +161,9 @@ def make_cell(A, n, atoms, ds, with_s=True) -> Cell:
                 atoms=np.asarray(atoms, float).reshape(-1, 3), ds=ds)
     build_lists(cell)
     build_projectors(cell, with_s=with_s)
+    if filtered:
+        from .projectors import projector_tables
+        cell.vnlocp = projector_tables(cell, npmesh=npmesh)
     return cell
 
 

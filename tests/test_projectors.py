@@ -140,3 +140,25 @@ def test_projector_tables_gpu_match_oracle(oracle, cuda, which, npmesh):
     PR.projector_tables(cell, npmesh=npmesh, out=dev)
     torch.cuda.synchronize()
     assert np.array_equal(dev.cpu().numpy(), got)
+
+
+@pytest.mark.gpu
+def test_filtered_tables_drive_the_fp64_hpsi(oracle, cuda):
+    """A cell built with the filtered tables (make_cell(filtered=True)) runs the
+    hot path like any other: FP64 H psi on the GPU equals the oracle's bits."""
+    import torch
+    from rspacedist_b200 import kukan as K, system as S
+    ds = S.load_dataset("si_paw")
+    cell = S.make_cell(10.26, 32, S.diamond_positions(1, 10.26, 0.02, 6), ds, filtered=True)
+    g = K.Geometry(cell)
+    veff = S.smooth_veff(cell, 3)
+    psi = S.random_bands(cell, 3, 8)
+    geo = dict(natom=cell.natom, nprjmx=cell.nprjmx, num_list=cell.num_list, nprj=cell.nprj,
+               natinf=cell.natinf, lst=cell.lst, v=cell.vnlocp.ravel())
+    sysk = oracle.make_sys(geo, cell.shape, 4, cell.h, veff, cell.dij, cell.sss)
+    rp = oracle.nl_dot(geo, psi, cell.N)
+    ref = oracle.hpsi(sysk, psi, rp)
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+    out = K.hpsi(g, t(veff), t(cell.dij), K.nonlocaloperation_01(g, t(psi)), t(psi))
+    assert np.array_equal(out.cpu().numpy(), ref)
+    g.close()
