@@ -83,3 +83,22 @@ def test_sphere_lists_capacity_error(built_lib):
                                    cell.h[1], cell.h[2], npm[0], npm[1], npm[2], 4, 100,
                                    *[ip(a) for a in out])
     assert st == -1 and "num_list is too small" in lib.last_error()
+
+
+def test_state_handle_reports_errors_without_a_device(built_lib):
+    """Without a GPU, rs_create fails with a status and a message instead of
+    crashing, and rs_destroy accepts a null handle."""
+    import ctypes as C
+    import pytest
+    import torch
+    from rspacedist_b200 import lib
+    if torch.cuda.is_available():
+        pytest.skip("needs a machine without a CUDA device")
+    L = lib.load()
+    h = C.c_void_p()
+    rc = L.rs_create(C.byref(h), 32, 16, 16, 16, 4, 0.3, 0.3, 0.3, 4, None)
+    assert rc != 0 and not h.value
+    assert lib.last_error()
+    assert L.rs_create(C.byref(h), 16, 16, 16, 16, 4, 0.3, 0.3, 0.3, 4, None) != 0
+    assert "precision" in lib.last_error()
+    assert L.rs_destroy(None) == 0

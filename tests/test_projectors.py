@@ -97,6 +97,21 @@ def test_channel_table_and_coefficients(built_lib):
     assert np.all(c[[3, 4, 5], 0] == 0.0)  # j_l(0) = 0 for l > 0
 
 
+def test_channel_table_of_the_nc_carbon_dataset(built_lib):
+    """The 4-projector case of pseudocalc_07 (s, p): columns 1, 3, 3, 3."""
+    from rspacedist_b200 import projectors as PR, system as S
+    col, ym = PR.channel_table(S.load_dataset("c_ncps"))
+    assert col.tolist() == [1, 3, 3, 3]
+    assert ym.tolist() == [1, 2, 3, 4]
+
+
+def test_dg_weights_higher_orders_match_the_library(oracle, built_lib):
+    from rspacedist_b200 import projectors as PR
+    for nfdg in (5, 6):
+        for npm in (1, 2, 3):
+            assert np.array_equal(oracle.dg_weights(nfdg, npm), PR.double_grid_weights(nfdg, npm))
+
+
 def _tables_case(cell, oracle, npmesh):
     from rspacedist_b200 import projectors as PR
     ds = cell.ds
