@@ -41,17 +41,29 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def make_cell():
+def make_cell(list_builder=None):
     from rspacedist_b200 import system as S
     ds = S.load_dataset("si_paw")
     pos = S.diamond_positions(NCELL, A_SI, SIGMA, SEED)
-    return S.make_cell(NCELL * A_SI, GRID, pos, ds)
+    return S.make_cell(NCELL * A_SI, GRID, pos, ds, list_builder=list_builder)
 
 
-# DRAM bytes (read + write) per band of one k_stencil_f32_zmarch launch on the
-# Si512 grid, from ncu (dram__bytes.sum.per_second x gpu__time_duration.sum of a
-# 200-band launch: 3.546 GB); the algorithmic figure is 16.8 MB per band.
-STENCIL_TRAFFIC_PER_BAND = 3.546e9 / 200
+def oracle_lists(atoms, rcut, nmax, h, npmax, nfdg, num_list):
+    """The list vectors of pseudocalc_01b from the CPU oracle (the reference
+    arm builds its cell with these, so it never loads the CUDA library)."""
+    from oracle import oracle as O
+    st, d = O.sphere_lists(atoms, rcut, nmax, h, npmax, nfdg, num_list)
+    if st != 0:
+        raise RuntimeError(f"oracle sphere_lists status {st}")
+    return (d["natx"], d["naty"], d["natz"], d["natinf"], d["lst"], d["lstx"], d["lsty"],
+            d["lstz"])
+
+
+# DRAM bytes (read + write) of one k_stencil_f32_zmarch launch on the Si512
+# grid per band: ncu dram__bytes_read.sum + dram__bytes_write.sum of a
+# 200-band launch, profiles/stencil_f32_zmarch_si512.md (see there for the
+# capture command and the per-launch figures).
+STENCIL_TRAFFIC_PER_BAND = (1905046016 + 1640433920) / 200
 
 
 def algorithmic_bytes(cell, nb, entries, s=4, s_p=4):
@@ -246,30 +258,63 @@ def run_gpu(args):
     st_gbs = st_bytes / (st_ms * 1e-3) / 1e9
     g0.close()
 
-    # end to end through the host-buffer entry point (pinned host psi/hpsi)
-    ne = min(E2E_BANDS, nb)
-    hin = psi[:ne].cpu().pin_memory()
-    hout = torch.empty_like(hin).pin_memory()
+    # the plain FP64 drop-in path on the same sweep (rs_hpsi_f64: FP64 psi,
+    # veff and tables), for an FP64-to-FP64 comparison with the CPU oracle
+    fp64 = None
+    if args.fp64_sweep:
+        psi64 = psi.double()
+        veff64 = veff.double()
+        rp64 = K.nonlocaloperation_01(g, psi64)
+        h64 = torch.empty_like(psi64)
+        for _ in range(args.warmup):
+            K.hpsi(g, veff64, dij, rp64, psi64, out=h64)
+        torch.cuda.synchronize()
+        ef0, ef1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ef0.record(stream)
+        for _ in range(args.steps):
+            K.hpsi(g, veff64, dij, rp64, psi64, out=h64)
+        ef1.record(stream)
+        torch.cuda.synchronize()
+        f_ms = ef0.elapsed_time(ef1) / args.steps
+        b64 = algorithmic_bytes(cell, nb, g.entries, s=8, s_p=8)
+        fp64 = {"ms_per_step": round(f_ms, 3), "gbs": round(b64 / (f_ms * 1e-3) / 1e9, 1),
+                "band_points_per_s": round(nb * cell.N / (f_ms * 1e-3), 1),
+                "algorithmic_bytes_per_step": b64, "entry_point": "rs_hpsi_f64"}
+        del psi64, veff64, rp64, h64
+        torch.cuda.empty_cache()
+
+    step()  # hpsi holds the sweep's output again (the stencil-only run wrote it)
+    # end to end through the host-buffer entry point: every band of the sweep
+    # from pinned host memory and back (rs_hpsi_host_f32), when the host has
+    # room for the two pinned copies
+    ne = nb if host_bytes_available() > 3 * 2 * nb * cell.N * 4 else min(E2E_BANDS, nb)
+    hin = torch.empty((ne, cell.N), dtype=torch.float32, pin_memory=True)
+    hin.copy_(psi[:ne])
+    hout = torch.empty_like(hin, pin_memory=True)
     rp_e = rp[:ne].contiguous()
     for _ in range(2):
-        K.hpsi_host(g, veff, dij, rp_e, hin, hout, chunk=8)
+        K.hpsi_host(g, veff, dij, rp_e, hin, hout, chunk=32)
     torch.cuda.synchronize()
     e0 = time.perf_counter()
     e2e_steps = max(3, min(args.steps, 10))
     for _ in range(e2e_steps):
-        K.hpsi_host(g, veff, dij, rp_e, hin, hout, chunk=8)
+        K.hpsi_host(g, veff, dij, rp_e, hin, hout, chunk=32)
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - e0) / e2e_steps
     e2e_bytes = algorithmic_bytes(cell, ne, g.entries)
     e2e_gbs = e2e_bytes / e2e_s / 1e9
     h2d_bytes, d2h_bytes = int(hin.numel() * 4), int(hout.numel() * 4)
+    e2e_ok = bool(torch.equal(hout[:8].to(dev), hpsi[:8]))
+    del hin, hout, rp_e
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(cell, nb)
+        sample = cpu_sample(cell)
+        cpu = cpu_baseline(cell, sample)
+        parity = check_parity(cell, g, dij, sample)
     scf_out = None
     if rank == 0 and world == 1 and args.scf_iters > 0:
-        del psi, hpsi, rp, hin, hout, rp_e
+        del psi, hpsi, rp
         torch.cuda.empty_cache()
         scf_out = run_scf_leg(cell, args.scf_iters)
     if rank == 0:
@@ -289,9 +334,12 @@ def run_gpu(args):
             "roofline": {"bound": "hbm", "kernel": "k_stencil_f32_zmarch",
                          "achieved": round(st_gbs, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(st_gbs / peak, 4),
-                         "traffic": round(STENCIL_TRAFFIC_PER_BAND * nb),
-                         "traffic_source": "ncu dram__bytes of one 200-band launch, scaled "
-                                           "by bands", "peak_source": peak_kind,
+                         "traffic": (round(STENCIL_TRAFFIC_PER_BAND * nb)
+                                     if STENCIL_TRAFFIC_PER_BAND else None),
+                         "traffic_source": "profiles/stencil_f32_zmarch_si512.md: ncu "
+                                           "dram__bytes_read.sum + dram__bytes_write.sum of "
+                                           "one 200-band launch, scaled by bands",
+                         "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": st_bytes,
                          "ms_per_launch": round(st_ms, 3)},
             "roofline_sweep": {"bound": "hbm",
@@ -302,12 +350,17 @@ def run_gpu(args):
             "e2e": {"value": round(e2e_gbs, 2), "unit": "GB/s",
                     "h2d_bytes_per_step": h2d_bytes,
                     "d2h_bytes_per_step": d2h_bytes,
-                    "bands": ne, "entry_point": "rs_hpsi_host_f32"},
+                    "bands": ne, "entry_point": "rs_hpsi_host_f32",
+                    "equals_device_sweep": e2e_ok},
             "gpu_launches": 3 * args.steps,
             "clocks": clk.summary(),
         }
         if cpu:
             out["cpu_baseline"] = cpu
+        if parity:
+            out["parity"] = parity
+        if fp64:
+            out["fp64_sweep"] = fp64
         if scf_out:
             out["scf"] = scf_out
         print(json.dumps(out), flush=True)
@@ -357,59 +410,120 @@ def run_scf_leg(cell, iters):
     }
 
 
-def cpu_baseline(cell, nb_full, nthreads=None, nbands=CPU_SAMPLE_BANDS):
-    """Times the oracle's threaded FP64 H*psi on a few bands of the same cell;
-    reports the sweep-equivalent GB/s (FP32 algorithmic bytes of the full
-    1100-band sweep over the extrapolated sweep time)."""
+def host_bytes_available() -> int:
+    """MemAvailable of this host in bytes (0 when unknown)."""
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def cpu_sample(cell, nthreads=None, nbands=CPU_SAMPLE_BANDS):
+    """Inputs of one bounded sample of the sweep on the host cores:
+    `nbands` seeded FP64 bands of the Si512 cell, their stored <p|psi>
+    (computed before any clock starts, as the GPU sweep also takes them as
+    input) and the oracle's system; run_cpu_sample times it."""
     from oracle import oracle as O
+    from rspacedist_b200 import system as S
     nthreads = nthreads or os.cpu_count()
     if nbands is None:
         nbands = max(4, min(64, nthreads))
     geo = dict(natom=cell.natom, nprjmx=cell.nprjmx, num_list=cell.num_list, nprj=cell.nprj,
                natinf=cell.natinf, lst=cell.lst, v=cell.vnlocp.ravel())
-    from rspacedist_b200 import system as S
     veff = S.smooth_veff(cell, 1)
     sysk = O.make_sys(geo, cell.shape, 4, cell.h, veff, cell.dij, cell.sss)
     psi = np.random.default_rng(0).standard_normal((nbands, cell.N)) * 0.1
-    rp = np.zeros((nbands, cell.natom, cell.nprjmx))
+    rp = O.nl_dot(geo, psi, cell.N).reshape(nbands, cell.natom, cell.nprjmx)
     O.hpsi_fast(sysk, psi[:1], rp[:1], 1)
+    sample = {"nbands": nbands, "threads": nthreads, "psi": psi, "rp": rp, "veff": veff,
+              "sys": sysk}
+    run_cpu_sample(sample)
+    return sample
+
+
+def run_cpu_sample(sample):
+    """The oracle's FP64 H psi (kukan's loops, bands spread over the host
+    threads) of the sample; its wall time goes into sample['seconds']."""
+    from oracle import oracle as O
     t0 = time.perf_counter()
-    O.hpsi_fast(sysk, psi, rp, nthreads)
-    dt = time.perf_counter() - t0
-    sweep_s = dt / nbands * nb_full
+    sample["hpsi"] = O.hpsi_fast(sample["sys"], sample["psi"], sample["rp"], sample["threads"])
+    sample["seconds"] = time.perf_counter() - t0
+    return sample["seconds"]
+
+
+def cpu_baseline(cell, sample):
+    """GB/s of the oracle sample: the algorithmic bytes of an H psi call on
+    the sample's bands (the same formula as the GPU value) over its time."""
     entries = int(sum(int(n) for n in cell.natinf))
-    byts = algorithmic_bytes(cell, nb_full, entries)
-    return {"value": round(byts / sweep_s / 1e9, 3), "unit": "GB/s", "cores": nthreads,
-            "kind": "port",
-            "sample": f"{nbands} of {nb_full} bands of the Si512 sweep (FP64 oracle H*psi, "
-                      f"{dt:.1f} s), extrapolated to the full sweep",
-            "sweep_seconds": round(sweep_s, 2)}
+    byts = algorithmic_bytes(cell, sample["nbands"], entries)
+    return {"value": round(byts / sample["seconds"] / 1e9, 3), "unit": "GB/s",
+            "cores": sample["threads"], "kind": "port",
+            "sample": f"{sample['nbands']} of {NB} bands of the Si512 sweep (FP64 oracle H*psi "
+                      f"with stored <p|psi>, {sample['seconds']:.2f} s on "
+                      f"{sample['threads']} threads)",
+            "band_points_per_s": round(sample["nbands"] * cell.N / sample["seconds"], 1)}
+
+
+def check_parity(cell, g, dij, sample):
+    """The GPU H psi of the CPU sample's bands against the oracle's output:
+    <p|psi> and H psi on the FP64 path (bit for bit), H psi on the FP32 path
+    (largest difference relative to max |H psi|)."""
+    import torch
+    from rspacedist_b200 import kukan as K
+    dev = torch.device("cuda")
+    psi64 = torch.tensor(sample["psi"], device=dev)
+    rp_ref = sample["rp"]
+    rp_gpu = K.nonlocaloperation_01(g, psi64).cpu().numpy()
+    rp_t = torch.tensor(rp_ref, device=dev)
+    h64 = K.hpsi(g, torch.tensor(sample["veff"], device=dev), dij, rp_t, psi64).cpu().numpy()
+    h32 = K.hpsi(g, torch.tensor(sample["veff"], dtype=torch.float32, device=dev), dij, rp_t,
+                 psi64.float()).cpu().numpy()
+    ref = sample["hpsi"]
+    scale = float(np.abs(ref).max())
+    return {"bands": sample["nbands"], "against": "CPU oracle (FP64 restatement of "
+            "kslaplacian_r + nonlocaloperation_r_01/_02) on the sampled bands",
+            "nl_dot_f64_bitexact": bool(np.array_equal(rp_gpu, rp_ref)),
+            "hpsi_f64_bitexact": bool(np.array_equal(h64, ref)),
+            "max_abs_err_f64": float(np.abs(h64 - ref).max()),
+            "max_rel_err_f32": float(np.abs(h32 - ref).max() / scale)}
 
 
 def run_reference(args):
+    """The CPU arm: every step is one bounded sample of the Si512 sweep run by
+    the oracle on all host threads (set-up, lists included, by the oracle:
+    the CUDA library is never loaded).  ms_per_step is the sample's measured
+    time and value its algorithmic bytes over that time."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cell = make_cell()
-    vals = []
-    for _ in range(min(args.warmup, 1)):
-        cpu_baseline(cell, NB)
-    for _ in range(args.steps):
-        vals.append(cpu_baseline(cell, NB))
-    v = statistics.mean(x["value"] for x in vals)
-    sweep_s = statistics.mean(x["sweep_seconds"] for x in vals)
-    cores = vals[0]["cores"]
+    cell = make_cell(list_builder=oracle_lists)
+    sample = cpu_sample(cell)
+    for _ in range(args.warmup):
+        run_cpu_sample(sample)
+    secs = [run_cpu_sample(sample) for _ in range(args.steps)]
+    nbands, cores = sample["nbands"], sample["threads"]
+    entries = int(sum(int(n) for n in cell.natinf))
+    byts = algorithmic_bytes(cell, nbands, entries)
+    v = byts * len(secs) / sum(secs) / 1e9
     print(json.dumps({
         "impl": "reference",
         "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi); SCF time per iteration in 'scf'",
         "value": round(v, 3), "unit": "GB/s", "n_gpus": 0, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(sweep_s * 1e3, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded Si512 geometry)",
+        "warmup": args.warmup, "ms_per_step": round(statistics.mean(secs) * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Si512 geometry, random psi, synthetic smooth veff)",
         "config": {"workload": "Si512 H*psi sweep: 128^3 grid, 1100 bands, 512 Si atoms x 12 "
-                               "projectors; CPU oracle (FP64 restatement of kukan's loops)"},
+                               "projectors; each step a sample of "
+                               f"{nbands} bands on the CPU oracle (FP64 restatement of "
+                               "kukan's loops)", "bands_per_step": nbands},
+        "band_points_per_s": round(nbands * cell.N * len(secs) / sum(secs), 1),
         "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": cores, "kind": "port",
-                         "sample": vals[0]["sample"]},
+                         "sample": f"{nbands} of {NB} bands per step (FP64 oracle H*psi with "
+                                   "stored <p|psi>)"},
         "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -648,6 +762,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-fp64-sweep", dest="fp64_sweep", action="store_false",
+                    help="skip the plain FP64 sweep")
     ap.add_argument("--bands", type=int, default=NB,
                     help="bands per sweep (default 1100; smaller values for profiling only)")
     ap.add_argument("--scf-iters", type=int, default=3,

@@ -335,10 +335,11 @@ int rs_hartree_cg_f32(int nx, int ny, int nz, int nfh, double xmax, double ymax,
  * not be taken).  Same arguments, results and iterates as rs_hartree_cg, but
  * the work vectors live in a fixed array inside the library (about 10.5 MB
  * per GPU, held until exit), so grids are limited to 262144 points (64^3);
- * larger grids return RS_EINVAL.  The first call on a device looks up the
- * array's device address, so make it before any stream capture.  Calls that
- * overlap on one GPU share the array and race.  This entry point has no
- * counterpart in the reference. */
+ * larger grids return RS_EINVAL.  Every call looks up the array's device
+ * address in the current context and runs its iterations as plain kernel
+ * launches (no CUDA graph is instantiated on any stream).  Calls that overlap
+ * on one GPU share the array and race.  This entry point has no counterpart
+ * in the reference. */
 int rs_hartree_cg_noalloc(int nx, int ny, int nz, int nfh, double xmax, double ymax,
                           double zmax, double epsvh, int ncgmin, int ncgmax, int ncgres,
                           const double* rho, double* vh, int* iters, double* dp, void* stream);

@@ -874,10 +874,12 @@ int launch_hartree_ap_f32(int nx, int ny, int nz, const double* cx, const double
 // work32: nullptr for the FP64 solve; 4 N floats for the mixed solve (used
 // when nfh and nx are even, which its paired FP32 stencil needs; other grids
 // run the FP64 iteration)
+// allow_graph: false keeps every batch as plain launches on any stream (no
+// graph is captured or instantiated)
 int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double zmax,
                double epsvh, int ncgmin, int ncgmax, int ncgres, const double* rho, double* vh,
                double* work, int* iters, double* dp_out, cudaStream_t st,
-               float* work32) {
+               float* work32, bool allow_graph) {
   const long N = (long)nx * ny * nz;
   const long nblk = tree_chunks(N);
   double* b = work;
@@ -1012,7 +1014,7 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
     }
   };
   cudaGraphExec_t exec = nullptr;
-  if (st != nullptr) {
+  if (st != nullptr && allow_graph) {
     cudaGraph_t gph = nullptr;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
       batch();
@@ -1168,7 +1170,7 @@ extern "C" int rs_hartree_cg_f32(int nx, int ny, int nz, int nfh, double xmax, d
   RS_CUDA(cudaMallocAsync((void**)&work, bytes, st));
   float* work32 = (float*)(((uintptr_t)work + bytes64 + 15) & ~(uintptr_t)15);
   int rc = rs::hartree_cg(nx, ny, nz, nfh, xmax, ymax, zmax, epsvh, ncgmin, ncgmax, ncgres, rho,
-                          vh, work, iters, dp, st, work32);
+                          vh, work, iters, dp, st, work32, true);
   cudaFreeAsync(work, st);
   return rc;
 }
@@ -1189,7 +1191,7 @@ extern "C" int rs_hartree_cg(int nx, int ny, int nz, int nfh, double xmax, doubl
   double* work = nullptr;
   RS_CUDA(cudaMallocAsync((void**)&work, bytes, st));
   int rc = rs::hartree_cg(nx, ny, nz, nfh, xmax, ymax, zmax, epsvh, ncgmin, ncgmax, ncgres, rho,
-                          vh, work, iters, dp, st, nullptr);
+                          vh, work, iters, dp, st, nullptr, true);
   cudaFreeAsync(work, st);
   if (rc == RS_OK && iters && *iters >= ncgmax && dp && *dp > epsvh) {
     rs::set_error("rs_hartree_cg: ncgmax reached");

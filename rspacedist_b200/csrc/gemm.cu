@@ -11,7 +11,8 @@
 // the canonical tcgen05 layouts; a warp-specialised pipeline (bulk-copy
 // producer, MMA issuer, drain warps) streams them through shared memory.
 // Gram products split K into chunks whose partial tiles are summed in FP64
-// in a fixed order.  FP64 operands use tiled FP64 kernels (CUDA cores).
+// in a fixed order.  FP64 operands (the plain FP64 drop-in path) go to cuBLAS
+// DGEMM.
 #include <cublas_v2.h>
 #include <math.h>
 #include <stdint.h>

@@ -156,6 +156,12 @@ extern "C" int rs_geom_destroy(rs_geom* g) {
                   g->d_cov_off, g->d_nz_off, g->d_nz_pt, g->d_nz_v32, g->d_nz_v64};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (g->host_buf) cudaFree(g->host_buf);
+  for (int i = 0; i < 2; ++i) {
+    if (g->host_cs[i]) cudaStreamDestroy(g->host_cs[i]);
+    if (g->host_ev_done[i]) cudaEventDestroy(g->host_ev_done[i]);
+  }
+  if (g->host_ev_start) cudaEventDestroy(g->host_ev_start);
   delete g;
   return RS_OK;
 }

@@ -10,15 +10,14 @@
 // library reserves the array (about 10.5 MB) until the process exits, so it is
 // sized for dense grids of up to 64^3 points (the Hartree grid of a 32^3
 // coarse cell with nmesh=2) and larger grids are rejected.
-#include <mutex>
-
 #include "reduce.cuh"
 #include "rs_common.cuh"
 
 namespace rs {
 int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double zmax,
                double epsvh, int ncgmin, int ncgmax, int ncgres, const double* rho, double* vh,
-               double* work, int* iters, double* dp_out, cudaStream_t st, float* work32);
+               double* work, int* iters, double* dp_out, cudaStream_t st, float* work32,
+               bool allow_graph);
 }
 
 namespace {
@@ -29,41 +28,30 @@ constexpr long kNoAllocMaxPoints = 64L * 64L * 64L;
 constexpr long kNoAllocWords = 5 * kNoAllocMaxPoints +
                                (kNoAllocMaxPoints + rs::kTreeChunk - 1) / rs::kTreeChunk + 1 +
                                16;
-constexpr int kMaxDevices = 64;
-
 static __device__ __align__(256) double g_hartree_scratch[kNoAllocWords];
 
-std::mutex g_mu;
-double* g_dev_ptr[kMaxDevices] = {};
-
-// Device address of the array on the current device.  The first call on a
-// device looks it up (host code cannot use the symbol's name as a device
-// address) and caches it.
+// Device address of the array in the current device's context.  Host code
+// cannot use the symbol's name as a device address, so it is looked up on
+// every call (a cheap query next to a CG solve); nothing is cached, which
+// keeps the address right after a context is torn down and created again.
 int scratch_address(double** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return rs::cuda_status(e, "rs_hartree_cg_noalloc: cudaGetDevice");
-  if (dev < 0 || dev >= kMaxDevices)
-    return rs::fail(RS_EINVAL, "rs_hartree_cg_noalloc: device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_dev_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_hartree_scratch);
-    if (e != cudaSuccess)
-      return rs::cuda_status(e, "rs_hartree_cg_noalloc: cudaGetSymbolAddress");
-    g_dev_ptr[dev] = static_cast<double*>(p);
-  }
-  *out = g_dev_ptr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_hartree_scratch);
+  if (e != cudaSuccess) return rs::cuda_status(e, "rs_hartree_cg_noalloc: cudaGetSymbolAddress");
+  *out = static_cast<double*>(p);
   return RS_OK;
 }
 
 }  // namespace
 
 // Same arguments and results as rs_hartree_cg.  No device memory is
-// allocated or freed.  Every word of the array is written before it is read
-// within a call, so nothing needs clearing between calls; calls that
-// overlap on the GPU (other streams, other host threads, same device) share
-// the one array and race.
+// allocated or freed, and the iteration batches run as plain kernel launches
+// on every stream (rs_hartree_cg instantiates a CUDA graph of them on a
+// non-default stream, which this entry point never does).  Every word of the
+// array is written before it is read within a call (the CG scalars are
+// cleared at the start of each solve), so nothing needs clearing between
+// calls; calls that overlap on the GPU (other streams, other host threads,
+// same device) share the one array and race.
 extern "C" int rs_hartree_cg_noalloc(int nx, int ny, int nz, int nfh, double xmax, double ymax,
                                      double zmax, double epsvh, int ncgmin, int ncgmax,
                                      int ncgres, const double* rho, double* vh, int* iters,
@@ -80,6 +68,11 @@ extern "C" int rs_hartree_cg_noalloc(int nx, int ny, int nz, int nfh, double xma
   double* work = nullptr;
   int rc = scratch_address(&work);
   if (rc != RS_OK) return rc;
-  return rs::hartree_cg(nx, ny, nz, nfh, xmax, ymax, zmax, epsvh, ncgmin, ncgmax, ncgres, rho,
-                        vh, work, iters, dp, rs::as_stream(stream), nullptr);
+  // plain launches on every stream: no CUDA graph is captured or instantiated
+  rc = rs::hartree_cg(nx, ny, nz, nfh, xmax, ymax, zmax, epsvh, ncgmin, ncgmax, ncgres, rho, vh,
+                      work, iters, dp, rs::as_stream(stream), nullptr, false);
+  // the same diagnostic as rs_hartree_cg when the iteration limit stops the solve
+  if (rc == RS_OK && iters && *iters >= ncgmax && dp && *dp > epsvh)
+    rs::set_error("rs_hartree_cg_noalloc: ncgmax reached");
+  return rc;
 }

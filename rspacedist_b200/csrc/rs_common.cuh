@@ -71,6 +71,15 @@ struct rs_geom {
   double* d_nz_v64; // [nnz*nprjmx]
   // Laplacian coefficients, computed as acfd(m)/dx/dx*(-0.5d0)
   double cx[9], cy[9], cz[9];
+  // staging of the host-buffer H psi (rs_hpsi_host_f32): two copy streams,
+  // their completion events and one event on the caller's stream, created by
+  // the first call; the device chunk buffers, grown on demand.  Released by
+  // rs_geom_destroy.
+  cudaStream_t host_cs[2];
+  cudaEvent_t host_ev_done[2];
+  cudaEvent_t host_ev_start;
+  float* host_buf;
+  size_t host_buf_bytes;
 };
 
 namespace rs {

@@ -145,11 +145,15 @@ class Cell:
         return np.full(self.natom, self.nprjmx, np.int32)
 
 
-def make_cell(A, n, atoms, ds, with_s=True, filtered: bool = False, npmesh: int = 2) -> Cell:
+def make_cell(A, n, atoms, ds, with_s=True, filtered: bool = False, npmesh: int = 2,
+              list_builder=None) -> Cell:
     """A: cell edge(s) in bohr, n: grid points per axis (even), atoms (natom,3).
     filtered: the projector tables of pseudocalc_07 (Fourier-filtered radial
     functions on the npmesh double grid, built on the GPU by
-    rs_projector_tables) in place of the directly sampled ones."""
+    rs_projector_tables) in place of the directly sampled ones.
+    list_builder: a function with the arguments and results of
+    rs_sphere_lists (see sphere_lists_library) that builds the list vectors;
+    None uses the library's."""
     A = np.broadcast_to(np.asarray(A, float), (3,))
     n = np.broadcast_to(np.asarray(n, int), (3,))
     if np.any(n % 2):
@@ -159,7 +163,7 @@ def make_cell(A, n, atoms, ds, with_s=True, filtered: bool = False, npmesh: int 
     h = tuple(xmax[i] / nmax[i] for i in range(3))
     cell = Cell(shape=tuple(int(v) for v in n), h=h, xmax=xmax, nmax=nmax,
                 atoms=np.asarray(atoms, float).reshape(-1, 3), ds=ds)
-    build_lists(cell)
+    build_lists(cell, list_builder)
     build_projectors(cell, with_s=with_s)
     if filtered:
         from .projectors import projector_tables
@@ -185,26 +189,34 @@ def list_dims(cell: Cell):
     return tuple(npm), int(np.prod(nl))
 
 
-def build_lists(cell: Cell):
-    npmax, num_list = list_dims(cell)
-    A = cell.natom
-    at = np.ascontiguousarray(cell.atoms, dtype=np.float64)
+def sphere_lists_library(atoms, rcut, nmax, h, npmax, nfdg, num_list):
+    """List vectors of pseudocalc_01b by the library (rs_sphere_lists):
+    returns natx, naty, natz, natinf, lst, lstx, lsty, lstz."""
+    A = len(atoms)
+    at = np.ascontiguousarray(atoms, dtype=np.float64)
     ax, ay, az = (np.ascontiguousarray(at[:, k]) for k in range(3))
-    rc = np.full(A, cell.ds["rcut"] * PSCTOFF)
+    rc = np.full(A, rcut)
     nat = [np.zeros(A, np.int32) for _ in range(3)]
     natinf = np.zeros(A, np.int32)
     lst = np.zeros(A * num_list, np.int32)
     lx, ly, lz = (np.zeros(A * num_list, np.int32) for _ in range(3))
     dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
     ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
-    _lib.call("rs_sphere_lists", A, dp(ax), dp(ay), dp(az), dp(rc), cell.nmax[0], cell.nmax[1],
-              cell.nmax[2], cell.h[0], cell.h[1], cell.h[2], npmax[0], npmax[1], npmax[2], NFDG,
-              num_list, ip(nat[0]), ip(nat[1]), ip(nat[2]), ip(natinf), ip(lst), ip(lx), ip(ly),
-              ip(lz))
+    _lib.call("rs_sphere_lists", A, dp(ax), dp(ay), dp(az), dp(rc), nmax[0], nmax[1], nmax[2],
+              h[0], h[1], h[2], npmax[0], npmax[1], npmax[2], nfdg, num_list, ip(nat[0]),
+              ip(nat[1]), ip(nat[2]), ip(natinf), ip(lst), ip(lx), ip(ly), ip(lz))
+    return nat[0], nat[1], nat[2], natinf, lst, lx, ly, lz
+
+
+def build_lists(cell: Cell, list_builder=None):
+    npmax, num_list = list_dims(cell)
+    fn = list_builder or sphere_lists_library
+    nx_, ny_, nz_, natinf, lst, lx, ly, lz = fn(cell.atoms, cell.ds["rcut"] * PSCTOFF, cell.nmax,
+                                                 cell.h, npmax, NFDG, num_list)
     cell.npmax, cell.num_list = npmax, num_list
     cell.natinf, cell.lst = natinf, lst
     cell.lstxyz = (lx, ly, lz)
-    cell.natxyz = tuple(nat)
+    cell.natxyz = (nx_, ny_, nz_)
 
 
 def build_projectors(cell: Cell, with_s=True):

@@ -131,7 +131,7 @@ def test_rayleighritz(system, oracle):
     np.testing.assert_allclose(got[:4].T @ got[:4], P_ref, atol=1e-9 * np.abs(P_ref).max())
     b32 = make_bands(sy, torch.float32)
     K.rayleighritz(b32, T(sy["veff"], torch.float32), T(sy["cell"].dij), 1)
-    np.testing.assert_allclose(b32.sval, sval, atol=2e-5)
+    np.testing.assert_allclose(b32.sval, sval, atol=1e-5)
 
 
 def test_scf_diag_fp32_converges_like_fp64(system, oracle):

@@ -1,0 +1,77 @@
+"""Parity at the size of the Si64 PAW workload: the 2x2x2 diamond supercell
+of silicon (a = 20.52 bohr, 64 atoms displaced by sigma = 0.05 bohr from
+seed 1), PAW Si projectors (12 per atom), 64^3 grid, 160 bands.
+
+* <p|psi> and H psi of all 160 bands on the FP64 path equal the CPU oracle
+  bit for bit (nonlocaloperation_r_01/_02 and kslaplacian_r);
+* the FP32 path's H psi is within 1e-5 of max |H psi| of the oracle's;
+* Rayleigh-Ritz eigenvalues: FP64 within 1e-10 Ha of the oracle's, FP32
+  within 1e-5 Ha of the oracle's on the same (FP32-rounded) bands."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+M = 160
+
+
+def T(a, dtype=torch.float64):
+    return torch.tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+def geo_dict(cell):
+    return dict(natom=cell.natom, nprjmx=cell.nprjmx, num_list=cell.num_list, nprj=cell.nprj,
+                natinf=cell.natinf, lst=cell.lst, v=cell.vnlocp.ravel())
+
+
+@pytest.fixture(scope="module")
+def si64(built_lib, oracle, cuda):
+    from rspacedist_b200 import kukan as K, system as S
+    import test_gpu_bands as TB
+    ds = S.load_dataset("si_paw")
+    cell = S.make_cell(20.52, 64, S.diamond_positions(2, 10.26, 0.05, 1), ds)
+    g = K.Geometry(cell)
+    veff = S.smooth_veff(cell, 1)
+    sysk = oracle.make_sys(geo_dict(cell), cell.shape, 4, cell.h, veff, cell.dij, cell.sss)
+    psi = TB.smooth_bands(cell.shape, M, 5)
+    return dict(cell=cell, g=g, veff=veff, sysk=sysk, psi=psi)
+
+
+def test_si64_nl_dot_and_hpsi(si64, oracle):
+    from rspacedist_b200 import kukan as K
+    cell, g, psi = si64["cell"], si64["g"], si64["psi"]
+    rp = oracle.nl_dot(geo_dict(cell), psi, cell.N).reshape(M, cell.natom, cell.nprjmx)
+    rp_gpu = K.nonlocaloperation_01(g, T(psi)).cpu().numpy()
+    assert np.array_equal(rp_gpu, rp)
+    ref = oracle.hpsi(si64["sysk"], psi, rp)
+    got = K.hpsi(g, T(si64["veff"]), T(cell.dij), T(rp), T(psi)).cpu().numpy()
+    assert np.array_equal(got, ref)
+    rp32 = K.nonlocaloperation_01(g, T(psi, torch.float32)).cpu().numpy()
+    np.testing.assert_allclose(rp32, rp, atol=1e-6 * np.abs(rp).max())
+    h32 = K.hpsi(g, T(si64["veff"], torch.float32), T(cell.dij), T(rp),
+                 T(psi, torch.float32)).cpu().numpy()
+    assert np.abs(h32 - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+def test_si64_rayleighritz(si64, oracle):
+    from rspacedist_b200 import kukan as K
+    cell, g, sysk = si64["cell"], si64["g"], si64["sysk"]
+    # an S-orthonormal start from the oracle, rounded to FP32 so that both
+    # paths see the same bands
+    psi = si64["psi"].astype(np.float32).astype(np.float64)
+    rp = oracle.nl_dot(geo_dict(cell), psi, cell.N)
+    sp = oracle.spsi(sysk, psi, rp)
+    psi, sp, rp = oracle.ortho(sysk, M, psi, sp, rp, 0, 1)
+    psi = psi.astype(np.float32).astype(np.float64)
+    rp = oracle.nl_dot(geo_dict(cell), psi, cell.N)
+    sp = oracle.spsi(sysk, psi, rp)
+    st, _, _, _, sval = oracle.rayleighritz(sysk, M, psi, sp, rp)
+    assert st == 0
+    for dtype, tol in ((torch.float64, 1e-10), (torch.float32, 1e-5)):
+        b = K.Bands(g, T(psi, dtype), T(cell.sss))
+        b.spsi.copy_(T(sp, dtype))
+        b.rp.copy_(T(rp).view_as(b.rp))
+        K.rayleighritz(b, T(si64["veff"], dtype), T(cell.dij), 1)
+        err = np.abs(np.asarray(b.sval) - sval).max()
+        assert err <= tol, (str(dtype), err)
