@@ -208,6 +208,13 @@ def run_gpu(args):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    import ctypes as C
+    from rspacedist_b200 import lib as RL
+    chunk = C.c_int(0)
+    RL.call("rs_hpsi_f32_tuning", g.handle, C.byref(chunk))
+    nl_chunk = chunk.value
+    nchunks = 1 if nl_chunk <= 0 else -(-nb // nl_chunk)
+    launches_per_step = 1 + 2 * nchunks  # k_tcoef_f32, then stencil + nonlocal per chunk
     if world > 1:
         dist.barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -313,13 +320,13 @@ def run_gpu(args):
         cpu = cpu_baseline(cell, sample)
         parity = check_parity(cell, g, dij, sample)
     scf_out = None
-    if rank == 0 and world == 1 and args.scf_iters > 0:
+    if rank == 0 and world == 1 and args.scf_loops > 0:
         del psi, hpsi, rp
         torch.cuda.empty_cache()
-        scf_out = run_scf_leg(cell, args.scf_iters)
+        scf_out = run_scf_leg(cell, args.scf_loops)
     if rank == 0:
         out = {
-            "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi); SCF time per iteration in 'scf'",
+            "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi); SCF time to eps in 'scf'",
             "value": round(value, 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -329,6 +336,7 @@ def run_gpu(args):
                        "grid": [GRID] * 3, "bands": nb, "atoms": cell.natom,
                        "projectors": cell.nprjmx, "inverse_entries": g.entries,
                        "l2": "inputs (9.2 GB psi) larger than L2; no flush",
+                       "nl_band_chunk": nl_chunk,
                        "parallelism": f"bands replicated per GPU x{world}"},
             "band_points_per_s": round(nb * cell.N * world / (ms * 1e-3), 1),
             "roofline": {"bound": "hbm", "kernel": "k_stencil_f32_zmarch",
@@ -343,7 +351,8 @@ def run_gpu(args):
                          "algorithmic_bytes_per_launch": st_bytes,
                          "ms_per_launch": round(st_ms, 3)},
             "roofline_sweep": {"bound": "hbm",
-                               "kernels": "k_stencil_f32_zmarch + k_tcoef_f32 + k_nl_rmw_f32",
+                               "kernels": "k_tcoef_f32, then k_stencil_f32_zmarch and "
+                                          "k_nl_rmw_f32_part per band chunk",
                                "achieved": round(sweep_gbs, 1), "peak": peak, "unit": "GB/s",
                                "frac": round(sweep_gbs / peak, 4),
                                "algorithmic_bytes_per_step": nbytes},
@@ -352,7 +361,7 @@ def run_gpu(args):
                     "d2h_bytes_per_step": d2h_bytes,
                     "bands": ne, "entry_point": "rs_hpsi_host_f32",
                     "equals_device_sweep": e2e_ok},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(),
         }
         if cpu:
@@ -368,46 +377,112 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
-def run_scf_leg(cell, iters):
-    """The SCF half of the metric on the same Si512 cell: `iters` SCF
-    iterations (Broyden mixing, potentials, scf_diag with RR + DIIS, density,
-    charge difference) on the mixed path (FP32 bands) and on the plain FP64
-    path, from the same start, timed per iteration on the wall clock with the
-    device synchronised.  The local potential and start charge are model
-    fields (a Gaussian well / valence Gaussian per atom); 1024 of 1100 bands
-    are filled by Fermi-Dirac occupation (kT = 3e-3 Ha)."""
+def run_scf_leg(cell, looplimit, eps_scf=1e-6):
+    """The SCF half of the metric on the same Si512 cell: kukan's SCF
+    (local pseudopotential of the dataset, setup_initialwave start, Broyden
+    mixing eta 0.1, RR + CG for the first two iterations then RR + DIIS,
+    Hartree CG, PZ LDA, Fermi-Dirac occupations for 2048 electrons in 1100
+    bands) to diff_charge < eps_scf on the mixed path (FP32 bands) and on the
+    plain FP64 path, each timed on the wall clock with the device
+    synchronised, then the total energies of output_energy."""
     import torch
     from rspacedist_b200 import lib, scf
-    prm = lib.solver_prm(ncgscf=0)
+    prm = lib.solver_prm(ncgscf=2)
     res = {}
     for name, dt in (("mixed", torch.float32), ("fp64", torch.float64)):
-        r = scf.run_scf(cell, NB, 1024, dtype=dt, prm=prm, looplimit=iters, eta=0.1,
-                        profile=True)
-        res[name] = r
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = scf.run_scf(cell, NB, 1024, dtype=dt, prm=prm, looplimit=looplimit, eta=0.1,
+                        eps_scf=eps_scf, profile=True)
+        total = time.perf_counter() - t0
+        r.bands = r.rho_out = None
+        res[name] = (r, total)
         torch.cuda.empty_cache()
-        log(f"[scf] {name}: {[round(s, 3) for s in r.seconds_per_iter]} s per iteration")
-    a, b = res["mixed"], res["fp64"]
-    steady = lambda r: statistics.mean(r.seconds_per_iter[1:] or r.seconds_per_iter)
+        log(f"[scf] {name}: converged {r.converged} in {r.iterations} iterations, "
+            f"{r.seconds:.2f} s (+{total - r.seconds:.2f} s set-up); E {r.energy['total']:.8f}")
+    (a, ta), (b, tb) = res["mixed"], res["fp64"]
     nocc = 1024
+    per_it = lambda r: r.seconds / max(1, r.iterations)
     return {
-        "workload": "Si512 model SCF: 128^3 grid, 1100 bands (1024 filled, Fermi-Dirac kT "
-                    "3e-3 Ha), Si PAW projectors with fixed D and S, Gaussian-well local "
-                    "potential, Broyden mixing (eta 0.1, 20 steps), RR + DIIS each iteration, "
-                    "Hartree CG (epsvh 1e-12, at most 800 iterations) on the 256^3 dense grid",
-        "iterations": iters,
-        "mixed_s_per_iter": round(steady(a), 3),
-        "fp64_s_per_iter": round(steady(b), 3),
-        "speedup_mixed_vs_fp64": round(steady(b) / steady(a), 3),
-        "mixed_phase_s": {k: round(v / iters, 3) for k, v in a.phase_seconds.items()},
-        "fp64_phase_s": {k: round(v / iters, 3) for k, v in b.phase_seconds.items()},
-        "diff_charge_mixed": [float(f"{d:.3e}") for d in a.diff],
-        "diff_charge_fp64": [float(f"{d:.3e}") for d in b.diff],
+        "workload": "Si512 SCF: 128^3 grid, 1100 bands (2048 electrons, Fermi-Dirac kT 3e-3 Ha), "
+                    "Si PAW projectors with the dataset's D and S (no one-centre update), the "
+                    "dataset's local pseudopotential (pseudocalc soft + hard parts), "
+                    "setup_initialwave start, Broyden mixing (eta 0.1, 20 steps), RR + CG x2 "
+                    "then RR + DIIS, Hartree CG (epsvh 1e-12) on the 256^3 dense grid",
+        "eps_scf": eps_scf,
+        "converged": {"mixed": a.converged, "fp64": b.converged},
+        "iterations": {"mixed": a.iterations, "fp64": b.iterations},
+        "time_to_eps_s": {"mixed": round(a.seconds, 2), "fp64": round(b.seconds, 2)},
+        "setup_s": {"mixed": round(ta - a.seconds, 2), "fp64": round(tb - b.seconds, 2)},
+        "speedup_time_to_eps_mixed_vs_fp64": round(b.seconds / a.seconds, 3),
+        "s_per_iter": {"mixed": round(per_it(a), 3), "fp64": round(per_it(b), 3)},
+        "etot_ha": {"mixed": a.energy["total"], "fp64": b.energy["total"]},
+        "etot_diff_ha_per_atom": abs(a.energy["total"] - b.energy["total"]) / cell.natom,
+        "free_energy_diff_ha_per_atom": abs(a.energy["free"] - b.energy["free"]) / cell.natom,
+        "energy_terms_fp64": b.energy,
         "max_abs_occupied_eig_diff_ha": float(np.abs(np.sort(a.sval)[:nocc]
                                                      - np.sort(b.sval)[:nocc]).max()),
-        "eband_diff_ha_per_atom": abs(a.eband - b.eband) / cell.natom,
-        "timing": "wall clock per SCF iteration with device synchronisation; the first "
-                  "iteration (pool growth) is left out of the means",
+        "mixed_phase_s": {k: round(v, 3) for k, v in a.phase_seconds.items()},
+        "fp64_phase_s": {k: round(v, 3) for k, v in b.phase_seconds.items()},
+        "diff_charge_mixed": [float(f"{d:.3e}") for d in a.diff],
+        "diff_charge_fp64": [float(f"{d:.3e}") for d in b.diff],
+        "timing": "wall clock of the SCF loop (iteration 1 to the stopping rule) with the "
+                  "device synchronised; set-up (local potential, initial bands, their "
+                  "orthonormalisation and the start density) reported apart",
     }
+
+
+def run_force_check(ncomp=6):
+    """Forces of the Si64 PAW cell (2x2x2 diamond, a = 20.52 bohr, 64^3 grid,
+    160 bands, atoms displaced by sigma = 0.10 bohr from seed 3) by the
+    adjoint pass after a converged FP64 and mixed SCF: against minus the
+    central difference of the SCF free energy over +-1e-3 bohr on `ncomp`
+    atom-axis components drawn from seed 3, and the projector part against
+    force_eig_r (finite-difference band derivatives).  Prints one JSON line."""
+    import torch
+    from rspacedist_b200 import forces, kukan as K, lib, scf, system as S
+    ds = S.load_dataset("si_paw")
+    pos0 = S.diamond_positions(2, A_SI, 0.10, 3)
+    mk = lambda p: S.make_cell(2 * A_SI, 64, p, ds)
+    prm = lib.solver_prm(ncgscf=2)
+    run = lambda c, dt: scf.run_scf(c, 160, 128, dtype=dt, prm=prm, eta=0.1, eps_scf=1e-8,
+                                    looplimit=300)
+    cell = mk(pos0)
+    out = {"force_check": {"cell": "Si64 PAW 64^3, 160 bands, sigma 0.10 seed 3",
+                           "step_bohr": 1e-3}}
+    t = time.perf_counter()
+    r64 = run(cell, torch.float64)
+    f64 = forces.atomic_forces(cell, r64)
+    out["fp64_scf"] = {"converged": r64.converged, "iterations": r64.iterations,
+                       "seconds": round(r64.seconds, 2)}
+    r32 = run(cell, torch.float32)
+    f32 = forces.atomic_forces(cell, r32)
+    out["mixed_scf"] = {"converged": r32.converged, "iterations": r32.iterations,
+                        "seconds": round(r32.seconds, 2)}
+    out["max_abs_force_diff_mixed_vs_fp64"] = float(np.abs(f32["total"] - f64["total"]).max())
+    g = K.Geometry(cell)
+    dij = torch.tensor(cell.dij, dtype=torch.float64, device="cuda")
+    sss = torch.tensor(cell.sss, dtype=torch.float64, device="cuda")
+    fe = K.force_eig(g, dij, sss, r64.bands.psi, torch.tensor(r64.sval, device="cuda"),
+                     torch.tensor(r64.occ, device="cuda")).cpu().numpy()
+    out["max_abs_diff_projector_vs_force_eig"] = float(np.abs(f64["projector"] - fe).max())
+    out["max_abs_force"] = float(np.abs(f64["total"]).max())
+    rng = np.random.default_rng(3)
+    comps = [(int(rng.integers(cell.natom)), int(rng.integers(3))) for _ in range(ncomp)]
+    rows = []
+    for a, ax in comps:
+        es = []
+        for sgn in (1, -1):
+            p = pos0.copy()
+            p[a, ax] += sgn * 1e-3
+            es.append(run(mk(p), torch.float64).energy["free"])
+        fd = -(es[0] - es[1]) / 2e-3
+        rows.append({"atom": a, "axis": ax, "adjoint": float(f64["total"][a, ax]), "fd": fd,
+                     "diff": float(f64["total"][a, ax] - fd)})
+    out["fd_components"] = rows
+    out["max_abs_diff_adjoint_vs_fd"] = max(abs(x["diff"]) for x in rows)
+    out["seconds"] = round(time.perf_counter() - t, 1)
+    print(json.dumps(out), flush=True)
 
 
 def host_bytes_available() -> int:
@@ -511,7 +586,7 @@ def run_reference(args):
     v = byts * len(secs) / sum(secs) / 1e9
     print(json.dumps({
         "impl": "reference",
-        "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi); SCF time per iteration in 'scf'",
+        "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi); SCF time to eps in 'scf'",
         "value": round(v, 3), "unit": "GB/s", "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(statistics.mean(secs) * 1e3, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -766,8 +841,10 @@ def main():
                     help="skip the plain FP64 sweep")
     ap.add_argument("--bands", type=int, default=NB,
                     help="bands per sweep (default 1100; smaller values for profiling only)")
-    ap.add_argument("--scf-iters", type=int, default=3,
-                    help="SCF iterations timed per path on the Si512 cell (0 skips the leg)")
+    ap.add_argument("--scf-loops", "--scf-iters", dest="scf_loops", type=int, default=60,
+                    help="iteration limit of the Si512 SCF run per path (0 skips the leg)")
+    ap.add_argument("--force-check", action="store_true",
+                    help="run the Si64 force check (adjoint vs energy differences) and exit")
     ap.add_argument("--diag-profile", choices=["f32", "f64"],
                     help="run one profiled scf_diag call of the SCF leg and exit")
     ap.add_argument("--gemm-profile", type=int, metavar="POINTS",
@@ -782,7 +859,9 @@ def main():
                     help="time H*psi of CELLS small cells, per-cell calls vs one batched "
                          "launch, and exit")
     args = ap.parse_args()
-    if args.proj_profile:
+    if args.force_check:
+        run_force_check()
+    elif args.proj_profile:
         run_proj_profile(args.proj_profile, 4)
     elif args.batch_profile:
         run_batch_profile(args.batch_profile, 20)

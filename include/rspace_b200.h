@@ -104,6 +104,12 @@ int rs_nonlocal_dot_f32(const rs_geom* g, const float* psi, int nb, double* rp, 
 int rs_nonlocal_apply_f64(const rs_geom* g, const double* mat, const double* rp, int nb,
                           double* out, void* stream);
 
+/* The band-chunk size the FP32 H psi of g chose for running its nonlocal
+ * pass behind the stencil (rs_hpsi_f32 times the candidates on its first
+ * call with at least 64 bands): 0 before that call, -1 for one stencil
+ * launch followed by one pass.  No counterpart in the reference. */
+int rs_hpsi_f32_tuning(const rs_geom* g, int* nl_chunk);
+
 /* Fused H psi = nonlocal(D) + stencil + veff, one pass over psi (the H*psi of
  * kscg8f.F90:147-183 and rayleighritz_hamiltonian_r, rayleigh-ritz8f.F90:493-575).
  * hpsi(dev) is overwritten. */
@@ -408,6 +414,106 @@ int rs_density(rs_state* s, const double* occ, double* rho);
 int rs_download_bands(rs_state* s, void* psi);
 int rs_state_arrays(rs_state* s, void** psi, void** spsi, void** hpsi, double** rp, void** veff);
 int rs_destroy(rs_state* s);
+
+/* ---- local pseudopotential, ion-ion energy, initial bands (nperi = 3) ---- */
+/* Soft local part of pseudocalc_02 case (3) with its real-space images
+ * (pseudocalc8f.F90:1443-1568), summed over the atoms as pseudocalc_03 does
+ * (:1600-1678), on the coarse grid: vsoft (device, N) is overwritten.  Host
+ * inputs: atxyz (x, y, z per atom) and prm (5 per atom: cp1 = the valence
+ * charge, and a, b, c of tools_bisec (tools8f.F90:922-953), and
+ * rcut = radial(nradct)); veta and new_pw{x,y,z} are kukan's Ewald
+ * parameters (read_input_kukan8f.F90:273-276). */
+int rs_vloc_soft(int natom, const double* atxyz, const double* prm, int nx, int ny, int nz,
+                 double dx, double dy, double dz, double xmax, double ymax, double zmax,
+                 double veta, int npwx, int npwy, int npwz, double* vsoft, void* stream);
+
+/* Hard local part of pseudocalc_02 (pseudocalc8f.F90:1245-1290) on the dense
+ * grid (nmesh points per coarse spacing, the list of pseudocalc_01b within
+ * rcut*psctoff, :1035-1144), added to dense (device, 8N for nmesh = 2) atom by
+ * atom as pseudocalc_04 does (:1682-1706).  Host inputs: atxyz, spe (species
+ * index per atom), per species sprm (rcut, rcuts = rcut*psftrad, filpp) and
+ * nqct, coef (nspe x (nqmx+1): the local-part Fourier-Bessel coefficients
+ * coef(0:nqmx, 0) of filterpseudopotentials8f.F90:107-131); npxmax.. are the
+ * coarse list half-widths of tools_listvecdim. */
+int rs_vloc_hard_add(int natom, const double* atxyz, const int* spe, int nspe,
+                     const double* sprm, const int* nqct, int nqmx, const double* coef, int nx,
+                     int ny, int nz, double dx, double dy, double dz, double xmax, double ymax,
+                     double zmax, int nmesh, int npxmax, int npymax, int npzmax,
+                     double psctoff, double eps, int nfiltyp, double* dense, void* stream);
+
+/* Ewald energy of the ions, eneat of totalenergy_space_03 case (3)
+ * (totalenergy8f.F90:520-565), and, when force (host, 3 per atom) is not
+ * NULL, its forces (the ion-ion part of force8f.F90:1900-1950).  Host inputs
+ * atxyz and q (cp1 per atom); energy (host) in Ha.  Returns after the
+ * result is on the host. */
+int rs_ewald(int natom, const double* atxyz, const double* q, double xmax, double ymax,
+             double zmax, double veta, int npwx, int npwy, int npwz, double* energy,
+             double* force, void* stream);
+
+/* kukan's initial bands, setup_initialwave real branch
+ * (setup_initialwave8f.F90:48-130): band l of atom a is exp(-zs_a r) times
+ * 1 (l < natom), x, y, z (next 3 natom) or the five d forms (when
+ * neig > 4 natom), r the minimum-image distance, normalised to
+ * sum psi^2 dV = 1.  zs (host, per atom) = cp1 * zs_pre; psi device
+ * (neig x N). */
+int rs_initial_wave_f64(int natom, const double* atxyz, const double* zs, int neig, int nx,
+                        int ny, int nz, double dx, double dy, double dz, double xmax,
+                        double ymax, double zmax, double* psi, void* stream);
+int rs_initial_wave_f32(int natom, const double* atxyz, const double* zs, int neig, int nx,
+                        int ny, int nz, double dx, double dy, double dz, double xmax,
+                        double ymax, double zmax, float* psi, void* stream);
+
+/* ---- forces by one adjoint pass over the bands --------------------------- */
+/* Local-pseudopotential part of the atomic forces as the exact derivative
+ * of E_loc = dV sum_p rho(p) vloc_coarse(p), vloc_coarse = d2c(c2d(soft) +
+ * hard) built as rs_vloc_soft / rs_vloc_hard_add do: with d2c the adjoint of
+ * c2d (over 8), F_a = dV sum_p rho_soft(p) grad soft_a(p) + dV/8
+ * sum_q rho_dense(q) grad hard_a(q), where rho_dense = c2d(rho) and
+ * rho_soft = d2c(rho_dense) (device, coarse and dense).  The gradients are
+ * those kukan stores as dvlocd*_scw and dvlocd*_hdp (pseudocalc8f.F90:
+ * 1252-1289, 1443-1568), summed as force_01 does (force8f.F90:2016-2109) but
+ * recomputed instead of stored; the reciprocal part runs as a separable
+ * transform of rho_soft.  Arguments as rs_vloc_soft (prm) and
+ * rs_vloc_hard_add (spe .. coef, nmesh .. nfiltyp); force: host, 3 per atom
+ * (Ha/bohr), returned after it is on the host. */
+int rs_force_local(int natom, const double* atxyz, const double* prm, const int* spe, int nspe,
+                   const double* sprm, const int* nqct, int nqmx, const double* coef, int nx,
+                   int ny, int nz, double dx, double dy, double dz, double xmax, double ymax,
+                   double zmax, double veta, int npwx, int npwy, int npwz, int nmesh,
+                   int npxmax, int npymax, int npzmax, double psctoff, double eps,
+                   int nfiltyp, const double* rho_soft, const double* rho_dense, double* force,
+                   void* stream);
+
+/* Projector part of the atomic forces as the exact derivative of the
+ * discrete energy: F_a = 2 sum_l occ_l sum_ij (D_a - sval_l S_a)_ij
+ * <p_i|psi_l> <grad p_j|psi_l> (the quantity force_eig_r forms with
+ * finite-difference band derivatives, force8f.F90:9-195).  The projector
+ * values and gradients are recomputed at every sphere-list point from the
+ * radial tables, nothing per projector is stored: tabs (host, ntab x nr) on
+ * the radial grid i*dr, linearly interpolated and zero from r >= rcut; per
+ * projector j its table prj_tab[j], angular momentum prj_l[j] and real
+ * harmonic prj_form[j] (0: s; 1-3: x, y, z; 4-8: x^2-y^2, -zx, 3z^2-r^2, -yz,
+ * xy, each over r^l, normalised as pseudocalc8f.F90:2962-2970), times
+ * dx dy dz.  Host lists: atxyz (3 per atom), natxyz ([3][natom]), natinf,
+ * lstxyz ([3][natom*num_list] offsets), lst (natom*num_list point indices)
+ * from rs_sphere_lists.  Device: dij, sss ([natom][nprj][nprj], sss NULL for
+ * NC), psi [nb][N], sval, occ [nb].  force: host, 3 per atom (Ha/bohr);
+ * rp: NULL or device [nb][natom][nprj], the recomputed <p|psi>.  Returns
+ * after force is on the host. */
+int rs_force_adjoint_f64(int natom, int nprj, int num_list, const double* atxyz,
+                         const int* natxyz, const int* natinf, const int* lstxyz, const int* lst,
+                         int ntab, int nr, double dr, const double* tabs, const int* prj_tab,
+                         const int* prj_l, const int* prj_form, double rcut, int nx, int ny,
+                         int nz, double dx, double dy, double dz, const double* dij,
+                         const double* sss, const double* psi, const double* sval,
+                         const double* occ, int nb, double* force, double* rp, void* stream);
+int rs_force_adjoint_f32(int natom, int nprj, int num_list, const double* atxyz,
+                         const int* natxyz, const int* natinf, const int* lstxyz, const int* lst,
+                         int ntab, int nr, double dr, const double* tabs, const int* prj_tab,
+                         const int* prj_l, const int* prj_form, double rcut, int nx, int ny,
+                         int nz, double dx, double dy, double dz, const double* dij,
+                         const double* sss, const float* psi, const double* sval,
+                         const double* occ, int nb, double* force, double* rp, void* stream);
 
 /* ---- fixed-tree reductions (shared order with the oracle) --------------- */
 /* out(dev, 1 double) = sum_i a_i b_i in the documented block tree. */

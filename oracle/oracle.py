@@ -419,3 +419,77 @@ def projector_tables(atoms, lists, nmax, h, npmax, nfdg, npmesh, num_list, prj_c
         _d(_f64(wxyz)), _d(v))
     assert st == 0, "orc_projector_tables: out of memory"
     return v
+
+
+# ---- local pseudopotential, Ewald energy, initial bands (rs_oracle_vloc.c) ----
+
+def bisec(z, r, eps=1.0e-12):
+    a, b, c = C.c_double(), C.c_double(), C.c_double()
+    lib().orc_bisec(C.c_double(z), C.c_double(r), C.c_double(eps), C.byref(a), C.byref(b),
+                    C.byref(c))
+    return a.value, b.value, c.value
+
+
+def vloc_coef(radial, dradial, potc, nradct, a, b, c, rcuts, nqct):
+    radial, dradial, potc = _f64(radial), _f64(dradial), _f64(potc)
+    coef = np.zeros(nqct + 1)
+    lib().orc_vloc_coef(len(radial), nradct, _d(radial), _d(dradial), _d(potc), C.c_double(a),
+                        C.c_double(b), C.c_double(c), C.c_double(rcuts), nqct, _d(coef))
+    return coef
+
+
+def vloc_soft(atoms, cp1, a, b, c, rc, shape, h, xmax, veta, npw, grad=False):
+    atoms = _f64(atoms).reshape(-1, 3)
+    A = atoms.shape[0]
+    ax, ay, az = (np.ascontiguousarray(atoms[:, k]) for k in range(3))
+    N = int(np.prod(shape))
+    out = np.zeros(N)
+    g = np.zeros(3 * A * N) if grad else None
+    f = C.c_double
+    lib().orc_vloc_soft(A, _d(ax), _d(ay), _d(az), f(cp1), f(a), f(b), f(c), f(rc), shape[0],
+                        shape[1], shape[2], f(h[0]), f(h[1]), f(h[2]), f(xmax[0]), f(xmax[1]),
+                        f(xmax[2]), f(veta), npw[0], npw[1], npw[2], _d(out),
+                        _d(g) if grad else None)
+    return (out, g.reshape(3, A, N)) if grad else out
+
+
+def vloc_hard(atoms, nmax, nmesh, h, xmax, npmax, rcut, psctoff, rcuts, nqct, coef, filpp, eps,
+              nfiltyp, dense=None, rho_dense=None):
+    """Adds each atom's hard part to dense (8N for nmesh 2, modified in place
+    when given); with rho_dense returns the per-atom sums of rho times the
+    hard part's gradient times the dense volume element (natom x 3)."""
+    atoms = _f64(atoms).reshape(-1, 3)
+    A = atoms.shape[0]
+    ax, ay, az = (np.ascontiguousarray(atoms[:, k]) for k in range(3))
+    f = C.c_double
+    facc = np.zeros(3 * A) if rho_dense is not None else None
+    rd = _f64(rho_dense) if rho_dense is not None else None
+    lib().orc_vloc_hard(A, _d(ax), _d(ay), _d(az), nmax[0], nmax[1], nmax[2], nmesh, f(h[0]),
+                        f(h[1]), f(h[2]), f(xmax[0]), f(xmax[1]), f(xmax[2]), npmax[0], npmax[1],
+                        npmax[2], f(rcut), f(psctoff), f(rcuts), nqct, _d(_f64(coef)), f(filpp),
+                        f(eps), nfiltyp, _d(dense) if dense is not None else None,
+                        _d(rd) if rd is not None else None,
+                        _d(facc) if facc is not None else None)
+    return facc.reshape(A, 3) if facc is not None else dense
+
+
+def ewald(atoms, cp1, xmax, veta, npw, nrs):
+    atoms = _f64(atoms).reshape(-1, 3)
+    ax, ay, az = (np.ascontiguousarray(atoms[:, k]) for k in range(3))
+    fn = lib().orc_ewald
+    fn.restype = C.c_double
+    f = C.c_double
+    return fn(atoms.shape[0], _d(ax), _d(ay), _d(az), f(cp1), f(xmax[0]), f(xmax[1]),
+              f(xmax[2]), f(veta), npw[0], npw[1], npw[2], nrs[0], nrs[1], nrs[2])
+
+
+def initial_wave(atoms, cp1, zs_pre, neig, shape, h, xmax):
+    atoms = _f64(atoms).reshape(-1, 3)
+    ax, ay, az = (np.ascontiguousarray(atoms[:, k]) for k in range(3))
+    N = int(np.prod(shape))
+    psi = np.zeros(neig * N)
+    f = C.c_double
+    lib().orc_initial_wave(atoms.shape[0], _d(ax), _d(ay), _d(az), f(cp1), f(zs_pre), neig,
+                           shape[0], shape[1], shape[2], f(h[0]), f(h[1]), f(h[2]), f(xmax[0]),
+                           f(xmax[1]), f(xmax[2]), _d(psi))
+    return psi.reshape(neig, N)

@@ -166,6 +166,29 @@ void orc_force_nl(const orc_sys* s, int M, const double* psi, const double* sval
 void orc_hpsi_fast(const orc_sys* s, const double* psi, const double* rp, double* hpsi,
                    int nb, int nthreads);
 
+/* ---- local pseudopotential, Ewald energy, initial bands (rs_oracle_vloc.c) ---- */
+void orc_bisec(double z, double r, double eps, double* a, double* b, double* c);
+void orc_vloc_coef(int nradps, int nradct, const double* radial, const double* dradial,
+                   const double* potc, double a, double b, double c, double rcuts, int nqct,
+                   double* coef);
+void orc_vloc_soft(int natom, const double* atx, const double* aty, const double* atz,
+                   double cp1, double ca, double cb, double cc, double rc, int nx, int ny,
+                   int nz, double dx, double dy, double dz, double xmax, double ymax,
+                   double zmax, double veta, int npwx, int npwy, int npwz, double* out,
+                   double* grad);
+void orc_vloc_hard(int natom, const double* atx, const double* aty, const double* atz,
+                   int nxmax, int nymax, int nzmax, int nmesh, double dx, double dy, double dz,
+                   double xmax, double ymax, double zmax, int npxmax, int npymax, int npzmax,
+                   double rcut, double psctoff, double rcuts, int nqct, const double* coef,
+                   double filpp, double eps, int nfiltyp, double* dense,
+                   const double* rho_dense, double* force_acc);
+double orc_ewald(int natom, const double* atx, const double* aty, const double* atz,
+                 double cp1, double xmax, double ymax, double zmax, double veta, int npwx,
+                 int npwy, int npwz, int nrsx, int nrsy, int nrsz);
+void orc_initial_wave(int natom, const double* atx, const double* aty, const double* atz,
+                      double cp1, double zs_pre, int neig, int nx, int ny, int nz, double dx,
+                      double dy, double dz, double xmax, double ymax, double zmax, double* psi);
+
 #ifdef __cplusplus
 }
 #endif

@@ -162,6 +162,9 @@ extern "C" int rs_geom_destroy(rs_geom* g) {
     if (g->host_ev_done[i]) cudaEventDestroy(g->host_ev_done[i]);
   }
   if (g->host_ev_start) cudaEventDestroy(g->host_ev_start);
+  if (g->nl_cs) cudaStreamDestroy(g->nl_cs);
+  if (g->nl_ev_in) cudaEventDestroy(g->nl_ev_in);
+  if (g->nl_ev_out) cudaEventDestroy(g->nl_ev_out);
   delete g;
   return RS_OK;
 }

@@ -10,7 +10,14 @@ int launch_gather(const rs_geom* g, const double* mat, const double* rp, const T
 int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
                          const double* rp, const float* psi, float* hpsi, int nb,
                          cudaStream_t st, bool local_only = false);
+int hpsi_f32_nl_chunk(const rs_geom* g);
 }  // namespace rs
+
+extern "C" int rs_hpsi_f32_tuning(const rs_geom* g, int* nl_chunk) {
+  if (!g || !nl_chunk) return rs::fail(RS_EINVAL, "rs_hpsi_f32_tuning: null argument");
+  *nl_chunk = rs::hpsi_f32_nl_chunk(g);
+  return RS_OK;
+}
 
 extern "C" int rs_hpsi_f32(const rs_geom* g, const float* veff, const double* dij,
                            const double* rp, const float* psi, float* hpsi, int nb,

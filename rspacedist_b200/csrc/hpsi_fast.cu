@@ -16,6 +16,8 @@
 //    projector support (a fraction of the grid).  A thread owns one such
 //    point and a block of 16 bands: it loads the point's projector entries
 //    once and adds sum_e sum_j t[atom_e][b][j] p_e[j] to 16 bands of hpsi.
+#include <algorithm>
+
 #include "rs_common.cuh"
 #include "stencil.cuh"
 
@@ -319,6 +321,52 @@ __global__ void __launch_bounds__(128) k_nl_rmw_f32(
     if (b < nbb) out[(long)(b0 + b) * N + p] = h[b];
 }
 
+// k_nl_rmw_f32 on bands [b0, b0 + n) of an H psi of nb bands (t holds the
+// coefficients of all nb bands, atom-major: t[a][b][i])
+__global__ void __launch_bounds__(128) k_nl_rmw_f32_part(
+    const int* __restrict__ cov, const int* __restrict__ cov_off, long ncov,
+    const int* __restrict__ inv_atom, const float* __restrict__ inv_v,
+    const float* __restrict__ tco, int P, long N, int nb, int bstart, int n,
+    float* __restrict__ out) {
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncov) return;
+  const int b0 = bstart + blockIdx.y * NL_BANDS;
+  const int nbb = min(NL_BANDS, bstart + n - b0);
+  const int p = __ldg(cov + c);
+  const int e0 = __ldg(cov_off + c), e1 = __ldg(cov_off + c + 1);
+  float h[NL_BANDS];
+#pragma unroll
+  for (int b = 0; b < NL_BANDS; ++b) h[b] = b < nbb ? out[(long)(b0 + b) * N + p] : 0.f;
+  const int nq = P / 4;
+  for (int e = e0; e < e1; ++e) {
+    const int at = __ldg(inv_atom + e);
+    float4 v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = k < nq ? ld4(inv_v + (long)e * P + 4 * k) : zero4();
+    const float* tb = tco + ((long)at * nb + b0) * P;
+#pragma unroll
+    for (int b = 0; b < NL_BANDS; ++b) {
+      if (b < nbb) {
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (k < nq) {
+            const float4 t = ld4(tb + (long)b * P + 4 * k);
+            s = fmaf(t.x, v[k].x, s);
+            s = fmaf(t.y, v[k].y, s);
+            s = fmaf(t.z, v[k].z, s);
+            s = fmaf(t.w, v[k].w, s);
+          }
+        }
+        h[b] += s;
+      }
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < NL_BANDS; ++b)
+    if (b < nbb) out[(long)(b0 + b) * N + p] = h[b];
+}
+
 // S psi in two passes.  k_entry_sums: s[b][e] = sum_j t[atom_e][b][j] p_e[j]
 // for every inverse-list entry e, one FMA chain in projector order (the sum
 // k_nl_rmw_f32 adds per entry); a thread owns one entry and NL_BANDS bands,
@@ -406,17 +454,9 @@ bool hpsi_f32_fast_ok(const rs_geom* g, int nb) {
   return shape_ok && proj_ok;
 }
 
-// local_only: (-1/2 lap + veff) psi alone, without the nonlocal term (only
-// where hpsi_f32_fast_ok holds)
-int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
-                         const double* rp, const float* psi, float* hpsi, int nb,
-                         cudaStream_t st, bool local_only) {
-  if (nb <= 0) return RS_OK;
-  if (!hpsi_f32_fast_ok(g, nb)) {
-    if (local_only) return fail(RS_EINVAL, "H psi: local part alone needs the z-march shape");
-    return launch_gather<float, 1>(g, dij, rp, psi, veff, hpsi, nb, st);
-  }
-  StArgs a;
+namespace {
+
+void stencil_args(const rs_geom* g, const float* veff, StArgs& a) {
   a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
   a.zchunk = g->nz <= 160 ? g->nz : 64;
   a.ntx = (g->nx + TX - 1) / TX;
@@ -425,30 +465,124 @@ int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
     a.cx[m] = (float)g->cx[m]; a.cy[m] = (float)g->cy[m]; a.cz[m] = (float)g->cz[m];
   }
   a.c0 = (float)(g->cx[0] + g->cy[0] + g->cz[0]);
-  a.psi = psi; a.out = hpsi; a.veff = veff;
-  const int nzc = (g->nz + a.zchunk - 1) / a.zchunk;
-  dim3 grid(a.ntx * a.nty * nzc, nb);
-  const size_t smem = sizeof(float) * RING * HY * HX;
+  a.veff = veff;
   a.done = nullptr;
   a.part = nullptr;
+}
+
+// stencil of bands [b0, b0 + n) on st
+void launch_stencil(const rs_geom* g, StArgs a, const float* psi, float* hpsi, int b0, int n,
+                    cudaStream_t st) {
+  a.psi = psi + (long)b0 * g->N;
+  a.out = hpsi + (long)b0 * g->N;
+  const int nzc = (g->nz + a.zchunk - 1) / a.zchunk;
+  dim3 grid(a.ntx * a.nty * nzc, n);
+  k_stencil_f32_zmarch<false><<<grid, NTHREADS, sizeof(float) * RING * HY * HX, st>>>(a);
+}
+
+// nonlocal pass of bands [b0, b0 + n) (t holds all nb bands' coefficients)
+void launch_nl(const rs_geom* g, const float* t, float* hpsi, int b0, int n, int nb,
+               cudaStream_t st) {
+  // k_nl_rmw_f32 reads t[a][b0 + b] through its band offset: shift the
+  // coefficient pointer by b0 bands within each atom's block of nb bands
+  dim3 g2(div_up(g->n_cov, 128), div_up(n, NL_BANDS));
+  k_nl_rmw_f32_part<<<g2, 128, 0, st>>>(g->d_cov, g->d_cov_off, g->n_cov, g->d_inv_atom,
+                                         g->d_inv_v32, t, g->nprjmx, g->N, nb, b0, n, hpsi);
+}
+
+}  // namespace
+
+// local_only: (-1/2 lap + veff) psi alone, without the nonlocal term (only
+// where hpsi_f32_fast_ok holds).
+//
+// The nonlocal pass re-reads H psi at the covered points.  It runs on a side
+// stream chunk by chunk behind the stencil, so that a chunk's pass overlaps
+// the next chunk's stencil and finds much of the chunk's H psi still in L2.
+// The chunk size (bands) is chosen once per geometry, on its first call with
+// at least 64 bands, by timing the candidates on that call's own data (the
+// call's result is the same whichever ran last); -1 is the unchunked form.
+int launch_hpsi_f32_fast(const rs_geom* gc, const float* veff, const double* dij,
+                         const double* rp, const float* psi, float* hpsi, int nb,
+                         cudaStream_t st, bool local_only) {
+  if (nb <= 0) return RS_OK;
+  rs_geom* g = const_cast<rs_geom*>(gc);
+  if (!hpsi_f32_fast_ok(g, nb)) {
+    if (local_only) return fail(RS_EINVAL, "H psi: local part alone needs the z-march shape");
+    return launch_gather<float, 1>(g, dij, rp, psi, veff, hpsi, nb, st);
+  }
+  StArgs a;
+  stencil_args(g, veff, a);
   RS_CUDA(cudaFuncSetAttribute(k_stencil_f32_zmarch<false>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_stencil_f32_zmarch<false><<<grid, NTHREADS, smem, st>>>(a);
-  RS_LAUNCH_CHECK("k_stencil_f32_zmarch");
-  if (local_only || g->natom == 0 || g->n_cov == 0) return RS_OK;
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(sizeof(float) * RING * HY * HX)));
+  if (local_only || g->natom == 0 || g->n_cov == 0) {
+    launch_stencil(g, a, psi, hpsi, 0, nb, st);
+    RS_LAUNCH_CHECK("k_stencil_f32_zmarch");
+    return RS_OK;
+  }
   const long nt = (long)nb * g->natom * g->nprjmx;
   float* t = nullptr;
   RS_CUDA(cudaMallocAsync((void**)&t, nt * sizeof(float), st));
   k_tcoef_f32<<<div_up(nt, 256), 256, 0, st>>>(g->natom, g->nprjmx, g->d_nprj, dij, rp,
                                                1.0 / (g->dx * g->dy * g->dz), nb, t);
-  dim3 g2(div_up(g->n_cov, 128), div_up(nb, NL_BANDS));
-  k_nl_rmw_f32<<<g2, 128, 0, st>>>(g->d_cov, g->d_cov_off, g->n_cov, g->d_inv_atom,
-                                    g->d_inv_v32, t, g->nprjmx, g->N, nb, hpsi);
-  cudaError_t e = cudaGetLastError();
+  if (!g->nl_cs) {
+    RS_CUDA(cudaStreamCreateWithFlags(&g->nl_cs, cudaStreamNonBlocking));
+    RS_CUDA(cudaEventCreateWithFlags(&g->nl_ev_in, cudaEventDisableTiming));
+    RS_CUDA(cudaEventCreateWithFlags(&g->nl_ev_out, cudaEventDisableTiming));
+  }
+  auto run = [&](int chunk) -> cudaError_t {
+    if (chunk <= 0 || chunk >= nb) {
+      launch_stencil(g, a, psi, hpsi, 0, nb, st);
+      launch_nl(g, t, hpsi, 0, nb, nb, st);
+      return cudaGetLastError();
+    }
+    for (int b0 = 0; b0 < nb; b0 += chunk) {
+      const int n = std::min(chunk, nb - b0);
+      launch_stencil(g, a, psi, hpsi, b0, n, st);
+      cudaEventRecord(g->nl_ev_in, st);
+      cudaStreamWaitEvent(g->nl_cs, g->nl_ev_in, 0);
+      launch_nl(g, t, hpsi, b0, n, nb, g->nl_cs);
+    }
+    cudaEventRecord(g->nl_ev_out, g->nl_cs);
+    cudaStreamWaitEvent(st, g->nl_ev_out, 0);
+    return cudaGetLastError();
+  };
+  cudaError_t e = cudaSuccess;
+  if (g->nl_chunk == 0 && nb >= 64) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs == cudaStreamCaptureStatusNone) {
+      const int cand[] = {-1, 8, 16, 32, 64};
+      cudaEvent_t e0, e1;
+      float best = 0.f;
+      int pick = -1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      for (int c : cand) {
+        run(c);  // warm
+        cudaEventRecord(e0, st);
+        run(c);
+        cudaEventRecord(e1, st);
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (pick == -1 && best == 0.f) { best = ms; pick = c; }
+        else if (ms < best) { best = ms; pick = c; }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      if (e == cudaSuccess) g->nl_chunk = pick;
+    }
+  }
+  if (e == cudaSuccess) e = run(g->nl_chunk == 0 ? -1 : g->nl_chunk);
   cudaFreeAsync(t, st);
-  if (e != cudaSuccess) return cuda_status(e, "k_nl_rmw_f32");
+  if (e != cudaSuccess) return cuda_status(e, "H psi (k_stencil_f32_zmarch, k_nl_rmw_f32)");
   return RS_OK;
 }
+
+// the band-chunk size the FP32 H psi of this geometry picked (0: not yet
+// chosen, -1: unchunked)
+int hpsi_f32_nl_chunk(const rs_geom* g) { return g->nl_chunk; }
 
 // A p of the mixed Hartree CG (nfh = 4) by the H psi z-march: coefficients
 // cx, cy, cz [1..4] and diag from hartree_coefs, runs of 32 z planes (so one

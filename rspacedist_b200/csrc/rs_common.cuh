@@ -80,6 +80,13 @@ struct rs_geom {
   cudaEvent_t host_ev_start;
   float* host_buf;
   size_t host_buf_bytes;
+  // FP32 H psi: the nonlocal pass runs on nl_cs band chunk by band chunk
+  // behind the stencil (nl_ev_in after a stencil chunk, nl_ev_out at its
+  // end); nl_chunk bands per chunk, 0 until the first large call has timed
+  // the candidates (nl_chunk < 0: one stencil launch, then one pass)
+  cudaStream_t nl_cs;
+  cudaEvent_t nl_ev_in, nl_ev_out;
+  int nl_chunk;
 };
 
 namespace rs {

@@ -12,7 +12,12 @@ For each dataset it keeps what the real-space hot path consumes:
   * the charge-deficit matrix qvd (sss0, :213-217) and dion (akv0, in Ry,
     halved to Ha as at :221-225) over the dyadic slots;
   * the cut-off radius radial(nradct), the valence charge and the short-range
-    local potential potc = (vloc - vh)/2 in Ha (:160-167) on the same grid.
+    local potential potc = (vloc - vh)/2 in Ha (:160-167) on the same grid;
+  * the dataset's own radial mesh r, dr/di (nradps points, nradct of them
+    inside the cut-off), potc on that mesh and, for PAW datasets, the density
+    column the reader feeds to the LDA before subtracting v_xc from potc
+    (:158-186): the local pseudopotential's Fourier-Bessel coefficients are
+    summed over this mesh as filterpseudopotentials does.
 """
 import json
 import os
@@ -66,7 +71,7 @@ def parse(path):
     nxt(); nxt()
     dion = np.array([[float(x) for x in nxt().split()] for _ in range(nrprj)]) * 0.5
     return dict(kind=kind, z=z, zv=zv, lmax=lmax, nprmx=nprmx, npr=npr, mesh=mesh,
-                nradct=nradct, prj=prj, qvd=qvd, dion=dion)
+                nradps=nradps, nradct=nradct, prj=prj, qvd=qvd, dion=dion)
 
 
 def derive(d):
@@ -93,6 +98,12 @@ def derive(d):
     rr = np.arange(DR, min(12.0, m[sel, 0].max()), DR)
     out["potc_dr"] = DR
     out["potc"] = [float(cs(DR))] + [float(x) for x in cs(rr)]
+    out["nradps"] = int(d["nradps"])
+    out["nradct"] = int(d["nradct"])
+    out["mesh_r"] = [float(x) for x in m[:, 0]]
+    out["mesh_drdi"] = [float(x) for x in m[:, 1]]
+    out["mesh_potc"] = [float(x) for x in potc]
+    out["mesh_rho"] = [float(x) for x in m[:, 6]]
     return out
 
 
@@ -107,4 +118,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/RSPACEes.v08.01")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python -m rspacedist_b200.data.make_pp_tables <RSPACEes.v08.01 directory>")
+    main(sys.argv[1])

@@ -45,6 +45,18 @@ SIGNATURES = {
     "rs_geom_create": [C.POINTER(_p), _i, _i, _i, _i, _d, _d, _d, _i, _i, _i, _ip, _ip, _ip,
                        _dp],
     "rs_geom_destroy": [_p],
+    "rs_vloc_soft": [_i, _dp, _dp, _i, _i, _i, _d, _d, _d, _d, _d, _d, _d, _i, _i, _i, _p, _p],
+    "rs_vloc_hard_add": [_i, _dp, _ip, _i, _dp, _ip, _i, _dp, _i, _i, _i, _d, _d, _d, _d, _d, _d,
+                         _i, _i, _i, _i, _d, _d, _i, _p, _p],
+    "rs_ewald": [_i, _dp, _dp, _d, _d, _d, _d, _i, _i, _i, _dp, _dp, _p],
+    "rs_force_local": [_i, _dp, _dp, _ip, _i, _dp, _ip, _i, _dp, _i, _i, _i, _d, _d, _d, _d, _d,
+                       _d, _d, _i, _i, _i, _i, _i, _i, _i, _d, _d, _i, _p, _p, _dp, _p],
+    "rs_force_adjoint_f64": [_i, _i, _i, _dp, _ip, _ip, _ip, _ip, _i, _i, _d, _dp, _ip, _ip, _ip,
+                             _d, _i, _i, _i, _d, _d, _d, _p, _p, _p, _p, _p, _i, _dp, _p, _p],
+    "rs_force_adjoint_f32": [_i, _i, _i, _dp, _ip, _ip, _ip, _ip, _i, _i, _d, _dp, _ip, _ip, _ip,
+                             _d, _i, _i, _i, _d, _d, _d, _p, _p, _p, _p, _p, _i, _dp, _p, _p],
+    "rs_initial_wave_f64": [_i, _dp, _dp, _i, _i, _i, _i, _d, _d, _d, _d, _d, _d, _p, _p],
+    "rs_initial_wave_f32": [_i, _dp, _dp, _i, _i, _i, _i, _d, _d, _d, _d, _d, _d, _p, _p],
     "rs_kslaplacian_f64": [_p, _p, _p, _p, _i, _p],
     "rs_kslaplacian_f32": [_p, _p, _p, _p, _i, _p],
     "rs_nonlocal_dot_f64": [_p, _p, _i, _p, _p],
@@ -52,6 +64,7 @@ SIGNATURES = {
     "rs_nonlocal_apply_f64": [_p, _p, _p, _i, _p, _p],
     "rs_hpsi_f64": [_p, _p, _p, _p, _p, _p, _i, _p],
     "rs_hpsi_f32": [_p, _p, _p, _p, _p, _p, _i, _p],
+    "rs_hpsi_f32_tuning": [_p, _ip],
     "rs_spsi_f64": [_p, _p, _p, _p, _p, _i, _p],
     "rs_spsi_f32": [_p, _p, _p, _p, _p, _i, _p],
     "rs_hpsi_host_f32": [_p, _p, _p, _p, _p, _p, _i, _i, _p],

@@ -1,6 +1,10 @@
-"""The Kohn-Sham SCF loop of kukan (kukan8f.F90:513-680) driven through the
+"""The Kohn-Sham SCF loop of kukan (kukan8f.F90:466-762) driven through the
 B200 library, one k-point and spin, periodic cell:
 
+    set-up             vloc_coarse of pseudocalc                    (pseudo.local_potential)
+                       bands of setup_initialwave, S-orthonormalised (rs_initial_wave_*,
+                       and the start density scf_charge of them       rs_orthogonalize_*,
+                       with the occupations of equal eigenvalues      rs_density_*)
     iscf = 1, 2, ...
       scf_chargemixing   rho_in  <- Broyden(rho_out, rho_in)      (rs_mixer_step)
       scf_potentials     rho_dense = c2d(rho_in)                   (rs_interp_c2d)
@@ -8,21 +12,23 @@ B200 library, one k-point and spin, periodic cell:
                          V_xc dense = PZ LDA(rho_dense)            (rs_vxc_pz)
                          veff = d2c(V_xc) + (vloc + d2c(V_H))     (rs_interp_d2c, rs_veff_sum)
       scf_diag           RR / CG / DIIS / reorder                  (rs_scf_diag_f64|f32)
+      scf_occupation     Fermi-Dirac, kT = tf                      (host bisection)
       scf_charge         rho_out = sum_l f_l psi_l^2               (rs_density_*)
       scf_diffcharge     stop when sqrt(sum (rho_in-rho_out)^2 dV/V) < eps_scf
+    totalenergy_space / totalenergy_eig / output_energy (kukan8f.F90:722-762,
+    totalenergy8f.F90:8-199, output8f.F90:240-242) on the last input density:
+      E = sum f e - 1/2 sum V_H rho_d dV_d - sum rho vx dV + sum rho_d e_xc dV_d + E_ewald
+    with the dot products in FP64 on the device (rs_dot_f64) and the ion-ion
+    energy from rs_ewald.
 
 `dtype=torch.float64` is the plain FP64 path, `torch.float32` the mixed path
 (FP32 bands, FP64 potentials, densities, subspace eigensolve and sums).
 
-Inputs the library does not build (they sit outside the ported hot path):
-the local pseudopotential and the starting charge are model fields given per
-atom (a Gaussian well and a normalised Gaussian of the valence charge), D and
-S stay at their dataset values (no PAW one-centre update), and occupations
-follow kukan's Fermi-Dirac smearing (scf_occupation, kT = 3e-3 Ha) for
-nelec = 2 nocc electrons, or are fixed at 2 for the lowest nocc bands with
-smearing=False (kukan's mpre /= 0).  Every grid step that kukan performs on
-these inputs runs on the GPU; the occupations (a bisection over M
-eigenvalues) are host logic."""
+For PAW datasets D and S stay at the dataset's values and the density is the
+smooth part only: the one-centre terms of scf_dij, scf_charge_onecenter and
+scf_augcharge are not part of this loop.  `potential="model"` replaces the
+local potential and start density by Gaussians per atom (a depth-1.5 Ha well
+and the valence charge), as an analytic test input."""
 from __future__ import annotations
 
 import time
@@ -161,6 +167,22 @@ class ScfResult:
     fermi: float = 0.0                             # Fermi level (Ha), smearing only
     hartree_iters: list = field(default_factory=list)
     phase_seconds: dict = field(default_factory=dict)  # with profile=True only
+    energy: dict = field(default_factory=dict)    # output_energy's terms (Ha)
+    occ: np.ndarray | None = None                  # final occupations
+
+
+def helmholtz_entropy(occ, tf: float) -> float:
+    """eneth of totalenergy_eig (totalenergy8f.F90:166-196), one k-point and
+    spin (tmpfac = 1/2): tf sum_l (f ln f + (1-f) ln(1-f)) / tmpfac, with
+    f = occ/2 and the logarithms dropped below 1e-8."""
+    tmpfac = 0.5
+    e = 0.0
+    for o in np.asarray(occ, dtype=np.float64):
+        t = o * tmpfac
+        t1 = np.log(t) if t > 1.0e-8 else 0.0
+        t2 = np.log(1.0 - t) if 1.0 - t > 1.0e-8 else 0.0
+        e = e + (t * t1 + (1.0 - t) * t2) / tmpfac
+    return float(e * tf)
 
 
 def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float = 1e-6,
@@ -168,15 +190,23 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
             seed: int = 0, zval: float = 4.0, epsvh: float = 1e-12, vloc=None, rho0=None,
             psi0=None, log=None, profile: bool = False, smearing: bool = True,
             tf: float = 3.0e-3, restart_dir: str | None = None,
-            save_dir: str | None = None) -> ScfResult:
-    """kukan's SCF loop (kukan8f.F90:513-680) over the C ABI.
+            save_dir: str | None = None, potential: str = "kukan",
+            polish: bool = True) -> ScfResult:
+    """kukan's SCF loop (kukan8f.F90:466-762) over the C ABI.
 
+    potential: "kukan" (the dataset's local pseudopotential, setup_initialwave
+    start) or "model" (Gaussian wells and charges per atom, smooth random
+    start bands); vloc / rho0 / psi0 override the local potential, the start
+    density and the start bands.
     restart_dir: start from kukan restart files there (wfc.00000.000 for the
     bands, rho.00000 for the start density, vht.00000 for the Hartree warm
-    start; missing density or potential files fall back to the model start).
+    start).
     save_dir: write the same files after the last iteration (the last input
     density as rho.*, the output density as r_o.*), as write_wf and
-    write_rhovht do."""
+    write_rhovht do.
+    polish: on the mixed path, finish with one FP64 orthonormalisation and
+    Rayleigh-Ritz step of the converged bands (its time is part of the
+    loop's), so that eigenvalues and energies are FP64 quantities."""
     dev = torch.device("cuda")
     # the loop runs on a stream of its own (launches are stream-ordered there
     # and the Hartree solve can replay its iteration batches as CUDA graphs)
@@ -185,13 +215,17 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
     with torch.cuda.stream(side):
         res = _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, zval,
                        epsvh, vloc, rho0, psi0, log, profile, smearing, tf, restart_dir,
-                       save_dir, dev)
+                       save_dir, dev, potential, polish)
     side.synchronize()
     return res
 
 
 def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, zval, epsvh,
-             vloc, rho0, psi0, log, profile, smearing, tf, restart_dir, save_dir, dev):
+             vloc, rho0, psi0, log, profile, smearing, tf, restart_dir, save_dir, dev,
+             potential, polish):
+    from . import pseudo as PP
+    if potential not in ("kukan", "model"):
+        raise ValueError(f"potential must be 'kukan' or 'model', not {potential!r}")
     g = K.Geometry(cell)
     N, shape = cell.N, cell.shape
     dshape = tuple(2 * s for s in shape)
@@ -205,21 +239,37 @@ def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, z
         got = CK.read_rho(restart_dir, shape)
         rho_start = None if got is None else got[0]
         vh_start = CK.read_vht(restart_dir, shape)
-    elif psi0 is None:
-        psi = smooth_start_bands_device(shape, M, seed, dtype)
-    else:
+    elif psi0 is not None:
         psi = torch.as_tensor(np.ascontiguousarray(psi0), device=dev).to(dtype)
+    elif potential == "kukan":
+        psi = PP.initial_bands(cell, M, dtype)
+    else:
+        psi = smooth_start_bands_device(shape, M, seed, dtype)
     sss = None if cell.sss is None else torch.tensor(cell.sss, dtype=f64, device=dev)
     b = K.Bands(g, psi, sss)
     K.orthogonalization(b, 1)
+    # kukan's first occupations: scf_occupation of the initial all-zero
+    # eigenvalues (equal occupations) with smearing, the lowest nocc bands
+    # otherwise
     occ = torch.zeros(M, dtype=f64, device=dev)
-    occ[:nocc] = 2.0
-    vloc_t = torch.tensor(model_local_potential(cell) if vloc is None else vloc, dtype=f64,
-                          device=dev)
+    if smearing:
+        occ.copy_(torch.from_numpy(scf_occupation(np.zeros(M), 2.0 * nocc, tf)[0]))
+    else:
+        occ[:nocc] = 2.0
+    if vloc is not None:
+        vloc_t = torch.as_tensor(np.ascontiguousarray(vloc), dtype=f64, device=dev)
+    elif potential == "kukan":
+        vloc_t = PP.local_potential(cell)[0]
+    else:
+        vloc_t = torch.tensor(model_local_potential(cell), dtype=f64, device=dev)
     if rho_start is not None:
         rho0 = rho_start
-    rho_o = torch.tensor(atomic_density(cell, zval) if rho0 is None else rho0, dtype=f64,
-                         device=dev)
+    if rho0 is not None:
+        rho_o = torch.as_tensor(np.ascontiguousarray(rho0), dtype=f64, device=dev)
+    elif potential == "kukan":
+        rho_o = K.scf_charge_smt(occ, b.psi, N)
+    else:
+        rho_o = torch.tensor(atomic_density(cell, zval), dtype=f64, device=dev)
     rho_i = torch.zeros(N, dtype=f64, device=dev)
     vh_d = torch.zeros(8 * N, dtype=f64, device=dev)
     if vh_start is not None:
@@ -243,6 +293,7 @@ def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, z
 
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    rho_d = vx = ex_d = None
     for iscf in range(1, looplimit + 1):
         ti = time.perf_counter()
         tp = ti
@@ -253,7 +304,7 @@ def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, z
                               mixed=dtype == torch.float32)
         tp = mark("hartree", tp)
         vh = K.trans_d2c(shape, 4, vh_d)
-        vx_d, _ = K.vxpot_lda_pz(rho_d)
+        vx_d, ex_d = K.vxpot_lda_pz(rho_d)
         vx = K.trans_d2c(shape, 4, vx_d)
         K.veff_sum(vx, vloc_t, vh, veff64, veff32)
         tp = mark("xc+transfer", tp)
@@ -275,15 +326,42 @@ def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, z
         if diff < eps_scf:
             res.converged = True
             break
+    if polish and dtype == torch.float32:
+        # FP64 polish of the mixed path: the converged FP32 bands in FP64,
+        # S-orthonormalised and rotated by one FP64 Rayleigh-Ritz step with
+        # the last effective potential, so that the eigenvalue sums carry no
+        # FP32 rounding of H psi or of the tensor-core Gram products
+        b64 = K.Bands(g, b.psi.double(), sss)
+        K.orthogonalization(b64, 1)
+        K.rayleighritz(b64, veff64, dij, 1)
+        K.reorderstates(b64)
+        b = b64
+        if smearing:
+            fn, res.fermi = scf_occupation(b.sval, 2.0 * nocc, tf)
+            occ.copy_(torch.from_numpy(fn))
+        rho_o = K.scf_charge_smt(occ, b.psi, N)
+        tp = mark("fp64_polish", tp)
     torch.cuda.synchronize()
     res.seconds = time.perf_counter() - t0
     res.sval = np.array(b.sval)
     occ_h = occ.cpu().numpy()
-    res.eband = float(np.sum(occ_h * res.sval))
+    res.occ = occ_h
+    res.eband = float(np.cumsum(occ_h * res.sval)[-1])
+    # totalenergy_space on the last input density and its potentials
+    ddv = dvol / 8.0
+    eneha = -0.5 * float(K.dot(vh_d, rho_d).item()) * ddv
+    eneex = -float(K.dot(rho_i, vx).item()) * dvol + float(K.dot(rho_d, ex_d).item()) * ddv
+    eneat = PP.ion_energy(cell) if potential == "kukan" else 0.0
+    eneth = helmholtz_entropy(occ_h, tf) if smearing else 0.0
+    etot = res.eband + eneex + eneha + eneat
+    res.energy = dict(eneel=res.eband, eneex=eneex, eneha=eneha, eneat=eneat, eneth=eneth,
+                      total=etot, free=etot + eneth)
     if save_dir is not None:
         CK.write_wf(save_dir, b.psi, res.sval, shape)
         CK.write_rho(save_dir, rho_i, shape)
         CK.write_rho(save_dir, rho_o, shape, name="r_o")
         CK.write_vht(save_dir, vh_d, shape)
+    res.bands = b
+    res.rho_out = rho_o
     mixer.close()
     return res
