@@ -210,8 +210,8 @@ def run_gpu(args):
     torch.cuda.synchronize()
     import ctypes as C
     from rspacedist_b200 import lib as RL
-    chunk = C.c_int(0)
-    RL.call("rs_hpsi_f32_tuning", g.handle, C.byref(chunk))
+    chunk, nlb = C.c_int(0), C.c_int(0)
+    RL.call("rs_hpsi_f32_tuning", g.handle, C.byref(chunk), C.byref(nlb))
     nl_chunk = chunk.value
     nchunks = 1 if nl_chunk <= 0 else -(-nb // nl_chunk)
     launches_per_step = 1 + 2 * nchunks  # k_tcoef_f32, then stencil + nonlocal per chunk
@@ -336,7 +336,7 @@ def run_gpu(args):
                        "grid": [GRID] * 3, "bands": nb, "atoms": cell.natom,
                        "projectors": cell.nprjmx, "inverse_entries": g.entries,
                        "l2": "inputs (9.2 GB psi) larger than L2; no flush",
-                       "nl_band_chunk": nl_chunk,
+                       "nl_band_chunk": nl_chunk, "nl_bands_per_thread": nlb.value,
                        "parallelism": f"bands replicated per GPU x{world}"},
             "band_points_per_s": round(nb * cell.N * world / (ms * 1e-3), 1),
             "roofline": {"bound": "hbm", "kernel": "k_stencil_f32_zmarch",
@@ -352,7 +352,7 @@ def run_gpu(args):
                          "ms_per_launch": round(st_ms, 3)},
             "roofline_sweep": {"bound": "hbm",
                                "kernels": "k_tcoef_f32, then k_stencil_f32_zmarch and "
-                                          "k_nl_rmw_f32_part per band chunk",
+                                          "k_nl_rmw_f32 per band chunk",
                                "achieved": round(sweep_gbs, 1), "peak": peak, "unit": "GB/s",
                                "frac": round(sweep_gbs / peak, 4),
                                "algorithmic_bytes_per_step": nbytes},
@@ -379,21 +379,21 @@ def run_gpu(args):
 
 def run_scf_leg(cell, looplimit, eps_scf=1e-6):
     """The SCF half of the metric on the same Si512 cell: kukan's SCF
-    (local pseudopotential of the dataset, setup_initialwave start, Broyden
-    mixing eta 0.1, RR + CG for the first two iterations then RR + DIIS,
-    Hartree CG, PZ LDA, Fermi-Dirac occupations for 2048 electrons in 1100
-    bands) to diff_charge < eps_scf on the mixed path (FP32 bands) and on the
-    plain FP64 path, each timed on the wall clock with the device
-    synchronised, then the total energies of output_energy."""
+    (local pseudopotential of the dataset, Broyden mixing eta 0.3, RR + DIIS
+    every iteration, Hartree CG, PZ LDA, Fermi-Dirac occupations for 2048
+    electrons in 1100 bands) from seeded smooth random bands to
+    diff_charge < eps_scf on the mixed path (FP32 bands) and on the plain FP64
+    path, each timed on the wall clock with the device synchronised, then the
+    total energies of output_energy."""
     import torch
     from rspacedist_b200 import lib, scf
-    prm = lib.solver_prm(ncgscf=2)
+    prm = lib.solver_prm(ncgscf=0)
     res = {}
     for name, dt in (("mixed", torch.float32), ("fp64", torch.float64)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r = scf.run_scf(cell, NB, 1024, dtype=dt, prm=prm, looplimit=looplimit, eta=0.1,
-                        eps_scf=eps_scf, profile=True)
+        r = scf.run_scf(cell, NB, 1024, dtype=dt, prm=prm, looplimit=looplimit, eta=0.3,
+                        eps_scf=eps_scf, profile=True, start="random", seed=0)
         total = time.perf_counter() - t0
         r.bands = r.rho_out = None
         res[name] = (r, total)
@@ -406,9 +406,10 @@ def run_scf_leg(cell, looplimit, eps_scf=1e-6):
     return {
         "workload": "Si512 SCF: 128^3 grid, 1100 bands (2048 electrons, Fermi-Dirac kT 3e-3 Ha), "
                     "Si PAW projectors with the dataset's D and S (no one-centre update), the "
-                    "dataset's local pseudopotential (pseudocalc soft + hard parts), "
-                    "setup_initialwave start, Broyden mixing (eta 0.1, 20 steps), RR + CG x2 "
-                    "then RR + DIIS, Hartree CG (epsvh 1e-12) on the 256^3 dense grid",
+                    "dataset's local pseudopotential (pseudocalc soft + hard parts), seeded "
+                    "smooth random start bands, Broyden mixing (eta 0.3, 20 steps), RR + DIIS "
+                    "every iteration, Hartree CG (epsvh 1e-12, at most 800 iterations) on the "
+                    "256^3 dense grid",
         "eps_scf": eps_scf,
         "converged": {"mixed": a.converged, "fp64": b.converged},
         "iterations": {"mixed": a.iterations, "fp64": b.iterations},
@@ -841,7 +842,7 @@ def main():
                     help="skip the plain FP64 sweep")
     ap.add_argument("--bands", type=int, default=NB,
                     help="bands per sweep (default 1100; smaller values for profiling only)")
-    ap.add_argument("--scf-loops", "--scf-iters", dest="scf_loops", type=int, default=60,
+    ap.add_argument("--scf-loops", "--scf-iters", dest="scf_loops", type=int, default=200,
                     help="iteration limit of the Si512 SCF run per path (0 skips the leg)")
     ap.add_argument("--force-check", action="store_true",
                     help="run the Si64 force check (adjoint vs energy differences) and exit")

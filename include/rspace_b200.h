@@ -104,11 +104,13 @@ int rs_nonlocal_dot_f32(const rs_geom* g, const float* psi, int nb, double* rp, 
 int rs_nonlocal_apply_f64(const rs_geom* g, const double* mat, const double* rp, int nb,
                           double* out, void* stream);
 
-/* The band-chunk size the FP32 H psi of g chose for running its nonlocal
- * pass behind the stencil (rs_hpsi_f32 times the candidates on its first
- * call with at least 64 bands): 0 before that call, -1 for one stencil
- * launch followed by one pass.  No counterpart in the reference. */
-int rs_hpsi_f32_tuning(const rs_geom* g, int* nl_chunk);
+/* The launch shape the FP32 H psi of g chose (rs_hpsi_f32 times the
+ * candidates on its first call with at least 64 bands): nl_chunk, the band
+ * chunk whose nonlocal pass runs on a side stream behind the next chunk's
+ * stencil (-1: one stencil launch, then one pass), and nl_bands, the bands
+ * per thread of that pass (16 or 32); both 0 before that call.  No
+ * counterpart in the reference. */
+int rs_hpsi_f32_tuning(const rs_geom* g, int* nl_chunk, int* nl_bands);
 
 /* Fused H psi = nonlocal(D) + stencil + veff, one pass over psi (the H*psi of
  * kscg8f.F90:147-183 and rayleighritz_hamiltonian_r, rayleigh-ritz8f.F90:493-575).

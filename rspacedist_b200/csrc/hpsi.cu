@@ -13,9 +13,11 @@ int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
 int hpsi_f32_nl_chunk(const rs_geom* g);
 }  // namespace rs
 
-extern "C" int rs_hpsi_f32_tuning(const rs_geom* g, int* nl_chunk) {
-  if (!g || !nl_chunk) return rs::fail(RS_EINVAL, "rs_hpsi_f32_tuning: null argument");
-  *nl_chunk = rs::hpsi_f32_nl_chunk(g);
+extern "C" int rs_hpsi_f32_tuning(const rs_geom* g, int* nl_chunk, int* nl_bands) {
+  if (!g || !nl_chunk || !nl_bands) return rs::fail(RS_EINVAL, "rs_hpsi_f32_tuning: null argument");
+  const int code = rs::hpsi_f32_nl_chunk(g);
+  *nl_chunk = code > 0 ? code / 64 : (code < 0 ? -1 : 0);
+  *nl_bands = code > 0 ? code % 64 : (code < 0 ? -code : 0);
   return RS_OK;
 }
 

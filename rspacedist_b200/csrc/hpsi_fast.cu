@@ -278,74 +278,33 @@ __global__ void k_tcoef_f32(int natom, int nprjmx, const int* __restrict__ nprj,
 // hpsi[b][p] += sum over p's entries e of t[a_e][b] . p_e for NL_BANDS bands.
 // All loads of a thread are independent of each other except through the
 // entry's atom index, so many are in flight at once.
+// tstride: the band count of the coefficient array (t[a][b] at (a tstride +
+// b) P), so that a band range of a larger H psi runs with tco and out offset
+// to its first band.
+template <int NLB = NL_BANDS>
 __global__ void __launch_bounds__(128) k_nl_rmw_f32(
     const int* __restrict__ cov, const int* __restrict__ cov_off, long ncov,
     const int* __restrict__ inv_atom, const float* __restrict__ inv_v,
-    const float* __restrict__ tco, int P, long N, int nb, float* __restrict__ out) {
-  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncov) return;
-  const int b0 = blockIdx.y * NL_BANDS;
-  const int nbb = min(NL_BANDS, nb - b0);
-  const int p = __ldg(cov + c);
-  const int e0 = __ldg(cov_off + c), e1 = __ldg(cov_off + c + 1);
-  float h[NL_BANDS];
-#pragma unroll
-  for (int b = 0; b < NL_BANDS; ++b) h[b] = b < nbb ? out[(long)(b0 + b) * N + p] : 0.f;
-  const int nq = P / 4;
-  for (int e = e0; e < e1; ++e) {
-    const int at = __ldg(inv_atom + e);
-    float4 v[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] = k < nq ? ld4(inv_v + (long)e * P + 4 * k) : zero4();
-    const float* tb = tco + ((long)at * nb + b0) * P;
-#pragma unroll
-    for (int b = 0; b < NL_BANDS; ++b) {
-      if (b < nbb) {
-        float s = 0.f;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          if (k < nq) {
-            const float4 t = ld4(tb + (long)b * P + 4 * k);
-            s = fmaf(t.x, v[k].x, s);
-            s = fmaf(t.y, v[k].y, s);
-            s = fmaf(t.z, v[k].z, s);
-            s = fmaf(t.w, v[k].w, s);
-          }
-        }
-        h[b] += s;
-      }
-    }
-  }
-#pragma unroll
-  for (int b = 0; b < NL_BANDS; ++b)
-    if (b < nbb) out[(long)(b0 + b) * N + p] = h[b];
-}
-
-// k_nl_rmw_f32 on bands [b0, b0 + n) of an H psi of nb bands (t holds the
-// coefficients of all nb bands, atom-major: t[a][b][i])
-__global__ void __launch_bounds__(128) k_nl_rmw_f32_part(
-    const int* __restrict__ cov, const int* __restrict__ cov_off, long ncov,
-    const int* __restrict__ inv_atom, const float* __restrict__ inv_v,
-    const float* __restrict__ tco, int P, long N, int nb, int bstart, int n,
+    const float* __restrict__ tco, int P, long N, int nb, int tstride,
     float* __restrict__ out) {
   const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncov) return;
-  const int b0 = bstart + blockIdx.y * NL_BANDS;
-  const int nbb = min(NL_BANDS, bstart + n - b0);
+  const int b0 = blockIdx.y * NLB;
+  const int nbb = min(NLB, nb - b0);
   const int p = __ldg(cov + c);
   const int e0 = __ldg(cov_off + c), e1 = __ldg(cov_off + c + 1);
-  float h[NL_BANDS];
+  float h[NLB];
 #pragma unroll
-  for (int b = 0; b < NL_BANDS; ++b) h[b] = b < nbb ? out[(long)(b0 + b) * N + p] : 0.f;
+  for (int b = 0; b < NLB; ++b) h[b] = b < nbb ? out[(long)(b0 + b) * N + p] : 0.f;
   const int nq = P / 4;
   for (int e = e0; e < e1; ++e) {
     const int at = __ldg(inv_atom + e);
     float4 v[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) v[k] = k < nq ? ld4(inv_v + (long)e * P + 4 * k) : zero4();
-    const float* tb = tco + ((long)at * nb + b0) * P;
+    const float* tb = tco + ((long)at * tstride + b0) * P;
 #pragma unroll
-    for (int b = 0; b < NL_BANDS; ++b) {
+    for (int b = 0; b < NLB; ++b) {
       if (b < nbb) {
         float s = 0.f;
 #pragma unroll
@@ -363,7 +322,7 @@ __global__ void __launch_bounds__(128) k_nl_rmw_f32_part(
     }
   }
 #pragma unroll
-  for (int b = 0; b < NL_BANDS; ++b)
+  for (int b = 0; b < NLB; ++b)
     if (b < nbb) out[(long)(b0 + b) * N + p] = h[b];
 }
 
@@ -480,14 +439,23 @@ void launch_stencil(const rs_geom* g, StArgs a, const float* psi, float* hpsi, i
   k_stencil_f32_zmarch<false><<<grid, NTHREADS, sizeof(float) * RING * HY * HX, st>>>(a);
 }
 
-// nonlocal pass of bands [b0, b0 + n) (t holds all nb bands' coefficients)
-void launch_nl(const rs_geom* g, const float* t, float* hpsi, int b0, int n, int nb,
+// nonlocal pass of bands [b0, b0 + n) (t holds all nb bands' coefficients),
+// nlb bands per thread (16 or 32)
+void launch_nl(const rs_geom* g, const float* t, float* hpsi, int b0, int n, int nb, int nlb,
                cudaStream_t st) {
-  // k_nl_rmw_f32 reads t[a][b0 + b] through its band offset: shift the
-  // coefficient pointer by b0 bands within each atom's block of nb bands
-  dim3 g2(div_up(g->n_cov, 128), div_up(n, NL_BANDS));
-  k_nl_rmw_f32_part<<<g2, 128, 0, st>>>(g->d_cov, g->d_cov_off, g->n_cov, g->d_inv_atom,
-                                         g->d_inv_v32, t, g->nprjmx, g->N, nb, b0, n, hpsi);
+  // t[a][b0 + b] lies b0 P floats past t[a][b]: offset the base, keep the
+  // stride of all nb bands
+  const float* tb = t + (long)b0 * g->nprjmx;
+  float* out = hpsi + (long)b0 * g->N;
+  if (nlb == 32) {
+    dim3 g2(div_up(g->n_cov, 128), div_up(n, 32));
+    k_nl_rmw_f32<32><<<g2, 128, 0, st>>>(g->d_cov, g->d_cov_off, g->n_cov, g->d_inv_atom,
+                                         g->d_inv_v32, tb, g->nprjmx, g->N, n, nb, out);
+  } else {
+    dim3 g2(div_up(g->n_cov, 128), div_up(n, NL_BANDS));
+    k_nl_rmw_f32<<<g2, 128, 0, st>>>(g->d_cov, g->d_cov_off, g->n_cov, g->d_inv_atom,
+                                      g->d_inv_v32, tb, g->nprjmx, g->N, n, nb, out);
+  }
 }
 
 }  // namespace
@@ -530,18 +498,26 @@ int launch_hpsi_f32_fast(const rs_geom* gc, const float* veff, const double* dij
     RS_CUDA(cudaEventCreateWithFlags(&g->nl_ev_in, cudaEventDisableTiming));
     RS_CUDA(cudaEventCreateWithFlags(&g->nl_ev_out, cudaEventDisableTiming));
   }
-  auto run = [&](int chunk) -> cudaError_t {
+  // tuning code: chunk size in bands (<= 0: unchunked) times 64, plus the
+  // nonlocal band block (16 or 32)
+  auto run = [&](int code) -> cudaError_t {
+    const int chunk = code >= 0 ? code / 64 : -1;
+    const int nlb = code >= 0 ? code % 64 : (-code) % 64;
     if (chunk <= 0 || chunk >= nb) {
       launch_stencil(g, a, psi, hpsi, 0, nb, st);
-      launch_nl(g, t, hpsi, 0, nb, nb, st);
+      launch_nl(g, t, hpsi, 0, nb, nb, nlb, st);
       return cudaGetLastError();
     }
+    // small chunks split z into runs of 32 planes so that a chunk's stencil
+    // still fills the GPU
+    StArgs ac = a;
+    if (chunk <= 16 && g->nz > 64) ac.zchunk = 32;
     for (int b0 = 0; b0 < nb; b0 += chunk) {
       const int n = std::min(chunk, nb - b0);
-      launch_stencil(g, a, psi, hpsi, b0, n, st);
+      launch_stencil(g, ac, psi, hpsi, b0, n, st);
       cudaEventRecord(g->nl_ev_in, st);
       cudaStreamWaitEvent(g->nl_cs, g->nl_ev_in, 0);
-      launch_nl(g, t, hpsi, b0, n, nb, g->nl_cs);
+      launch_nl(g, t, hpsi, b0, n, nb, nlb, g->nl_cs);
     }
     cudaEventRecord(g->nl_ev_out, g->nl_cs);
     cudaStreamWaitEvent(st, g->nl_ev_out, 0);
@@ -552,10 +528,13 @@ int launch_hpsi_f32_fast(const rs_geom* gc, const float* veff, const double* dij
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(st, &cs);
     if (cs == cudaStreamCaptureStatusNone) {
-      const int cand[] = {-1, 8, 16, 32, 64};
+      // unchunked (negative codes) or chunks of 4 to 64 bands, with
+      // nonlocal band blocks of 16 or 32
+      const int cand[] = {-16, -32, 4 * 64 + 16, 8 * 64 + 16, 16 * 64 + 16, 16 * 64 + 32,
+                          32 * 64 + 16, 32 * 64 + 32, 64 * 64 + 32};
       cudaEvent_t e0, e1;
       float best = 0.f;
-      int pick = -1;
+      int pick = -NL_BANDS;
       cudaEventCreate(&e0);
       cudaEventCreate(&e1);
       for (int c : cand) {
@@ -566,15 +545,17 @@ int launch_hpsi_f32_fast(const rs_geom* gc, const float* veff, const double* dij
         if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (pick == -1 && best == 0.f) { best = ms; pick = c; }
-        else if (ms < best) { best = ms; pick = c; }
+        if (best == 0.f || ms < best) {
+          best = ms;
+          pick = c;
+        }
       }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       if (e == cudaSuccess) g->nl_chunk = pick;
     }
   }
-  if (e == cudaSuccess) e = run(g->nl_chunk == 0 ? -1 : g->nl_chunk);
+  if (e == cudaSuccess) e = run(g->nl_chunk == 0 ? -NL_BANDS : g->nl_chunk);
   cudaFreeAsync(t, st);
   if (e != cudaSuccess) return cuda_status(e, "H psi (k_stencil_f32_zmarch, k_nl_rmw_f32)");
   return RS_OK;
@@ -668,7 +649,7 @@ int launch_spsi_f32_fast(const rs_geom* g, const double* sss, const double* rp, 
   if (e == cudaSuccess && g->n_cov > 0) {
     dim3 g2(div_up(g->n_cov, 128), div_up(nb, NL_BANDS));
     k_nl_rmw_f32<<<g2, 128, 0, st>>>(g->d_cov, g->d_cov_off, g->n_cov, g->d_inv_atom,
-                                      g->d_inv_v32, t, g->nprjmx, g->N, nb, out);
+                                      g->d_inv_v32, t, g->nprjmx, g->N, nb, nb, out);
     e = cudaGetLastError();
   }
   cudaFreeAsync(t, st);

@@ -82,8 +82,9 @@ struct rs_geom {
   size_t host_buf_bytes;
   // FP32 H psi: the nonlocal pass runs on nl_cs band chunk by band chunk
   // behind the stencil (nl_ev_in after a stencil chunk, nl_ev_out at its
-  // end); nl_chunk bands per chunk, 0 until the first large call has timed
-  // the candidates (nl_chunk < 0: one stencil launch, then one pass)
+  // end).  nl_chunk codes the chosen shape, 0 until the first large call has
+  // timed the candidates: chunk * 64 + bands per nonlocal thread, or minus
+  // the bands per thread for one stencil launch followed by one pass.
   cudaStream_t nl_cs;
   cudaEvent_t nl_ev_in, nl_ev_out;
   int nl_chunk;

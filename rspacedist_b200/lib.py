@@ -64,7 +64,7 @@ SIGNATURES = {
     "rs_nonlocal_apply_f64": [_p, _p, _p, _i, _p, _p],
     "rs_hpsi_f64": [_p, _p, _p, _p, _p, _p, _i, _p],
     "rs_hpsi_f32": [_p, _p, _p, _p, _p, _p, _i, _p],
-    "rs_hpsi_f32_tuning": [_p, _ip],
+    "rs_hpsi_f32_tuning": [_p, _ip, _ip],
     "rs_spsi_f64": [_p, _p, _p, _p, _p, _i, _p],
     "rs_spsi_f32": [_p, _p, _p, _p, _p, _i, _p],
     "rs_hpsi_host_f32": [_p, _p, _p, _p, _p, _p, _i, _i, _p],

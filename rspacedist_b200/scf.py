@@ -191,7 +191,7 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
             psi0=None, log=None, profile: bool = False, smearing: bool = True,
             tf: float = 3.0e-3, restart_dir: str | None = None,
             save_dir: str | None = None, potential: str = "kukan",
-            polish: bool = True) -> ScfResult:
+            polish: bool = True, start: str = "kukan") -> ScfResult:
     """kukan's SCF loop (kukan8f.F90:466-762) over the C ABI.
 
     potential: "kukan" (the dataset's local pseudopotential, setup_initialwave
@@ -206,7 +206,13 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
     write_rhovht do.
     polish: on the mixed path, finish with one FP64 orthonormalisation and
     Rayleigh-Ritz step of the converged bands (its time is part of the
-    loop's), so that eigenvalues and energies are FP64 quantities."""
+    loop's), so that eigenvalues and energies are FP64 quantities.
+    start: "kukan" (setup_initialwave's s and p orbitals) or "random" (seeded
+    smooth random bands, `seed`); the start density is the density of the
+    start bands either way.  RR + DIIS from the first iteration needs a start
+    whose span reaches the lowest states: with fewer bands than four per atom
+    kukan's orbitals leave out the p orbitals of the later atoms, and DIIS
+    then settles on high states (measured on Si512, 1100 bands)."""
     dev = torch.device("cuda")
     # the loop runs on a stream of its own (launches are stream-ordered there
     # and the Hartree solve can replay its iteration batches as CUDA graphs)
@@ -215,14 +221,14 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
     with torch.cuda.stream(side):
         res = _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, zval,
                        epsvh, vloc, rho0, psi0, log, profile, smearing, tf, restart_dir,
-                       save_dir, dev, potential, polish)
+                       save_dir, dev, potential, polish, start)
     side.synchronize()
     return res
 
 
 def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, zval, epsvh,
              vloc, rho0, psi0, log, profile, smearing, tf, restart_dir, save_dir, dev,
-             potential, polish):
+             potential, polish, start):
     from . import pseudo as PP
     if potential not in ("kukan", "model"):
         raise ValueError(f"potential must be 'kukan' or 'model', not {potential!r}")
@@ -240,8 +246,11 @@ def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, z
         rho_start = None if got is None else got[0]
         vh_start = CK.read_vht(restart_dir, shape)
     elif psi0 is not None:
-        psi = torch.as_tensor(np.ascontiguousarray(psi0), device=dev).to(dtype)
-    elif potential == "kukan":
+        if torch.is_tensor(psi0):
+            psi = psi0.to(device=dev, dtype=dtype).contiguous()
+        else:
+            psi = torch.as_tensor(np.ascontiguousarray(psi0), device=dev).to(dtype)
+    elif potential == "kukan" and start == "kukan":
         psi = PP.initial_bands(cell, M, dtype)
     else:
         psi = smooth_start_bands_device(shape, M, seed, dtype)
@@ -321,7 +330,8 @@ def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, z
         res.seconds_per_iter.append(time.perf_counter() - ti)
         res.iterations = iscf
         if log:
-            log(f"iscf {iscf:3d}  diff_charge {diff:.3e}  hartree_cg {it}  "
+            eb = float(np.dot(occ.cpu().numpy(), np.asarray(b.sval)))
+            log(f"iscf {iscf:3d}  diff_charge {diff:.3e}  hartree_cg {it}  eband {eb:.6f}  "
                 f"{res.seconds_per_iter[-1]:.3f} s")
         if diff < eps_scf:
             res.converged = True

@@ -49,9 +49,16 @@ def test_si64_nl_dot_and_hpsi(si64, oracle):
     assert np.array_equal(got, ref)
     rp32 = K.nonlocaloperation_01(g, T(psi, torch.float32)).cpu().numpy()
     np.testing.assert_allclose(rp32, rp, atol=1e-6 * np.abs(rp).max())
-    h32 = K.hpsi(g, T(si64["veff"], torch.float32), T(cell.dij), T(rp),
-                 T(psi, torch.float32)).cpu().numpy()
+    args = (g, T(si64["veff"], torch.float32), T(cell.dij), T(rp), T(psi, torch.float32))
+    h32 = K.hpsi(*args).cpu().numpy()  # the first call with >= 64 bands picks its launch shape
     assert np.abs(h32 - ref).max() <= 1e-5 * np.abs(ref).max()
+    import ctypes as C
+    from rspacedist_b200 import lib
+    chunk, nlb = C.c_int(0), C.c_int(0)
+    lib.call("rs_hpsi_f32_tuning", g.handle, C.byref(chunk), C.byref(nlb))
+    assert nlb.value in (16, 32) and (chunk.value == -1 or 4 <= chunk.value <= 64)
+    # every launch shape gives the same bits, so the tuned call equals the first
+    assert np.array_equal(K.hpsi(*args).cpu().numpy(), h32)
 
 
 def test_si64_rayleighritz(si64, oracle):
