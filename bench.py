@@ -220,11 +220,15 @@ def run_gpu(args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
+        if args.profile_range:
+            torch.cuda.cudart().cudaProfilerStart()
         ev0.record(stream)
         for _ in range(args.steps):
             step()
         ev1.record(stream)
         torch.cuda.synchronize()
+        if args.profile_range:
+            torch.cuda.cudart().cudaProfilerStop()
     ms = ev0.elapsed_time(ev1) / args.steps
     if world > 1:
         t = torch.tensor([ms], device=dev)
@@ -840,6 +844,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64-sweep", dest="fp64_sweep", action="store_false",
                     help="skip the plain FP64 sweep")
+    ap.add_argument("--profile-range", action="store_true",
+                    help="bracket the timed sweep steps with cudaProfilerStart/Stop (for "
+                         "ncu --profile-from-start off)")
     ap.add_argument("--bands", type=int, default=NB,
                     help="bands per sweep (default 1100; smaller values for profiling only)")
     ap.add_argument("--scf-loops", "--scf-iters", dest="scf_loops", type=int, default=200,

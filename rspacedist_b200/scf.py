@@ -168,6 +168,7 @@ class ScfResult:
     hartree_iters: list = field(default_factory=list)
     phase_seconds: dict = field(default_factory=dict)  # with profile=True only
     energy: dict = field(default_factory=dict)    # output_energy's terms (Ha)
+    energies: list = field(default_factory=list)  # free energy per iteration (when tracked)
     occ: np.ndarray | None = None                  # final occupations
 
 
@@ -191,7 +192,8 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
             psi0=None, log=None, profile: bool = False, smearing: bool = True,
             tf: float = 3.0e-3, restart_dir: str | None = None,
             save_dir: str | None = None, potential: str = "kukan",
-            polish: bool = True, start: str = "kukan") -> ScfResult:
+            polish: bool = True, start: str = "kukan",
+            eps_energy: float | None = None) -> ScfResult:
     """kukan's SCF loop (kukan8f.F90:466-762) over the C ABI.
 
     potential: "kukan" (the dataset's local pseudopotential, setup_initialwave
@@ -207,6 +209,9 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
     polish: on the mixed path, finish with one FP64 orthonormalisation and
     Rayleigh-Ritz step of the converged bands (its time is part of the
     loop's), so that eigenvalues and energies are FP64 quantities.
+    eps_energy: when given (Ha/atom), the loop also waits until the free
+    energy changed by less than eps_energy per atom over the last iteration
+    (kukan stops on diff_charge alone).
     start: "kukan" (setup_initialwave's s and p orbitals) or "random" (seeded
     smooth random bands, `seed`); the start density is the density of the
     start bands either way.  RR + DIIS from the first iteration needs a start
@@ -221,14 +226,14 @@ def run_scf(cell: Cell, M: int, nocc: int, dtype=torch.float64, eps_scf: float =
     with torch.cuda.stream(side):
         res = _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, zval,
                        epsvh, vloc, rho0, psi0, log, profile, smearing, tf, restart_dir,
-                       save_dir, dev, potential, polish, start)
+                       save_dir, dev, potential, polish, start, eps_energy)
     side.synchronize()
     return res
 
 
 def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, zval, epsvh,
              vloc, rho0, psi0, log, profile, smearing, tf, restart_dir, save_dir, dev,
-             potential, polish, start):
+             potential, polish, start, eps_energy):
     from . import pseudo as PP
     if potential not in ("kukan", "model"):
         raise ValueError(f"potential must be 'kukan' or 'model', not {potential!r}")
@@ -300,9 +305,24 @@ def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, z
         res.phase_seconds[name] = res.phase_seconds.get(name, 0.0) + now - t
         return now
 
+    eneat = PP.ion_energy(cell) if potential == "kukan" else 0.0
+    ddv = dvol / 8.0
+
+    def energy(occ_h, sval, rho_i, rho_d, vh_d, vx, ex_d):
+        # totalenergy_space / totalenergy_eig on an input density and its
+        # potentials (output8f.F90:240-242)
+        eneel = float(np.cumsum(occ_h * sval)[-1])
+        eneha = -0.5 * float(K.dot(vh_d, rho_d).item()) * ddv
+        eneex = -float(K.dot(rho_i, vx).item()) * dvol + float(K.dot(rho_d, ex_d).item()) * ddv
+        eneth = helmholtz_entropy(occ_h, tf) if smearing else 0.0
+        etot = eneel + eneex + eneha + eneat
+        return dict(eneel=eneel, eneex=eneex, eneha=eneha, eneat=eneat, eneth=eneth,
+                    total=etot, free=etot + eneth)
+
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     rho_d = vx = ex_d = None
+    e_prev = None
     for iscf in range(1, looplimit + 1):
         ti = time.perf_counter()
         tp = ti
@@ -329,11 +349,18 @@ def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, z
         res.hartree_iters.append(it)
         res.seconds_per_iter.append(time.perf_counter() - ti)
         res.iterations = iscf
+        e_now = None
+        if log or eps_energy is not None:
+            e_now = energy(occ.cpu().numpy(), np.asarray(b.sval), rho_i, rho_d, vh_d, vx,
+                           ex_d)["free"]
+            res.energies.append(e_now)
         if log:
-            eb = float(np.dot(occ.cpu().numpy(), np.asarray(b.sval)))
-            log(f"iscf {iscf:3d}  diff_charge {diff:.3e}  hartree_cg {it}  eband {eb:.6f}  "
-                f"{res.seconds_per_iter[-1]:.3f} s")
-        if diff < eps_scf:
+            log(f"iscf {iscf:3d}  diff_charge {diff:.3e}  hartree_cg {it}  free energy "
+                f"{e_now:.8f}  {res.seconds_per_iter[-1]:.3f} s")
+        e_ok = eps_energy is None or (e_prev is not None and
+                                      abs(e_now - e_prev) < eps_energy * cell.natom)
+        e_prev = e_now
+        if diff < eps_scf and e_ok:
             res.converged = True
             break
     if polish and dtype == torch.float32:
@@ -357,15 +384,7 @@ def _run_scf(cell, M, nocc, dtype, eps_scf, looplimit, prm, nbrydn, eta, seed, z
     occ_h = occ.cpu().numpy()
     res.occ = occ_h
     res.eband = float(np.cumsum(occ_h * res.sval)[-1])
-    # totalenergy_space on the last input density and its potentials
-    ddv = dvol / 8.0
-    eneha = -0.5 * float(K.dot(vh_d, rho_d).item()) * ddv
-    eneex = -float(K.dot(rho_i, vx).item()) * dvol + float(K.dot(rho_d, ex_d).item()) * ddv
-    eneat = PP.ion_energy(cell) if potential == "kukan" else 0.0
-    eneth = helmholtz_entropy(occ_h, tf) if smearing else 0.0
-    etot = res.eband + eneex + eneha + eneat
-    res.energy = dict(eneel=res.eband, eneex=eneex, eneha=eneha, eneat=eneat, eneth=eneth,
-                      total=etot, free=etot + eneth)
+    res.energy = energy(occ_h, res.sval, rho_i, rho_d, vh_d, vx, ex_d)
     if save_dir is not None:
         CK.write_wf(save_dir, b.psi, res.sval, shape)
         CK.write_rho(save_dir, rho_i, shape)
