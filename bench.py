@@ -59,11 +59,15 @@ def oracle_lists(atoms, rcut, nmax, h, npmax, nfdg, num_list):
             d["lstz"])
 
 
-# DRAM bytes (read + write) of one k_stencil_f32_zmarch launch on the Si512
-# grid per band: ncu dram__bytes_read.sum + dram__bytes_write.sum of a
-# 200-band launch, profiles/stencil_f32_zmarch_si512.md (see there for the
-# capture command and the per-launch figures).
-STENCIL_TRAFFIC_PER_BAND = (1905046016 + 1640433920) / 200
+# DRAM bytes (read + write) of one stencil launch on the Si512 grid per band:
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of a 200-band launch, from
+# the profile summary named beside it (capture command and per-launch figures
+# there); None where no capture exists.
+STENCIL_TRAFFIC_PER_BAND = {
+    "k_stencil_f32_zmarch": ((1905046016 + 1640433920) / 200,
+                             "profiles/stencil_f32_zmarch_si512.md"),
+    "k_stencil_f32_tma": (None, None),
+}
 
 
 def algorithmic_bytes(cell, nb, entries, s=4, s_p=4):
@@ -172,6 +176,16 @@ class ClockSampler:
                 "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
+def set_staging(g, staging, nb):
+    """Selects the FP32 stencil's plane staging on geometry g ("tma" or "cp");
+    True when nb-band calls run the TMA form."""
+    import ctypes as C
+    from rspacedist_b200 import lib as RL
+    tma = C.c_int(0)
+    RL.call("rs_hpsi_f32_staging", g.handle, 0 if staging == "tma" else 1, nb, C.byref(tma))
+    return bool(tma.value)
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -188,6 +202,8 @@ def run_gpu(args):
     t0 = time.time()
     cell = make_cell()
     g = K.Geometry(cell)
+    tma = set_staging(g, args.staging, args.bands)
+    stencil_kernel = "k_stencil_f32_tma" if tma else "k_stencil_f32_zmarch"
     log(f"[rank {rank}] set-up {time.time() - t0:.1f}s  entries={g.entries} "
         f"num_list={cell.num_list} natinf={int(cell.natinf.mean())}")
     from rspacedist_b200 import system as S
@@ -248,6 +264,7 @@ def run_gpu(args):
         shape=cell.shape, h=cell.h, natom=0, nprjmx=cell.nprjmx, num_list=1, N=cell.N,
         nprj=np.zeros(1, np.int32), natinf=np.zeros(1, np.int32), lst=np.zeros(1, np.int32),
         vnlocp=np.zeros(1)))
+    set_staging(g0, args.staging, nb)
     rp0 = torch.zeros(1, dtype=torch.float64, device=dev)
     for _ in range(args.warmup):
         K.hpsi(g0, veff, dij, rp0, psi, out=hpsi)
@@ -323,11 +340,13 @@ def run_gpu(args):
         sample = cpu_sample(cell)
         cpu = cpu_baseline(cell, sample)
         parity = check_parity(cell, g, dij, sample)
-    scf_out = None
+    scf_out = scf64_out = None
     if rank == 0 and world == 1 and args.scf_loops > 0:
         del psi, hpsi, rp
         torch.cuda.empty_cache()
         scf_out = run_scf_leg(cell, args.scf_loops)
+        scf64_out = run_scf_si64(args.scf_loops)
+    traffic_pb, traffic_src = STENCIL_TRAFFIC_PER_BAND[stencil_kernel]
     if rank == 0:
         out = {
             "metric": "Si512 H*psi sweep HBM GB/s (FP32 psi); SCF time to eps in 'scf'",
@@ -341,21 +360,21 @@ def run_gpu(args):
                        "projectors": cell.nprjmx, "inverse_entries": g.entries,
                        "l2": "inputs (9.2 GB psi) larger than L2; no flush",
                        "nl_band_chunk": nl_chunk, "nl_bands_per_thread": nlb.value,
+                       "stencil_staging": "tma" if tma else "cp.async",
                        "parallelism": f"bands replicated per GPU x{world}"},
             "band_points_per_s": round(nb * cell.N * world / (ms * 1e-3), 1),
-            "roofline": {"bound": "hbm", "kernel": "k_stencil_f32_zmarch",
+            "roofline": {"bound": "hbm", "kernel": stencil_kernel,
                          "achieved": round(st_gbs, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(st_gbs / peak, 4),
-                         "traffic": (round(STENCIL_TRAFFIC_PER_BAND * nb)
-                                     if STENCIL_TRAFFIC_PER_BAND else None),
-                         "traffic_source": "profiles/stencil_f32_zmarch_si512.md: ncu "
-                                           "dram__bytes_read.sum + dram__bytes_write.sum of "
-                                           "one 200-band launch, scaled by bands",
+                         "traffic": (round(traffic_pb * nb) if traffic_pb else None),
+                         "traffic_source": (f"{traffic_src}: ncu dram__bytes_read.sum + "
+                                            "dram__bytes_write.sum of one 200-band launch, "
+                                            "scaled by bands" if traffic_pb else None),
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": st_bytes,
                          "ms_per_launch": round(st_ms, 3)},
             "roofline_sweep": {"bound": "hbm",
-                               "kernels": "k_tcoef_f32, then k_stencil_f32_zmarch and "
+                               "kernels": f"k_tcoef_f32, then {stencil_kernel} and "
                                           "k_nl_rmw_f32 per band chunk",
                                "achieved": round(sweep_gbs, 1), "peak": peak, "unit": "GB/s",
                                "frac": round(sweep_gbs / peak, 4),
@@ -376,54 +395,61 @@ def run_gpu(args):
             out["fp64_sweep"] = fp64
         if scf_out:
             out["scf"] = scf_out
+        if scf64_out:
+            out["scf_si64"] = scf64_out
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
-def run_scf_leg(cell, looplimit, eps_scf=1e-6):
-    """The SCF half of the metric on the same Si512 cell: kukan's SCF
-    (local pseudopotential of the dataset, Broyden mixing eta 0.3, RR + DIIS
-    every iteration, Hartree CG, PZ LDA, Fermi-Dirac occupations for 2048
-    electrons in 1100 bands) from seeded smooth random bands to
-    diff_charge < eps_scf on the mixed path (FP32 bands) and on the plain FP64
-    path, each timed on the wall clock with the device synchronised, then the
-    total energies of output_energy."""
+SCF_EPS_CHARGE = 1e-6      # kukan's diff_charge stopping rule
+SCF_EPS_ENERGY = 2e-8      # Ha/atom change of the free energy over one iteration
+SCF_ETA, SCF_NBRYDN = 0.3, 40
+
+
+def run_scf_pair(cell, M, nocc, looplimit, ncgscf):
+    """kukan's SCF of `cell` on the mixed path (FP32 bands, FP64 polish) and
+    on the plain FP64 path from the same seeded smooth random bands, each
+    until diff_charge < SCF_EPS_CHARGE and the free energy changed by less
+    than SCF_EPS_ENERGY per atom over the last iteration.  The loop's wall
+    time is taken with the device synchronised; the set-up (local potential,
+    start bands, their orthonormalisation, the start density) is reported
+    apart."""
     import torch
     from rspacedist_b200 import lib, scf
-    prm = lib.solver_prm(ncgscf=0)
+    prm = lib.solver_prm(ncgscf=ncgscf)
     res = {}
     for name, dt in (("mixed", torch.float32), ("fp64", torch.float64)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r = scf.run_scf(cell, NB, 1024, dtype=dt, prm=prm, looplimit=looplimit, eta=0.3,
-                        eps_scf=eps_scf, profile=True, start="random", seed=0)
+        r = scf.run_scf(cell, M, nocc, dtype=dt, prm=prm, looplimit=looplimit, eta=SCF_ETA,
+                        nbrydn=SCF_NBRYDN, eps_scf=SCF_EPS_CHARGE, eps_energy=SCF_EPS_ENERGY,
+                        profile=True, start="random", seed=0)
         total = time.perf_counter() - t0
         r.bands = r.rho_out = None
         res[name] = (r, total)
         torch.cuda.empty_cache()
-        log(f"[scf] {name}: converged {r.converged} in {r.iterations} iterations, "
-            f"{r.seconds:.2f} s (+{total - r.seconds:.2f} s set-up); E {r.energy['total']:.8f}")
+        log(f"[scf] {cell.natom} atoms {name}: converged {r.converged} in {r.iterations} "
+            f"iterations, {r.seconds:.2f} s (+{total - r.seconds:.2f} s set-up); "
+            f"F {r.energy['free']:.8f}")
     (a, ta), (b, tb) = res["mixed"], res["fp64"]
-    nocc = 1024
     per_it = lambda r: r.seconds / max(1, r.iterations)
+    tail = lambda r: (abs(r.energies[-1] - r.energies[-2]) / cell.natom
+                      if len(r.energies) > 1 else None)
     return {
-        "workload": "Si512 SCF: 128^3 grid, 1100 bands (2048 electrons, Fermi-Dirac kT 3e-3 Ha), "
-                    "Si PAW projectors with the dataset's D and S (no one-centre update), the "
-                    "dataset's local pseudopotential (pseudocalc soft + hard parts), seeded "
-                    "smooth random start bands, Broyden mixing (eta 0.3, 20 steps), RR + DIIS "
-                    "every iteration, Hartree CG (epsvh 1e-12, at most 800 iterations) on the "
-                    "256^3 dense grid",
-        "eps_scf": eps_scf,
+        "eps": {"diff_charge": SCF_EPS_CHARGE,
+                "free_energy_change_ha_per_atom_per_iteration": SCF_EPS_ENERGY},
         "converged": {"mixed": a.converged, "fp64": b.converged},
         "iterations": {"mixed": a.iterations, "fp64": b.iterations},
         "time_to_eps_s": {"mixed": round(a.seconds, 2), "fp64": round(b.seconds, 2)},
         "setup_s": {"mixed": round(ta - a.seconds, 2), "fp64": round(tb - b.seconds, 2)},
         "speedup_time_to_eps_mixed_vs_fp64": round(b.seconds / a.seconds, 3),
         "s_per_iter": {"mixed": round(per_it(a), 3), "fp64": round(per_it(b), 3)},
+        "free_energy_ha": {"mixed": a.energy["free"], "fp64": b.energy["free"]},
         "etot_ha": {"mixed": a.energy["total"], "fp64": b.energy["total"]},
         "etot_diff_ha_per_atom": abs(a.energy["total"] - b.energy["total"]) / cell.natom,
         "free_energy_diff_ha_per_atom": abs(a.energy["free"] - b.energy["free"]) / cell.natom,
+        "last_step_change_ha_per_atom": {"mixed": tail(a), "fp64": tail(b)},
         "energy_terms_fp64": b.energy,
         "max_abs_occupied_eig_diff_ha": float(np.abs(np.sort(a.sval)[:nocc]
                                                      - np.sort(b.sval)[:nocc]).max()),
@@ -431,10 +457,42 @@ def run_scf_leg(cell, looplimit, eps_scf=1e-6):
         "fp64_phase_s": {k: round(v, 3) for k, v in b.phase_seconds.items()},
         "diff_charge_mixed": [float(f"{d:.3e}") for d in a.diff],
         "diff_charge_fp64": [float(f"{d:.3e}") for d in b.diff],
-        "timing": "wall clock of the SCF loop (iteration 1 to the stopping rule) with the "
-                  "device synchronised; set-up (local potential, initial bands, their "
-                  "orthonormalisation and the start density) reported apart",
+        "free_energy_mixed": [round(e, 8) for e in a.energies],
+        "free_energy_fp64": [round(e, 8) for e in b.energies],
+        "timing": "wall clock of the SCF loop (iteration 1 to the stopping rule, the mixed "
+                  "path's FP64 polish included) with the device synchronised",
     }
+
+
+def run_scf_leg(cell, looplimit):
+    """The SCF half of the metric on the Si512 cell of the sweep: kukan's SCF
+    (the dataset's local pseudopotential, Broyden mixing, RR + DIIS every
+    iteration, Hartree CG, PZ LDA, Fermi-Dirac occupations for 2048 electrons
+    in 1100 bands), mixed against plain FP64."""
+    out = {"workload": "Si512 SCF: 128^3 grid, 1100 bands (2048 electrons, Fermi-Dirac kT "
+                       "3e-3 Ha), Si PAW projectors with the dataset's D and S (no one-centre "
+                       "update), the dataset's local pseudopotential (pseudocalc soft + hard "
+                       f"parts), seeded smooth random start bands, Broyden mixing (eta {SCF_ETA},"
+                       f" {SCF_NBRYDN} steps), RR + DIIS every iteration, Hartree CG (epsvh "
+                       "1e-12, at most 800 iterations) on the 256^3 dense grid"}
+    out.update(run_scf_pair(cell, NB, 1024, looplimit, ncgscf=0))
+    return out
+
+
+def run_scf_si64(looplimit):
+    """The same comparison on the Si64 PAW cell (2x2x2 diamond, a = 20.52 bohr,
+    64^3 grid, 160 bands for 256 electrons, atoms displaced by sigma = 0.05
+    bohr from seed 1, DIIS after 3 CG steps)."""
+    from rspacedist_b200 import system as S
+    ds = S.load_dataset("si_paw")
+    cell = S.make_cell(2 * A_SI, 64, S.diamond_positions(2, A_SI, 0.05, 1), ds)
+    out = {"workload": "Si64 SCF: 64^3 grid, 160 bands (256 electrons, Fermi-Dirac kT 3e-3 Ha),"
+                       " sigma 0.05 bohr seed 1, Si PAW projectors with the dataset's D and S, "
+                       "the dataset's local pseudopotential, seeded smooth random start bands, "
+                       f"Broyden (eta {SCF_ETA}, {SCF_NBRYDN} steps), 3 CG steps then RR + DIIS,"
+                       " Hartree CG on the 128^3 dense grid"}
+    out.update(run_scf_pair(cell, 160, 128, looplimit, ncgscf=3))
+    return out
 
 
 def run_force_check(ncomp=6):
@@ -611,7 +669,8 @@ def run_reference(args):
 
 def run_diag_profile(dtype_name):
     """One scf_diag call (RR + DIIS) on the Si512 cell with 1100 smooth start
-    bands, run once to warm the memory pool and once more between
+    bands and the cell's local pseudopotential as the potential, run once to
+    warm the memory pool and once more between
     cudaProfilerStart/Stop, so that `ncu --profile-from-start off` lists the
     kernels of exactly one call.  Prints the wall time of the profiled call."""
     import torch
@@ -619,7 +678,8 @@ def run_diag_profile(dtype_name):
     cell = make_cell()
     g = K.Geometry(cell)
     dt = torch.float32 if dtype_name == "f32" else torch.float64
-    veff = torch.tensor(scf.model_local_potential(cell), device="cuda").to(dt)
+    from rspacedist_b200 import pseudo
+    veff = pseudo.local_potential(cell)[0].to(dt)
     dij = torch.tensor(cell.dij, device="cuda")
     sss = torch.tensor(cell.sss, device="cuda")
     b = K.Bands(g, scf.smooth_start_bands_device(cell.shape, NB, 0, dt), sss)
@@ -847,9 +907,11 @@ def main():
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed sweep steps with cudaProfilerStart/Stop (for "
                          "ncu --profile-from-start off)")
+    ap.add_argument("--staging", choices=["tma", "cp"], default="tma",
+                    help="plane staging of the FP32 stencil: tensor-map loads or cp.async")
     ap.add_argument("--bands", type=int, default=NB,
                     help="bands per sweep (default 1100; smaller values for profiling only)")
-    ap.add_argument("--scf-loops", "--scf-iters", dest="scf_loops", type=int, default=200,
+    ap.add_argument("--scf-loops", "--scf-iters", dest="scf_loops", type=int, default=300,
                     help="iteration limit of the Si512 SCF run per path (0 skips the leg)")
     ap.add_argument("--force-check", action="store_true",
                     help="run the Si64 force check (adjoint vs energy differences) and exit")

@@ -112,6 +112,14 @@ int rs_nonlocal_apply_f64(const rs_geom* g, const double* mat, const double* rp,
  * counterpart in the reference. */
 int rs_hpsi_f32_tuning(const rs_geom* g, int* nl_chunk, int* nl_bands);
 
+/* How the FP32 stencil of g stages its planes: mode 0 (the default) copies
+ * them with tensor-map (TMA) loads where nx is 64, 128 or 256 and ny a
+ * multiple of 2048/nx, mode 1 with per-thread cp.async; mode < 0 keeps the
+ * current mode.  *tma is set to 1 when an nb-band call would take the TMA
+ * form.  Both forms give identical results.  No counterpart in the
+ * reference. */
+int rs_hpsi_f32_staging(rs_geom* g, int mode, int nb, int* tma);
+
 /* Fused H psi = nonlocal(D) + stencil + veff, one pass over psi (the H*psi of
  * kscg8f.F90:147-183 and rayleighritz_hamiltonian_r, rayleigh-ritz8f.F90:493-575).
  * hpsi(dev) is overwritten. */

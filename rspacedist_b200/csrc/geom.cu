@@ -165,6 +165,7 @@ extern "C" int rs_geom_destroy(rs_geom* g) {
   if (g->nl_cs) cudaStreamDestroy(g->nl_cs);
   if (g->nl_ev_in) cudaEventDestroy(g->nl_ev_in);
   if (g->nl_ev_out) cudaEventDestroy(g->nl_ev_out);
+  if (g->st_err_h) cudaFreeHost(g->st_err_h);
   delete g;
   return RS_OK;
 }

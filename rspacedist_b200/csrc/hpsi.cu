@@ -11,6 +11,7 @@ int launch_hpsi_f32_fast(const rs_geom* g, const float* veff, const double* dij,
                          const double* rp, const float* psi, float* hpsi, int nb,
                          cudaStream_t st, bool local_only = false);
 int hpsi_f32_nl_chunk(const rs_geom* g);
+int hpsi_f32_staging(rs_geom* g, int mode, int nb, int* tma);
 }  // namespace rs
 
 extern "C" int rs_hpsi_f32_tuning(const rs_geom* g, int* nl_chunk, int* nl_bands) {
@@ -19,6 +20,11 @@ extern "C" int rs_hpsi_f32_tuning(const rs_geom* g, int* nl_chunk, int* nl_bands
   *nl_chunk = code > 0 ? code / 64 : (code < 0 ? -1 : 0);
   *nl_bands = code > 0 ? code % 64 : (code < 0 ? -code : 0);
   return RS_OK;
+}
+
+extern "C" int rs_hpsi_f32_staging(rs_geom* g, int mode, int nb, int* tma) {
+  if (!g || !tma) return rs::fail(RS_EINVAL, "rs_hpsi_f32_staging: null argument");
+  return rs::hpsi_f32_staging(g, mode, nb, tma);
 }
 
 extern "C" int rs_hpsi_f32(const rs_geom* g, const float* veff, const double* dij,

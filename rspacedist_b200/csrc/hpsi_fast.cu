@@ -16,10 +16,14 @@
 //    projector support (a fraction of the grid).  A thread owns one such
 //    point and a block of 16 bands: it loads the point's projector entries
 //    once and adds sum_e sum_j t[atom_e][b][j] p_e[j] to 16 bands of hpsi.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 
 #include "rs_common.cuh"
 #include "stencil.cuh"
+#include "tc_ptx.cuh"
 
 namespace rs {
 
@@ -251,6 +255,244 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// k_stencil_f32_tma: the same operator and the same FMA order per point as
+// k_stencil_f32_zmarch<false> (so bit-identical results), with the planes
+// staged by the tensor-memory accelerator instead of per-thread cp.async.
+// A tile is TYT whole rows of a plane (all NXT points of x, NXT * TYT = 2048
+// points, 256 threads of 4 x 2 points), so the x halo is the tile's own row
+// (periodic x wraps inside shared memory) and only the y halo is extra: one
+// plane of a tile is three 2-D tensor loads of whole rows -- 4 halo rows
+// above, the TYT own rows, 4 halo rows below, the halo rows wrapped
+// periodically in y -- issued by one thread and counted in bytes on the
+// slot's mbarrier.  Bands and z planes are rows of the tensor map too (rows
+// of all bands, planes and y, NXT floats each), so z wraps by the row index.
+// Every mbarrier wait is bounded; a wait that gives up raises *err (a
+// host-mapped flag) and the CTA waits, again bounded, for the copies it
+// issued before it returns.
+constexpr int TRING = 8;   // staged planes
+constexpr int TAHEAD = 3;  // planes in flight beyond the newest plane the queue reads
+
+template <int NXT>
+struct TmaTile {
+  static constexpr int TYT = 2048 / NXT;   // own rows of a tile
+  static constexpr int NTX = NXT / 4;
+  static constexpr int ROWS = TYT + 8;     // with the two 4-row halos
+  static constexpr int SLOT = ROWS * NXT;  // floats per staged plane
+  static constexpr size_t SMEM = sizeof(float) * TRING * SLOT;
+};
+
+struct TmaArgs {
+  int ny, nz, zchunk;
+  float cx[5], cy[5], cz[5], c0;
+  const float* psi;  // band 0 of the launch (also the tensor maps' base)
+  float* out;
+  const float* veff;
+  int* err;
+};
+
+// Set by a CTA whose staging wait gave up: the CTAs that start after it
+// return at once (so a broken launch ends within a few wait limits), and the
+// host clears it when it reports the error.
+__device__ int g_st_abort;
+constexpr unsigned long long kStageWaitNs = 250000000ull;  // 0.25 s per wait
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// true once the phase of `parity` has completed; false after kStageWaitNs
+// (or tc::kSpinLimit polls)
+__device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity) {
+  if (tc::mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (long long i = 0; i < tc::kSpinLimit; ++i) {
+    if (tc::mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > kStageWaitNs) break;
+  }
+  return false;
+}
+__device__ __forceinline__ void raise_stage_error(int* err) {
+  atomicExch(&g_st_abort, 1);
+  *reinterpret_cast<volatile int*>(err) = 1;
+  __threadfence_system();
+}
+
+__device__ __forceinline__ void tma_rows(float* dst, const CUtensorMap* map, int row,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];\n" ::"r"(tc::smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(row), "r"(tc::smem_u32(bar))
+      : "memory");
+}
+
+template <int NXT>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    k_stencil_f32_tma(const __grid_constant__ CUtensorMap core,
+                      const __grid_constant__ CUtensorMap halo, TmaArgs a) {
+  using T = TmaTile<NXT>;
+  extern __shared__ __align__(1024) float tring[];  // [TRING][ROWS][NXT]
+  __shared__ __align__(8) uint64_t full[TRING];
+  __shared__ int s_abort;
+  const int tid = threadIdx.x;
+  const int tx = tid % T::NTX, ty = tid / T::NTX;
+  const int ny = a.ny, nz = a.nz;
+  const int nyt = ny / T::TYT;
+  const int tile = blockIdx.x % nyt;
+  const int zc = blockIdx.x / nyt;
+  const int band = blockIdx.y;
+  const int y0 = tile * T::TYT;
+  const long plane = (long)NXT * ny;
+  const long N = plane * nz;
+  const float* psi = a.psi + (long)band * N;
+  float* out = a.out + (long)band * N;
+  const int zs = zc * a.zchunk;
+  const int ze = min(zs + a.zchunk, nz);
+  const int last = ze + 3;  // newest plane the march reads
+  const int gx = 4 * tx, gy = y0 + 2 * ty;
+  const long own0 = (long)gy * NXT + gx, own1 = own0 + NXT;
+  const int ly = 2 * ty + 4;
+  const int lxm = gx >= 4 ? gx - 4 : gx - 4 + NXT;   // x - 4 .. x - 1, periodic
+  const int lxp = gx + 4 < NXT ? gx + 4 : gx + 4 - NXT;
+  const int ytop = y0 >= 4 ? y0 - 4 : y0 - 4 + ny;
+  const int ybot = y0 + T::TYT < ny ? y0 + T::TYT : y0 + T::TYT - ny;
+  const int prow = band * nz;  // this band's first plane in the maps' rows / ny
+
+  if (tid == 0) {
+    // an earlier CTA gave up: leave at once (one read, so the CTA agrees)
+    s_abort = *reinterpret_cast<volatile int*>(&g_st_abort);
+    if (!s_abort) {
+      for (int s = 0; s < TRING; ++s) tc::mbar_init(&full[s], 1);
+      tc::fence_mbar_init();
+    }
+  }
+  __syncthreads();
+  if (s_abort) {
+    if (tid == 0) raise_stage_error(a.err);
+    return;
+  }
+  // thread 0: stage plane p (zs <= p <= last) into slot p % TRING
+  auto stage = [&](int p) {
+    const int s = p & (TRING - 1);
+    float* dst = tring + s * T::SLOT;
+    const int r0 = (prow + (p < nz ? p : p - nz)) * ny;
+    tc::mbar_arrive_expect_tx(&full[s], (uint32_t)(T::SLOT * sizeof(float)));
+    tma_rows(dst, &halo, r0 + ytop, &full[s]);
+    tma_rows(dst + 4 * NXT, &core, r0 + y0, &full[s]);
+    tma_rows(dst + (T::TYT + 4) * NXT, &halo, r0 + ybot, &full[s]);
+  };
+  auto parity = [&](int p) { return (uint32_t)(((p - zs) >> 3) & 1); };
+  int issued = zs - 1;
+  if (tid == 0) {
+    for (int p = zs; p <= min(zs + 3 + TAHEAD, last); ++p) stage(p);
+    issued = min(zs + 3 + TAHEAD, last);
+  }
+
+  float4 q[9][2];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int z = zs - 4 + k;
+    const float* pp = psi + (long)(z < 0 ? z + nz : z) * plane;
+    q[k][0] = ld4(pp + own0);
+    q[k][1] = ld4(pp + own1);
+  }
+  bool ok = true;
+#pragma unroll
+  for (int k = 4; k < 8; ++k) {
+    const int p = zs + k - 4;
+    ok = ok && stage_wait(&full[p & (TRING - 1)], parity(p));
+    const float* sl = tring + (p & (TRING - 1)) * T::SLOT;
+    q[k][0] = *reinterpret_cast<const float4*>(sl + ly * NXT + gx);
+    q[k][1] = *reinterpret_cast<const float4*>(sl + (ly + 1) * NXT + gx);
+  }
+  if (!ok) s_abort = 1;
+  float4 vreg[2];
+  vreg[0] = ld4(a.veff + (long)zs * plane + own0);
+  vreg[1] = ld4(a.veff + (long)zs * plane + own1);
+
+  for (int z = zs; z < ze; ++z) {
+    if (tid == 0 && z + 4 + TAHEAD <= last) {
+      // the slot of plane z - 1, whose last reads ended at the barrier below
+      tc::fence_async_smem();
+      stage(z + 4 + TAHEAD);
+      issued = z + 4 + TAHEAD;
+    }
+    const int pn = z + 4;
+    if (!stage_wait(&full[pn & (TRING - 1)], parity(pn))) s_abort = 1;
+    const float* cur = tring + (z & (TRING - 1)) * T::SLOT;
+    {
+      const float* nw = tring + (pn & (TRING - 1)) * T::SLOT;
+      q[8][0] = *reinterpret_cast<const float4*>(nw + ly * NXT + gx);
+      q[8][1] = *reinterpret_cast<const float4*>(nw + (ly + 1) * NXT + gx);
+    }
+    const float4 vcur[2] = {vreg[0], vreg[1]};
+    if (z + 1 < ze) {
+      vreg[0] = ld4(a.veff + (long)(z + 1) * plane + own0);
+      vreg[1] = ld4(a.veff + (long)(z + 1) * plane + own1);
+    }
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+      const float* row = cur + (ly + rr) * NXT;
+      const float4 L = *reinterpret_cast<const float4*>(row + lxm);
+      const float4 R = *reinterpret_cast<const float4*>(row + lxp);
+      const float4 C = q[4][rr];
+      const float xv[12] = {L.x, L.y, L.z, L.w, C.x, C.y, C.z, C.w, R.x, R.y, R.z, R.w};
+      const float vv[4] = {vcur[rr].x, vcur[rr].y, vcur[rr].z, vcur[rr].w};
+      float acc[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        float s = a.cx[4] * xv[i];
+        s = fmaf(a.cx[3], xv[i + 1], s);
+        s = fmaf(a.cx[2], xv[i + 2], s);
+        s = fmaf(a.cx[1], xv[i + 3], s);
+        s = fmaf(a.c0 + vv[i], xv[i + 4], s);
+        s = fmaf(a.cx[1], xv[i + 5], s);
+        s = fmaf(a.cx[2], xv[i + 6], s);
+        s = fmaf(a.cx[3], xv[i + 7], s);
+        s = fmaf(a.cx[4], xv[i + 8], s);
+        acc[i] = s;
+      }
+#pragma unroll
+      for (int m = 4; m >= 1; --m) {
+        const int yy = rr - m;
+        const float4 v =
+            yy == 0 ? q[4][0] : *reinterpret_cast<const float4*>(cur + (ly + yy) * NXT + gx);
+        fma4(a.cy[m], v, acc);
+      }
+#pragma unroll
+      for (int m = 1; m <= 4; ++m) {
+        const int yy = rr + m;
+        const float4 v =
+            yy == 1 ? q[4][1] : *reinterpret_cast<const float4*>(cur + (ly + yy) * NXT + gx);
+        fma4(a.cy[m], v, acc);
+      }
+#pragma unroll
+      for (int m = 4; m >= 1; --m) fma4(a.cz[m], q[4 - m][rr], acc);
+#pragma unroll
+      for (int m = 1; m <= 4; ++m) fma4(a.cz[m], q[4 + m][rr], acc);
+      *reinterpret_cast<float4*>(out + (long)z * plane + (rr ? own1 : own0)) =
+          make_float4(acc[0], acc[1], acc[2], acc[3]);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      q[k][0] = q[k + 1][0];
+      q[k][1] = q[k + 1][1];
+    }
+    __syncthreads();
+    if (s_abort) break;
+  }
+  if (s_abort && tid == 0) {
+    // wind down: let the copies still in flight land before the CTA exits
+    // (the newest TRING planes staged; older slots were reused, so their
+    // phases are gone)
+    for (int p = max(zs, issued - TRING + 1); p <= issued; ++p)
+      stage_wait(&full[p & (TRING - 1)], parity(p));
+    raise_stage_error(a.err);
+  }
+}
+
 // t coefficients in atom-major order t[a][b][i] = (sum_j rp[b][a][j] m[a][i][j]) / dV
 // (FP64 sum, stored FP32), so that one atom's coefficients for a block of
 // bands are contiguous.
@@ -429,14 +671,107 @@ void stencil_args(const rs_geom* g, const float* veff, StArgs& a) {
   a.part = nullptr;
 }
 
+using EncodeTiled = PFN_cuTensorMapEncodeTiled_v12000;
+
+// cuTensorMapEncodeTiled from the driver the runtime loaded (null if absent)
+EncodeTiled tensor_map_encoder() {
+  static const EncodeTiled fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeTiled>(p);
+  }();
+  return fn;
+}
+
+// the TMA form takes nx = 64, 128 or 256 (tiles of 32, 16 or 8 whole rows)
+// with ny a multiple of the tile height, and row indices of n bands that fit
+// in 32 bits
+bool stencil_tma_shape(const rs_geom* g, int n) {
+  const int nx = g->nx;
+  if (nx != 64 && nx != 128 && nx != 256) return false;
+  const int tyt = 2048 / nx;
+  return g->ny % tyt == 0 && (long)n * g->nz * g->ny < (1L << 31);
+}
+
+// n bands of nx floats per row, ny * nz rows per band, boxes of `rows` rows
+cudaError_t encode_rows(CUtensorMap* m, const float* base, int nx, long nrows, int rows) {
+  const cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)nrows};
+  const cuuint64_t strides[1] = {(cuuint64_t)nx * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)nx, (cuuint32_t)rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = tensor_map_encoder()(
+      m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, estr,
+      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <int NXT>
+cudaError_t launch_stencil_tma(rs_geom* g, const StArgs& sa, const float* psi, float* out, int n,
+                               cudaStream_t st) {
+  using T = TmaTile<NXT>;
+  cudaError_t e = cudaFuncSetAttribute(k_stencil_f32_tma<NXT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+  if (e != cudaSuccess) return e;
+  CUtensorMap core, halo;
+  const long nrows = (long)n * g->nz * g->ny;
+  e = encode_rows(&core, psi, NXT, nrows, T::TYT);
+  if (e == cudaSuccess) e = encode_rows(&halo, psi, NXT, nrows, 4);
+  if (e != cudaSuccess) return e;
+  TmaArgs a;
+  a.ny = g->ny; a.nz = g->nz; a.zchunk = sa.zchunk;
+  for (int m = 0; m < 5; ++m) { a.cx[m] = sa.cx[m]; a.cy[m] = sa.cy[m]; a.cz[m] = sa.cz[m]; }
+  a.c0 = sa.c0;
+  a.psi = psi; a.out = out; a.veff = sa.veff;
+  a.err = g->st_err_d;
+  const int nzc = (g->nz + a.zchunk - 1) / a.zchunk;
+  dim3 grid((g->ny / T::TYT) * nzc, n);
+  k_stencil_f32_tma<NXT><<<grid, NTHREADS, T::SMEM, st>>>(core, halo, a);
+  return cudaGetLastError();
+}
+
+// true when the stencil of n bands runs the TMA form; allocates its error
+// flag on first use (never inside a stream capture)
+bool use_stencil_tma(rs_geom* g, int n, cudaStream_t st) {
+  if (g->st_copy != 0 || !stencil_tma_shape(g, n) || !tensor_map_encoder()) return false;
+  if (!g->st_err_h) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs != cudaStreamCaptureStatusNone) return false;
+    int* h = nullptr;
+    if (cudaHostAlloc((void**)&h, sizeof(int), cudaHostAllocMapped) != cudaSuccess) return false;
+    *h = 0;
+    int* d = nullptr;
+    if (cudaHostGetDevicePointer((void**)&d, h, 0) != cudaSuccess) {
+      cudaFreeHost(h);
+      return false;
+    }
+    g->st_err_h = h;
+    g->st_err_d = d;
+  }
+  return true;
+}
+
 // stencil of bands [b0, b0 + n) on st
-void launch_stencil(const rs_geom* g, StArgs a, const float* psi, float* hpsi, int b0, int n,
-                    cudaStream_t st) {
+cudaError_t launch_stencil(rs_geom* g, StArgs a, const float* psi, float* hpsi, int b0, int n,
+                           cudaStream_t st) {
   a.psi = psi + (long)b0 * g->N;
   a.out = hpsi + (long)b0 * g->N;
+  if (use_stencil_tma(g, n, st)) {
+    switch (g->nx) {
+      case 64: return launch_stencil_tma<64>(g, a, a.psi, a.out, n, st);
+      case 128: return launch_stencil_tma<128>(g, a, a.psi, a.out, n, st);
+      default: return launch_stencil_tma<256>(g, a, a.psi, a.out, n, st);
+    }
+  }
   const int nzc = (g->nz + a.zchunk - 1) / a.zchunk;
   dim3 grid(a.ntx * a.nty * nzc, n);
   k_stencil_f32_zmarch<false><<<grid, NTHREADS, sizeof(float) * RING * HY * HX, st>>>(a);
+  return cudaGetLastError();
 }
 
 // nonlocal pass of bands [b0, b0 + n) (t holds all nb bands' coefficients),
@@ -483,9 +818,17 @@ int launch_hpsi_f32_fast(const rs_geom* gc, const float* veff, const double* dij
   RS_CUDA(cudaFuncSetAttribute(k_stencil_f32_zmarch<false>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)(sizeof(float) * RING * HY * HX)));
+  if (g->st_err_h && *reinterpret_cast<volatile int*>(g->st_err_h)) {
+    // raised by an earlier call on this geometry: report it once, clear it
+    *g->st_err_h = 0;
+    const int zero = 0;
+    cudaMemcpyToSymbolAsync(g_st_abort, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+    return fail(RS_ECUDA, "H psi: a plane-staging wait of k_stencil_f32_tma timed out");
+  }
   if (local_only || g->natom == 0 || g->n_cov == 0) {
-    launch_stencil(g, a, psi, hpsi, 0, nb, st);
-    RS_LAUNCH_CHECK("k_stencil_f32_zmarch");
+    const cudaError_t e = launch_stencil(g, a, psi, hpsi, 0, nb, st);
+    if (e != cudaSuccess) return cuda_status(e, "k_stencil_f32 (H psi local part)");
     return RS_OK;
   }
   const long nt = (long)nb * g->natom * g->nprjmx;
@@ -504,7 +847,8 @@ int launch_hpsi_f32_fast(const rs_geom* gc, const float* veff, const double* dij
     const int chunk = code >= 0 ? code / 64 : -1;
     const int nlb = code >= 0 ? code % 64 : (-code) % 64;
     if (chunk <= 0 || chunk >= nb) {
-      launch_stencil(g, a, psi, hpsi, 0, nb, st);
+      const cudaError_t e = launch_stencil(g, a, psi, hpsi, 0, nb, st);
+      if (e != cudaSuccess) return e;
       launch_nl(g, t, hpsi, 0, nb, nb, nlb, st);
       return cudaGetLastError();
     }
@@ -514,7 +858,8 @@ int launch_hpsi_f32_fast(const rs_geom* gc, const float* veff, const double* dij
     if (chunk <= 16 && g->nz > 64) ac.zchunk = 32;
     for (int b0 = 0; b0 < nb; b0 += chunk) {
       const int n = std::min(chunk, nb - b0);
-      launch_stencil(g, ac, psi, hpsi, b0, n, st);
+      const cudaError_t e = launch_stencil(g, ac, psi, hpsi, b0, n, st);
+      if (e != cudaSuccess) return e;
       cudaEventRecord(g->nl_ev_in, st);
       cudaStreamWaitEvent(g->nl_cs, g->nl_ev_in, 0);
       launch_nl(g, t, hpsi, b0, n, nb, nlb, g->nl_cs);
@@ -557,13 +902,24 @@ int launch_hpsi_f32_fast(const rs_geom* gc, const float* veff, const double* dij
   }
   if (e == cudaSuccess) e = run(g->nl_chunk == 0 ? -NL_BANDS : g->nl_chunk);
   cudaFreeAsync(t, st);
-  if (e != cudaSuccess) return cuda_status(e, "H psi (k_stencil_f32_zmarch, k_nl_rmw_f32)");
+  if (e != cudaSuccess) return cuda_status(e, "H psi (k_stencil_f32, k_nl_rmw_f32)");
   return RS_OK;
 }
 
 // the band-chunk size the FP32 H psi of this geometry picked (0: not yet
 // chosen, -1: unchunked)
 int hpsi_f32_nl_chunk(const rs_geom* g) { return g->nl_chunk; }
+
+// staging of the FP32 stencil: mode 0 = TMA where the grid allows it, 1 =
+// cp.async (mode < 0 leaves it); *tma = 1 when a call of nb bands would run
+// the TMA form
+int hpsi_f32_staging(rs_geom* g, int mode, int nb, int* tma) {
+  if (mode > 1) return fail(RS_EINVAL, "rs_hpsi_f32_staging: mode must be 0 or 1");
+  if (mode >= 0) g->st_copy = mode;
+  *tma = (g->st_copy == 0 && stencil_tma_shape(g, nb) && hpsi_f32_fast_ok(g, nb) &&
+          tensor_map_encoder() != nullptr) ? 1 : 0;
+  return RS_OK;
+}
 
 // A p of the mixed Hartree CG (nfh = 4) by the H psi z-march: coefficients
 // cx, cy, cz [1..4] and diag from hartree_coefs, runs of 32 z planes (so one

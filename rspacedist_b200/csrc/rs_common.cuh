@@ -88,6 +88,12 @@ struct rs_geom {
   cudaStream_t nl_cs;
   cudaEvent_t nl_ev_in, nl_ev_out;
   int nl_chunk;
+  // FP32 stencil staging: 0 = tensor-map (TMA) loads where the grid allows
+  // them, 1 = per-thread cp.async; st_err_h/_d: host-mapped flag that a
+  // bounded wait of the TMA form raises (allocated by its first launch)
+  int st_copy;
+  int* st_err_h;
+  int* st_err_d;
 };
 
 namespace rs {

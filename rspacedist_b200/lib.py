@@ -65,6 +65,7 @@ SIGNATURES = {
     "rs_hpsi_f64": [_p, _p, _p, _p, _p, _p, _i, _p],
     "rs_hpsi_f32": [_p, _p, _p, _p, _p, _p, _i, _p],
     "rs_hpsi_f32_tuning": [_p, _ip, _ip],
+    "rs_hpsi_f32_staging": [_p, _i, _i, _ip],
     "rs_spsi_f64": [_p, _p, _p, _p, _p, _i, _p],
     "rs_spsi_f32": [_p, _p, _p, _p, _p, _i, _p],
     "rs_hpsi_host_f32": [_p, _p, _p, _p, _p, _p, _i, _i, _p],
