@@ -66,7 +66,8 @@ def oracle_lists(atoms, rcut, nmax, h, npmax, nfdg, num_list):
 STENCIL_TRAFFIC_PER_BAND = {
     "k_stencil_f32_zmarch": ((1905046016 + 1640433920) / 200,
                              "profiles/stencil_f32_zmarch_si512.md"),
-    "k_stencil_f32_tma": (None, None),
+    "k_stencil_f32_tma": ((1842567936 + 1636464384) / 200,
+                          "profiles/stencil_f32_tma_si512.md"),
 }
 
 
@@ -182,7 +183,8 @@ def set_staging(g, staging, nb):
     import ctypes as C
     from rspacedist_b200 import lib as RL
     tma = C.c_int(0)
-    RL.call("rs_hpsi_f32_staging", g.handle, 0 if staging == "tma" else 1, nb, C.byref(tma))
+    mode = {"tma": 0, "cp": 1}[staging]
+    RL.call("rs_hpsi_f32_staging", g.handle, mode, nb, C.byref(tma))
     return bool(tma.value)
 
 
@@ -236,14 +238,14 @@ def run_gpu(args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
-        if args.profile_range:
+        if args.profile_range == "sweep":
             torch.cuda.cudart().cudaProfilerStart()
         ev0.record(stream)
         for _ in range(args.steps):
             step()
         ev1.record(stream)
         torch.cuda.synchronize()
-        if args.profile_range:
+        if args.profile_range == "sweep":
             torch.cuda.cudart().cudaProfilerStop()
     ms = ev0.elapsed_time(ev1) / args.steps
     if world > 1:
@@ -272,11 +274,15 @@ def run_gpu(args):
     if world > 1:
         dist.barrier()
     es0, es1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.profile_range == "stencil":
+        torch.cuda.cudart().cudaProfilerStart()
     es0.record(stream)
     for _ in range(args.steps):
         K.hpsi(g0, veff, dij, rp0, psi, out=hpsi)
     es1.record(stream)
     torch.cuda.synchronize()
+    if args.profile_range == "stencil":
+        torch.cuda.cudart().cudaProfilerStop()
     st_ms = es0.elapsed_time(es1) / args.steps
     if world > 1:
         t = torch.tensor([st_ms], device=dev)
@@ -904,9 +910,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64-sweep", dest="fp64_sweep", action="store_false",
                     help="skip the plain FP64 sweep")
-    ap.add_argument("--profile-range", action="store_true",
-                    help="bracket the timed sweep steps with cudaProfilerStart/Stop (for "
-                         "ncu --profile-from-start off)")
+    ap.add_argument("--profile-range", choices=["sweep", "stencil"],
+                    help="bracket the timed sweep steps (sweep) or the timed stencil-only "
+                         "launches (stencil) with cudaProfilerStart/Stop, for ncu "
+                         "--profile-from-start off")
     ap.add_argument("--staging", choices=["tma", "cp"], default="tma",
                     help="plane staging of the FP32 stencil: tensor-map loads or cp.async")
     ap.add_argument("--bands", type=int, default=NB,

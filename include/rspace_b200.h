@@ -114,9 +114,10 @@ int rs_hpsi_f32_tuning(const rs_geom* g, int* nl_chunk, int* nl_bands);
 
 /* How the FP32 stencil of g stages its planes: mode 0 (the default) copies
  * them with tensor-map (TMA) loads where nx is 64, 128 or 256 and ny a
- * multiple of 2048/nx, mode 1 with per-thread cp.async; mode < 0 keeps the
- * current mode.  *tma is set to 1 when an nb-band call would take the TMA
- * form.  Both forms give identical results.  No counterpart in the
+ * multiple of 2048/nx (k_stencil_f32_tma), mode 1 with per-thread cp.async
+ * (k_stencil_f32_zmarch, also the form for every other grid); mode < 0 keeps
+ * the current mode.  *tma is set to 1 when an nb-band call would take the
+ * TMA form.  Both forms give identical results.  No counterpart in the
  * reference. */
 int rs_hpsi_f32_staging(rs_geom* g, int mode, int nb, int* tma);
 

@@ -167,6 +167,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
   }
   double pacc = 0.0;  // Hartree form: p . A p over this thread's points
 
+  // the H psi form is unrolled by the queue length, so the queue rotates by
+  // renaming
+#pragma unroll(HARTREE ? 1 : 9)
   for (int z = zs; z < ze; ++z) {
     stage(z + 4 + AHEAD);   // reuses the slot of plane z-1 (freed by the last sync)
     cp_wait<AHEAD>();       // this thread's copies of plane z+4 have landed
@@ -203,24 +206,28 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
           s = fmaf(a.cx[4], xv[i + 8], s);
           acc[i] = s;
         }
+        // y and z terms as packed pair FMAs (each lane the scalar fma)
+        float2 lo = make_float2(acc[0], acc[1]), hi = make_float2(acc[2], acc[3]);
+        auto f2 = [&](const float c, const float4& v) {
+          const float2 cc = make_float2(c, c);
+          lo = __ffma2_rn(cc, make_float2(v.x, v.y), lo);
+          hi = __ffma2_rn(cc, make_float2(v.z, v.w), hi);
+        };
 #pragma unroll
         for (int m = 4; m >= 1; --m) {
           const int yy = rr - m;
-          const float4 v =
-              yy == 0 ? q[4][0] : *reinterpret_cast<const float4*>(&cur[ly + yy][lx]);
-          fma4(a.cy[m], v, acc);
+          f2(a.cy[m], yy == 0 ? q[4][0] : *reinterpret_cast<const float4*>(&cur[ly + yy][lx]));
         }
 #pragma unroll
         for (int m = 1; m <= 4; ++m) {
           const int yy = rr + m;
-          const float4 v =
-              yy == 1 ? q[4][1] : *reinterpret_cast<const float4*>(&cur[ly + yy][lx]);
-          fma4(a.cy[m], v, acc);
+          f2(a.cy[m], yy == 1 ? q[4][1] : *reinterpret_cast<const float4*>(&cur[ly + yy][lx]));
         }
 #pragma unroll
-        for (int m = 4; m >= 1; --m) fma4(a.cz[m], q[4 - m][rr], acc);
+        for (int m = 4; m >= 1; --m) f2(a.cz[m], q[4 - m][rr]);
 #pragma unroll
-        for (int m = 1; m <= 4; ++m) fma4(a.cz[m], q[4 + m][rr], acc);
+        for (int m = 1; m <= 4; ++m) f2(a.cz[m], q[4 + m][rr]);
+        acc[0] = lo.x; acc[1] = lo.y; acc[2] = hi.x; acc[3] = hi.y;
         *reinterpret_cast<float4*>(out + (long)z * plane + (rr ? own1 : own0)) =
             make_float4(acc[0], acc[1], acc[2], acc[3]);
         if (HARTREE) {
@@ -267,6 +274,12 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
 // periodically in y -- issued by one thread and counted in bytes on the
 // slot's mbarrier.  Bands and z planes are rows of the tensor map too (rows
 // of all bands, planes and y, NXT floats each), so z wraps by the row index.
+// The kernel is issue-bound, so it spends few instructions per point:
+//   * the y and z terms are packed FP32 pair FMAs (points 0,1 and 2,3 of a
+//     thread's 4-point row, each lane the same fma as the scalar form);
+//   * the march is unrolled by the length of the register queue (9), so the
+//     queue rotates by renaming instead of 64 register moves per plane;
+//   * veff is loaded two planes ahead.
 // Every mbarrier wait is bounded; a wait that gives up raises *err (a
 // host-mapped flag) and the CTA waits, again bounded, for the copies it
 // issued before it returns.
@@ -284,8 +297,9 @@ struct TmaTile {
 
 struct TmaArgs {
   int ny, nz, zchunk;
-  float cx[5], cy[5], cz[5], c0;
-  const float* psi;  // band 0 of the launch (also the tensor maps' base)
+  float cx[5], c0;
+  float2 cyy[5], czz[5];  // (cy, cy) and (cz, cz) pairs for the packed FMAs
+  const float* psi;       // band 0 of the launch (also the tensor maps' base)
   float* out;
   const float* veff;
   int* err;
@@ -386,8 +400,8 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   auto parity = [&](int p) { return (uint32_t)(((p - zs) >> 3) & 1); };
   int issued = zs - 1;
   if (tid == 0) {
-    for (int p = zs; p <= min(zs + 3 + TAHEAD, last); ++p) stage(p);
     issued = min(zs + 3 + TAHEAD, last);
+    for (int p = zs; p <= issued; ++p) stage(p);
   }
 
   float4 q[9][2];
@@ -408,10 +422,17 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     q[k][1] = *reinterpret_cast<const float4*>(sl + (ly + 1) * NXT + gx);
   }
   if (!ok) s_abort = 1;
-  float4 vreg[2];
-  vreg[0] = ld4(a.veff + (long)zs * plane + own0);
-  vreg[1] = ld4(a.veff + (long)zs * plane + own1);
+  // veff of planes z and z + 1 in registers, loaded two planes ahead
+  float4 vreg[2][2];
+  vreg[0][0] = ld4(a.veff + (long)zs * plane + own0);
+  vreg[0][1] = ld4(a.veff + (long)zs * plane + own1);
+  {
+    const int z1 = zs + 1 < nz ? zs + 1 : zs;
+    vreg[1][0] = ld4(a.veff + (long)z1 * plane + own0);
+    vreg[1][1] = ld4(a.veff + (long)z1 * plane + own1);
+  }
 
+#pragma unroll 9
   for (int z = zs; z < ze; ++z) {
     if (tid == 0 && z + 4 + TAHEAD <= last) {
       // the slot of plane z - 1, whose last reads ended at the barrier below
@@ -427,10 +448,12 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       q[8][0] = *reinterpret_cast<const float4*>(nw + ly * NXT + gx);
       q[8][1] = *reinterpret_cast<const float4*>(nw + (ly + 1) * NXT + gx);
     }
-    const float4 vcur[2] = {vreg[0], vreg[1]};
-    if (z + 1 < ze) {
-      vreg[0] = ld4(a.veff + (long)(z + 1) * plane + own0);
-      vreg[1] = ld4(a.veff + (long)(z + 1) * plane + own1);
+    const float4 vcur[2] = {vreg[0][0], vreg[0][1]};
+    vreg[0][0] = vreg[1][0];
+    vreg[0][1] = vreg[1][1];
+    if (z + 2 < ze) {
+      vreg[1][0] = ld4(a.veff + (long)(z + 2) * plane + own0);
+      vreg[1][1] = ld4(a.veff + (long)(z + 2) * plane + own1);
     }
 #pragma unroll
     for (int rr = 0; rr < 2; ++rr) {
@@ -454,26 +477,29 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         s = fmaf(a.cx[4], xv[i + 8], s);
         acc[i] = s;
       }
+      float2 lo = make_float2(acc[0], acc[1]), hi = make_float2(acc[2], acc[3]);
+      auto f2 = [&](const float2 c, const float4& v) {
+        lo = __ffma2_rn(c, make_float2(v.x, v.y), lo);
+        hi = __ffma2_rn(c, make_float2(v.z, v.w), hi);
+      };
 #pragma unroll
       for (int m = 4; m >= 1; --m) {
         const int yy = rr - m;
-        const float4 v =
-            yy == 0 ? q[4][0] : *reinterpret_cast<const float4*>(cur + (ly + yy) * NXT + gx);
-        fma4(a.cy[m], v, acc);
+        f2(a.cyy[m],
+           yy == 0 ? q[4][0] : *reinterpret_cast<const float4*>(cur + (ly + yy) * NXT + gx));
       }
 #pragma unroll
       for (int m = 1; m <= 4; ++m) {
         const int yy = rr + m;
-        const float4 v =
-            yy == 1 ? q[4][1] : *reinterpret_cast<const float4*>(cur + (ly + yy) * NXT + gx);
-        fma4(a.cy[m], v, acc);
+        f2(a.cyy[m],
+           yy == 1 ? q[4][1] : *reinterpret_cast<const float4*>(cur + (ly + yy) * NXT + gx));
       }
 #pragma unroll
-      for (int m = 4; m >= 1; --m) fma4(a.cz[m], q[4 - m][rr], acc);
+      for (int m = 4; m >= 1; --m) f2(a.czz[m], q[4 - m][rr]);
 #pragma unroll
-      for (int m = 1; m <= 4; ++m) fma4(a.cz[m], q[4 + m][rr], acc);
+      for (int m = 1; m <= 4; ++m) f2(a.czz[m], q[4 + m][rr]);
       *reinterpret_cast<float4*>(out + (long)z * plane + (rr ? own1 : own0)) =
-          make_float4(acc[0], acc[1], acc[2], acc[3]);
+          make_float4(lo.x, lo.y, hi.x, hi.y);
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -724,7 +750,11 @@ cudaError_t launch_stencil_tma(rs_geom* g, const StArgs& sa, const float* psi, f
   if (e != cudaSuccess) return e;
   TmaArgs a;
   a.ny = g->ny; a.nz = g->nz; a.zchunk = sa.zchunk;
-  for (int m = 0; m < 5; ++m) { a.cx[m] = sa.cx[m]; a.cy[m] = sa.cy[m]; a.cz[m] = sa.cz[m]; }
+  for (int m = 0; m < 5; ++m) {
+    a.cx[m] = sa.cx[m];
+    a.cyy[m] = make_float2(sa.cy[m], sa.cy[m]);
+    a.czz[m] = make_float2(sa.cz[m], sa.cz[m]);
+  }
   a.c0 = sa.c0;
   a.psi = psi; a.out = out; a.veff = sa.veff;
   a.err = g->st_err_d;

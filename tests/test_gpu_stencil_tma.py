@@ -1,8 +1,9 @@
 """The FP32 stencil's two staging forms: tensor-map (TMA) loads of whole rows
-and per-thread cp.async.
+(k_stencil_f32_tma, mode 0) and per-thread cp.async (k_stencil_f32_zmarch,
+mode 1).
 
 * On every grid the TMA form takes (nx = 64, 128 or 256, ny a multiple of
-  2048 / nx) it gives the same bits as the cp.async form, with and without
+  2048 / nx) the TMA form gives the same bits as the cp.async form, with and without
   atoms, over tiles at both y edges, one-tile grids and z runs shorter and
   longer than the shared-memory ring;
 * both are within the FP32 tolerance of the oracle's FP64 kslaplacian_r
