@@ -27,7 +27,7 @@ def test_batch_equals_single_cell(cuda, built_lib):
     plan.set(veff, dij, rp, psi, out)
     plan.run()
     torch.cuda.synchronize()
-    assert plan.info()["threads_per_cta"] in (64, 128, 256)
+    assert plan.info()["threads_per_cta"] in (64, 128, 256, 512)
     for c, s, o in zip(cells, single, out):
         zmarch = c.shape[0] % 4 == 0 and c.shape[1] % 2 == 0 and c.nprjmx % 4 == 0
         if zmarch:
@@ -48,4 +48,36 @@ def test_batch_equals_single_cell(cuda, built_lib):
     st.synchronize()
     for r, o in zip(ref, out):
         assert torch.equal(r, o)
+    plan.close()
+
+
+def test_batch_shapes_same_bits(cuda, built_lib):
+    """The per-point items and the shared-memory items (whole cell-band blocks)
+    give the same bits for every band block, on cells of uneven grids."""
+    from rspacedist_b200 import kukan as K, system as S
+    cells = S.small_cell_set(8)
+    geoms = [K.Geometry(c) for c in cells]
+    nb = [20, 7, 20, 13, 20, 20, 5, 20]
+    veff = [torch.tensor(S.smooth_veff(c, i), dtype=torch.float32, device="cuda")
+            for i, c in enumerate(cells)]
+    dij = [torch.tensor(c.dij, dtype=torch.float64, device="cuda") for c in cells]
+    psi = [torch.tensor(S.random_bands(c, n, i), dtype=torch.float32, device="cuda")
+           for i, (c, n) in enumerate(zip(cells, nb))]
+    rp = [K.nonlocaloperation_01(g, p) for g, p in zip(geoms, psi)]
+    out = [torch.full_like(p, float("nan")) for p in psi]
+    plan = K.HpsiBatch(geoms, nb)
+    plan.set(veff, dij, rp, psi, out)
+    plan.set_shape(128, 4, 8, False)
+    plan.run()
+    torch.cuda.synchronize()
+    ref = [o.clone() for o in out]
+    for shape in [(256, 2, 1, True), (256, 4, 1, True), (512, 8, 1, True)]:
+        for o in out:
+            o.fill_(float("nan"))
+        plan.set_shape(*shape)
+        plan.run()
+        torch.cuda.synchronize()
+        assert plan.info()["shared_memory_items"]
+        for r, o in zip(ref, out):
+            assert torch.equal(r, o), shape
     plan.close()
