@@ -894,14 +894,20 @@ def run_batch_profile(ncell, nbands):
     t_loop = timed(loop)
     t_batch = timed(lambda: plan.run(graph=False))
     t_graph = timed(lambda: plan.run(graph=True))
+    tuned = plan.info()
     pts = sum(c.N for c in cells) * nbands
+    # every candidate form, fixed in turn (the same bits; the autotuner's pick is above)
+    shapes = {}
+    for sh in [(128, 4, 8), (256, 4, 4), (256, 8, 4), (64, 2, 16)]:
+        plan.set_shape(*sh)
+        shapes["%d/%d/%d" % sh] = round(timed(lambda: plan.run(graph=False)), 4)
     print(json.dumps({"batch_profile": {"cells": ncell, "bands": nbands,
                                         "grids": sorted({c.shape[0] for c in cells}),
                                         "band_points": pts},
                       "per_cell_calls_ms": round(t_loop, 4), "batched_ms": round(t_batch, 4),
                       "batched_graph_ms": round(t_graph, 4),
                       "speedup_graph_vs_calls": round(t_loop / t_graph, 2),
-                      "autotuned": plan.info()}), flush=True)
+                      "autotuned": tuned, "fixed_shapes_ms": shapes}), flush=True)
     plan.close()
 
 

@@ -372,8 +372,7 @@ int rs_hartree_cg_noalloc(int nx, int ny, int nz, int nfh, double xmax, double y
  *   rs_hpsi_batch_set_f32: per-cell device pointers (veff, D per atom,
  *     <p|psi>, psi, H psi); waits for the device, so no run may be in flight;
  *   rs_hpsi_batch_run_f32: the first run times the candidate launch shapes
- *     (blocks of points per item, or whole cell-band blocks staged in shared
- *     memory) and keeps the fastest (rs_hpsi_batch_info reports it); with use_graph
+ *     and keeps the fastest (rs_hpsi_batch_info reports it); with use_graph
  *     and a non-null stream the launch is captured once into a CUDA graph and
  *     replayed on later runs (a new set_f32 drops the graph).
  * Returns 0, or a negative status (rs_last_error). */
@@ -384,17 +383,14 @@ int rs_hpsi_batch_set_f32(rs_hpsi_batch* plan, const float* const* veff,
                           const double* const* dij, const double* const* rp,
                           const float* const* psi, float* const* hpsi);
 int rs_hpsi_batch_run_f32(rs_hpsi_batch* plan, int use_graph, void* stream);
-/* the autotuned shape; returns 1 before the first run.  shared_form = 1:
- * work items are whole (cell, band block)s staged in shared memory
- * (k_batch_hpsi_smem), 0: blocks of points (k_batch_hpsi). */
+/* the autotuned shape; returns 1 before the first run */
 int rs_hpsi_batch_info(const rs_hpsi_batch* plan, int* threads_per_cta, int* bands_per_item,
-                       int* ctas_per_sm, int* shared_form);
+                       int* ctas_per_sm);
 /* fixes the launch shape instead of the first run's autotuning (threads per
- * CTA 64-512, bands per item 1/2/4/8 -- 2/4/8 in the shared form -- CTAs
- * per SM 1-16); every shape gives the same bits.  No counterpart in the
- * reference. */
+ * CTA 64/128/256, bands per item 1/2/4/8, CTAs per SM 1-16); every shape
+ * gives the same bits.  No counterpart in the reference. */
 int rs_hpsi_batch_set_shape(rs_hpsi_batch* plan, int threads_per_cta, int bands_per_item,
-                            int ctas_per_sm, int shared_form);
+                            int ctas_per_sm);
 int rs_hpsi_batch_destroy(rs_hpsi_batch* plan);
 
 /* ---- device-resident state handle (the drop-in surface of scf_diag and

@@ -52,7 +52,6 @@ struct BatchCell {
 
 struct Shape {
   int tpb, bpb, per_sm;
-  int smem;  // 1: k_batch_hpsi_smem (whole cell-band items), 0: per-point items
 };
 
 }  // namespace batch
@@ -124,90 +123,6 @@ __global__ void k_batch_hpsi(const BatchCell* __restrict__ cells, int ncell, lon
   }
 }
 
-// stencil_point with psi read from shared memory (the same terms in the same
-// order, so the same bits)
-__device__ __forceinline__ float stencil_point_sh(const StencilArgs<float>& s,
-                                                  const float* __restrict__ v, int ix, int iy,
-                                                  int iz, float vloc, float acc) {
-  const int nx = s.nx, ny = s.ny, nz = s.nz;
-  const int plane = nx * ny;
-  const float* row = v + iz * plane + iy * nx;
-  const float* col = v + iy * nx + ix;
-  for (int m = s.nf; m >= 1; --m) acc = fmaf(s.cx[m], row[wrap_near(ix - m, nx)], acc);
-  const float diag = s.c0 + vloc;
-  acc = fmaf(diag, row[ix], acc);
-  for (int m = 1; m <= s.nf; ++m) acc = fmaf(s.cx[m], row[wrap_near(ix + m, nx)], acc);
-  const float* pl = v + iz * plane + ix;
-  for (int m = s.nf; m >= 1; --m) acc = fmaf(s.cy[m], pl[wrap_near(iy - m, ny) * nx], acc);
-  for (int m = 1; m <= s.nf; ++m) acc = fmaf(s.cy[m], pl[wrap_near(iy + m, ny) * nx], acc);
-  for (int m = s.nf; m >= 1; --m) acc = fmaf(s.cz[m], col[wrap_near(iz - m, nz) * plane], acc);
-  for (int m = 1; m <= s.nf; ++m) acc = fmaf(s.cz[m], col[wrap_near(iz + m, nz) * plane], acc);
-  return acc;
-}
-
-// Shared-memory form: a work item is (cell, block of BPB bands) and a CTA
-// owns it whole.  First the nonlocal sums of every point for the BPB bands
-// (each entry's projector values loaded once for the block, the block's
-// coefficients staged in shared memory), written to H psi; then band by band
-// the cell's psi is copied into shared memory and every point adds its
-// stencil and veff terms from there to the partial sum it wrote.  The sums
-// run in the per-point kernel's order, so the results are the same bits.
-// Dynamic shared memory: smax_psi floats of psi, then the coefficients.
-template <int BPB>
-__global__ void k_batch_hpsi_smem(const BatchCell* __restrict__ cells, int ncell, long nitems,
-                                  int smax_psi) {
-  extern __shared__ __align__(16) float sh[];
-  float* tsm = sh + smax_psi;
-  for (long it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const BatchCell& C = cells[find_cell(cells, ncell, it, false)];
-    const int b0 = (int)(it - C.item0) * BPB;
-    const int nbb = min(BPB, C.nb - b0);
-    const int N = (int)C.N;
-    const int nx = C.s.nx, ny = C.s.ny;
-    const int na = C.natom, P = C.nprjmx;
-    const int ntc = nbb * na * P;
-    __syncthreads();  // the previous item's reads of shared memory are done
-    for (int k = threadIdx.x; k < ntc; k += blockDim.x) tsm[k] = C.t[(long)b0 * na * P + k];
-    __syncthreads();
-    for (int p = threadIdx.x; p < N; p += blockDim.x) {
-      const int e0 = __ldg(C.inv_off + p), e1 = __ldg(C.inv_off + p + 1);
-      float acc[BPB];
-#pragma unroll
-      for (int b = 0; b < BPB; ++b) acc[b] = 0.f;
-      for (int e = e0; e < e1; ++e) {
-        const int a = __ldg(C.inv_atom + e);
-        const int np = __ldg(C.nprj + a);
-        if (np <= 0) continue;
-        const float* pv = C.inv_v + (long)e * P;
-#pragma unroll
-        for (int b = 0; b < BPB; ++b) {
-          if (b < nbb) {
-            const float* tv = tsm + (b * na + a) * P;
-            float avr = tv[0] * __ldg(pv);
-            for (int j = 1; j < np; ++j) avr = fmaf(tv[j], __ldg(pv + j), avr);
-            acc[b] = acc[b] + avr;
-          }
-        }
-      }
-#pragma unroll
-      for (int b = 0; b < BPB; ++b)
-        if (b < nbb) C.out[(long)(b0 + b) * N + p] = acc[b];
-    }
-    for (int b = 0; b < nbb; ++b) {
-      const float* src = C.psi + (long)(b0 + b) * N;
-      __syncthreads();  // the previous band's stencil reads are done
-      for (int k = threadIdx.x; k < N; k += blockDim.x) sh[k] = __ldg(src + k);
-      __syncthreads();
-      float* dst = C.out + (long)(b0 + b) * N;
-      for (int p = threadIdx.x; p < N; p += blockDim.x) {
-        const int ix = p % nx, iy = (p / nx) % ny, iz = p / (nx * ny);
-        // the partial sum this thread wrote for p above
-        dst[p] = stencil_point_sh(C.s, sh, ix, iy, iz, __ldg(C.veff + p), dst[p]);
-      }
-    }
-  }
-}
-
 }  // namespace
 }  // namespace rs
 
@@ -222,10 +137,8 @@ struct rs_hpsi_batch {
   int nsm = 148;
   bool ready = false;  // pointers set
   bool tuned = false;
-  rs::batch::Shape shape{128, 4, 4, 0};
+  rs::batch::Shape shape{128, 4, 4};
   long nitems = 0;
-  long max_n = 0;      // largest cell grid (points)
-  long max_tco = 0;    // largest natom * nprjmx
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t graph_stream = nullptr;
@@ -242,17 +155,11 @@ void drop_graph(rs_hpsi_batch* b) {
 }
 
 // item layout for a shape, uploaded with the cell table
-// dynamic shared memory of the shared-memory form for a band block
-size_t smem_bytes(const rs_hpsi_batch* b, int bpb) {
-  return sizeof(float) * ((size_t)b->max_n + (size_t)bpb * b->max_tco);
-}
-constexpr size_t kMaxSmem = 227 * 1024;
-
 int layout(rs_hpsi_batch* b, const Shape& sh) {
   long item = 0;
   for (int c = 0; c < b->ncell; ++c) {
     BatchCell& C = b->host[c];
-    C.nblk_pts = sh.smem ? 1 : (int)div_up(C.N, sh.tpb);
+    C.nblk_pts = (int)div_up(C.N, sh.tpb);
     C.item0 = item;
     item += (long)C.nblk_pts * div_up(C.nb, sh.bpb);
   }
@@ -266,34 +173,6 @@ int launch(rs_hpsi_batch* b, const Shape& sh, cudaStream_t st) {
   if (b->total_t > 0)
     k_batch_tcoef<<<div_up(b->total_t, 256), 256, 0, st>>>(b->dev, b->ncell, b->total_t);
   const unsigned grid = (unsigned)std::max(1L, std::min(b->nitems, (long)b->nsm * sh.per_sm));
-  if (sh.smem) {
-    const size_t smem = smem_bytes(b, sh.bpb);
-    const int smax = (int)b->max_n;
-    cudaError_t e = cudaSuccess;
-    switch (sh.bpb) {
-      case 2:
-        e = cudaFuncSetAttribute(k_batch_hpsi_smem<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e == cudaSuccess)
-          k_batch_hpsi_smem<2><<<grid, sh.tpb, smem, st>>>(b->dev, b->ncell, b->nitems, smax);
-        break;
-      case 4:
-        e = cudaFuncSetAttribute(k_batch_hpsi_smem<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e == cudaSuccess)
-          k_batch_hpsi_smem<4><<<grid, sh.tpb, smem, st>>>(b->dev, b->ncell, b->nitems, smax);
-        break;
-      default:
-        e = cudaFuncSetAttribute(k_batch_hpsi_smem<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e == cudaSuccess)
-          k_batch_hpsi_smem<8><<<grid, sh.tpb, smem, st>>>(b->dev, b->ncell, b->nitems, smax);
-        break;
-    }
-    if (e != cudaSuccess) return cuda_status(e, "k_batch_hpsi_smem: shared-memory limit");
-    RS_LAUNCH_CHECK("k_batch_hpsi_smem");
-    return RS_OK;
-  }
   switch (sh.bpb) {
     case 1: k_batch_hpsi<1><<<grid, sh.tpb, 0, st>>>(b->dev, b->ncell, b->nitems); break;
     case 2: k_batch_hpsi<2><<<grid, sh.tpb, 0, st>>>(b->dev, b->ncell, b->nitems); break;
@@ -306,17 +185,8 @@ int launch(rs_hpsi_batch* b, const Shape& sh, cudaStream_t st) {
 
 // time every candidate shape twice (after one untimed run) and keep the fastest
 int autotune(rs_hpsi_batch* b, cudaStream_t st) {
-  // per-point items, then whole cell-band items in shared memory (as many
-  // CTAs per SM as the shared memory of the largest cell allows)
-  std::vector<Shape> cands = {{128, 2, 8, 0}, {128, 4, 8, 0}, {128, 8, 8, 0}, {256, 2, 4, 0},
-                              {256, 4, 4, 0}, {256, 8, 4, 0}, {64, 4, 16, 0}, {128, 1, 8, 0}};
-  for (int bpb : {2, 4, 8}) {
-    const size_t smem = smem_bytes(b, bpb);
-    if (smem > kMaxSmem) continue;
-    const int per_sm = std::max(1, std::min(4, (int)((228 * 1024) / (smem + 1024))));
-    for (int tpb : {256, 512})
-      if (tpb * per_sm <= 2048) cands.push_back({tpb, bpb, per_sm, 1});
-  }
+  const Shape cands[] = {{128, 2, 8}, {128, 4, 8}, {128, 8, 8}, {256, 2, 4},
+                         {256, 4, 4}, {256, 8, 4}, {64, 4, 16}, {128, 1, 8}};
   cudaEvent_t e0, e1;
   RS_CUDA(cudaEventCreate(&e0));
   RS_CUDA(cudaEventCreate(&e1));
@@ -376,8 +246,6 @@ extern "C" int rs_hpsi_batch_create(rs_hpsi_batch** out, int ncell, const rs_geo
     C.nprj = g->d_nprj;
     C.t_off = toff;
     toff += (long)nb[c] * g->natom * g->nprjmx;
-    b->max_n = std::max(b->max_n, (long)g->N);
-    b->max_tco = std::max(b->max_tco, (long)g->natom * g->nprjmx);
   }
   b->total_t = toff;
   int dev = 0;
@@ -447,31 +315,24 @@ extern "C" int rs_hpsi_batch_run_f32(rs_hpsi_batch* b, int use_graph, void* stre
   return RS_OK;
 }
 
-extern "C" int rs_hpsi_batch_info(const rs_hpsi_batch* b, int* tpb, int* bpb, int* ctas_per_sm,
-                                  int* shared_form) {
+extern "C" int rs_hpsi_batch_info(const rs_hpsi_batch* b, int* tpb, int* bpb, int* ctas_per_sm) {
   if (!b) return rs::fail(RS_EINVAL, "rs_hpsi_batch_info: null plan");
   if (tpb) *tpb = b->shape.tpb;
   if (bpb) *bpb = b->shape.bpb;
   if (ctas_per_sm) *ctas_per_sm = b->shape.per_sm;
-  if (shared_form) *shared_form = b->shape.smem;
   return b->tuned ? RS_OK : 1;
 }
 
-extern "C" int rs_hpsi_batch_set_shape(rs_hpsi_batch* b, int tpb, int bpb, int ctas_per_sm,
-                                       int shared_form) {
+extern "C" int rs_hpsi_batch_set_shape(rs_hpsi_batch* b, int tpb, int bpb, int ctas_per_sm) {
   if (!b) return rs::fail(RS_EINVAL, "rs_hpsi_batch_set_shape: null plan");
-  if (tpb != 64 && tpb != 128 && tpb != 256 && tpb != 512)
-    return rs::fail(RS_EINVAL, "rs_hpsi_batch_set_shape: threads per CTA must be 64..512");
-  if (shared_form ? (bpb != 2 && bpb != 4 && bpb != 8)
-                  : (bpb != 1 && bpb != 2 && bpb != 4 && bpb != 8))
-    return rs::fail(RS_EINVAL, "rs_hpsi_batch_set_shape: unsupported bands per item");
+  if (tpb != 64 && tpb != 128 && tpb != 256)
+    return rs::fail(RS_EINVAL, "rs_hpsi_batch_set_shape: threads per CTA must be 64, 128 or 256");
+  if (bpb != 1 && bpb != 2 && bpb != 4 && bpb != 8)
+    return rs::fail(RS_EINVAL, "rs_hpsi_batch_set_shape: bands per item must be 1, 2, 4 or 8");
   if (ctas_per_sm < 1 || ctas_per_sm > 16)
     return rs::fail(RS_EINVAL, "rs_hpsi_batch_set_shape: CTAs per SM must be 1..16");
-  if (shared_form && rs::smem_bytes(b, bpb) > rs::kMaxSmem)
-    return rs::fail(RS_EINVAL, "rs_hpsi_batch_set_shape: the largest cell does not fit in "
-                               "shared memory");
   rs::drop_graph(b);
-  b->shape = rs::batch::Shape{tpb, bpb, ctas_per_sm, shared_form ? 1 : 0};
+  b->shape = rs::batch::Shape{tpb, bpb, ctas_per_sm};
   b->tuned = true;
   RS_CUDA(cudaDeviceSynchronize());  // the table is rewritten in place
   return rs::layout(b, b->shape);

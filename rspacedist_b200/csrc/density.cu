@@ -127,6 +127,7 @@ struct CgScalars {
   double r2ref;  // mixed solve: r.r at the last FP64 residual
   int done, iters;
   int upd;       // mixed solve: recompute the residual in FP64 now
+  unsigned ticket;  // mixed solve: update blocks finished (the last one folds r.r)
 };
 static_assert(sizeof(CgScalars) <= 16 * sizeof(double), "CG scalars fit the work array");
 
@@ -686,12 +687,65 @@ __global__ void __launch_bounds__(HZ2_THREADS, 1) k_hlap_zmarch2f(int nx, int ny
   }
 }
 
+// beta, dp and the stopping rule of scf_hartree_cg from r2r (shared by the
+// two folds of the mixed solve)
+__device__ void cg_close_iteration(CgScalars* s, double t, int loop, int ncgres, int ncgmin,
+                                   int ncgmax, double epsvh, double ddx, double ddy, double ddz,
+                                   double vol) {
+  s->r2r = t;
+  double beta = t / s->r1r;
+  if (loop % ncgres == 0) beta = 0.0;
+  s->beta = beta;
+  s->dp = sqrt(t * ddx * ddy * ddz / vol);
+  s->r1r = t;
+  s->iters = loop;
+  bool stop = false;
+  if (loop >= ncgmin) {
+    if (loop >= ncgmax) stop = true;
+    else if (!(s->dp > epsvh)) stop = true;
+  }
+  if (stop) s->done = 1;
+}
+
+// Mixed solve, after the FP32 update: when r.r has dropped by kReliable since
+// the last FP64 residual, or the stopping test would fire, ask for the
+// residual to be recomputed in FP64 (reliable update) and close the
+// iteration after that; otherwise close it now.  Run by the last block of
+// k_cg_update_f (kTreeLanes threads) over the nblk r.r partials, in block
+// order.
+constexpr double kReliable = 1e-2;  // in r.r: a factor 10 in the residual norm
+struct CgFoldArgs {
+  int ncgres, ncgmin, ncgmax;
+  double epsvh, ddx, ddy, ddz, vol;
+};
+__device__ void cg_fold_beta_f(long nblk, const double* part, CgScalars* s,
+                               const CgFoldArgs& f, double* ws) {
+  double acc = 0.0;
+  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + __ldcg(part + k);
+  const double t = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) {
+    const int loop = s->iters + 1;
+    const double dp = sqrt(t * f.ddx * f.ddy * f.ddz / f.vol);
+    const bool would_stop = loop >= f.ncgmin && (loop >= f.ncgmax || !(dp > f.epsvh));
+    if (t < kReliable * s->r2ref || would_stop) {
+      s->upd = 1;
+      s->r2r = t;
+    } else {
+      s->upd = 0;
+      cg_close_iteration(s, t, loop, f.ncgres, f.ncgmin, f.ncgmax, f.epsvh, f.ddx, f.ddy, f.ddz,
+                         f.vol);
+    }
+  }
+}
+
 // alpha = r.r / p.Ap from the stencil's per-CTA partials (every block folds
 // them in the same order), then dvh += alpha p and r -= alpha A p (FP32, the
 // same alpha) and the r.r sum of this 4096-point chunk (FP64).  V consecutive
 // values per lane (V divides N).  dvh, the change of the solution since the
 // last FP64 residual, is added into vh (FP64) by k_cg_fold_dvh before each
-// FP64 residual.
+// FP64 residual.  The last block to finish (a ticket in the scalars) folds
+// the r.r partials and closes or hands on the iteration (cg_fold_beta_f), so
+// that fold needs no launch of its own.
 template <int V>
 __global__ void __launch_bounds__(kTreeLanes) k_cg_update_f(long N, CgScalars* s, long npap,
                                                             const double* __restrict__ pap_part,
@@ -699,10 +753,12 @@ __global__ void __launch_bounds__(kTreeLanes) k_cg_update_f(long N, CgScalars* s
                                                             const float* __restrict__ p,
                                                             const float* __restrict__ ap,
                                                             float* __restrict__ r,
-                                                            double* __restrict__ part) {
+                                                            double* __restrict__ part,
+                                                            CgFoldArgs fa) {
   if (s->done) return;
   __shared__ double ws[8];
   __shared__ double alph_s;
+  __shared__ int last_s;
   double q = 0.0;
   for (long k = threadIdx.x; k < npap; k += kTreeLanes) q = q + pap_part[k];
   q = tree_fold256(q, ws);
@@ -734,7 +790,16 @@ __global__ void __launch_bounds__(kTreeLanes) k_cg_update_f(long N, CgScalars* s
     }
   }
   const double t = tree_fold256(acc, ws);
-  if (threadIdx.x == 0) part[blockIdx.x] = t;
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = t;
+    __threadfence();
+    last_s = atomicAdd(&s->ticket, 1u) == gridDim.x - 1 ? 1 : 0;
+  }
+  __syncthreads();
+  if (!last_s) return;
+  __threadfence();
+  cg_fold_beta_f(gridDim.x, part, s, fa, ws);
+  if (threadIdx.x == 0) s->ticket = 0;
 }
 
 // blocks of the kernels that only run at an FP64 residual (and return at once
@@ -749,53 +814,6 @@ __global__ void k_cg_fold_dvh(long N, const CgScalars* __restrict__ s, float* __
        i += (long)gridDim.x * blockDim.x) {
     vh[i] = vh[i] + (double)dvh[i];
     dvh[i] = 0.f;
-  }
-}
-
-// beta, dp and the stopping rule of scf_hartree_cg from r2r (shared by the
-// two folds of the mixed solve)
-__device__ void cg_close_iteration(CgScalars* s, double t, int loop, int ncgres, int ncgmin,
-                                   int ncgmax, double epsvh, double ddx, double ddy, double ddz,
-                                   double vol) {
-  s->r2r = t;
-  double beta = t / s->r1r;
-  if (loop % ncgres == 0) beta = 0.0;
-  s->beta = beta;
-  s->dp = sqrt(t * ddx * ddy * ddz / vol);
-  s->r1r = t;
-  s->iters = loop;
-  bool stop = false;
-  if (loop >= ncgmin) {
-    if (loop >= ncgmax) stop = true;
-    else if (!(s->dp > epsvh)) stop = true;
-  }
-  if (stop) s->done = 1;
-}
-
-// Mixed solve, after the FP32 update: when r.r has dropped by kReliable since
-// the last FP64 residual, or the stopping test would fire, ask for the
-// residual to be recomputed in FP64 (reliable update) and close the
-// iteration after that; otherwise close it now.
-constexpr double kReliable = 1e-2;  // in r.r: a factor 10 in the residual norm
-__global__ void k_cg_fold_beta_f(long nblk, const double* __restrict__ part, CgScalars* s,
-                                 int ncgres, int ncgmin, int ncgmax, double epsvh, double ddx,
-                                 double ddy, double ddz, double vol) {
-  if (s->done) return;
-  __shared__ double ws[8];
-  double acc = 0.0;
-  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + part[k];
-  const double t = tree_fold256(acc, ws);
-  if (threadIdx.x == 0) {
-    const int loop = s->iters + 1;
-    const double dp = sqrt(t * ddx * ddy * ddz / vol);
-    const bool would_stop = loop >= ncgmin && (loop >= ncgmax || !(dp > epsvh));
-    if (t < kReliable * s->r2ref || would_stop) {
-      s->upd = 1;
-      s->r2r = t;
-    } else {
-      s->upd = 0;
-      cg_close_iteration(s, t, loop, ncgres, ncgmin, ncgmax, epsvh, ddx, ddy, ddz, vol);
-    }
   }
 }
 
@@ -838,7 +856,11 @@ __global__ void k_to_f32x2(long N, const double* __restrict__ a, const double* _
   fb[i] = (float)b[i];
 }
 
-__global__ void k_cg_ref(CgScalars* s) { s->r2ref = s->r1r; s->upd = 0; }
+__global__ void k_cg_ref(CgScalars* s) {
+  s->r2ref = s->r1r;
+  s->upd = 0;
+  s->ticket = 0;
+}
 
 constexpr size_t hz_smem(int nf) { return sizeof(double) * hz_ring(nf) * hz_plane(nf); }
 constexpr size_t hz2_smem(int nf) { return sizeof(double) * hz2_ring(nf) * hz2_plane(nf); }
@@ -978,14 +1000,13 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
     }
     // p.Ap: one partial per stencil CTA (in the FP64 A p array, which the
     // mixed iteration leaves unused), folded by every block of the update
+    const CgFoldArgs fa{ncgres, ncgmin, lmax, epsvh, ddx, ddy, ddz, vol};
     if (N % 4 == 0)
       k_cg_update_f<4><<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, (long)nap, ap, fdv, fp, fap,
-                                                              fr, part);
+                                                              fr, part, fa);
     else
       k_cg_update_f<1><<<(unsigned)nblk, kTreeLanes, 0, st>>>(N, sc, (long)nap, ap, fdv, fp, fap,
-                                                              fr, part);
-    k_cg_fold_beta_f<<<1, kTreeLanes, 0, st>>>(nblk, part, sc, ncgres, ncgmin, lmax, epsvh, ddx,
-                                               ddy, ddz, vol);
+                                                              fr, part, fa);
     k_cg_fold_dvh<<<std::min(gN, kGatedBlocks), 256, 0, st>>>(N, sc, fdv, vh);
     // the FP64 residual rounded into r, with its r.r partials per CTA (in the
     // FP64 A p array too: the update has consumed the p.Ap partials by now)

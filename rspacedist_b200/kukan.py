@@ -289,16 +289,13 @@ class HpsiBatch:
         L.call("rs_hpsi_batch_run_f32", self.h, 1 if graph else 0, _stream())
 
     def info(self):
-        t, b, c, f = C.c_int(), C.c_int(), C.c_int(), C.c_int()
-        L.load().rs_hpsi_batch_info(self.h, C.byref(t), C.byref(b), C.byref(c), C.byref(f))
-        return {"threads_per_cta": t.value, "bands_per_item": b.value, "ctas_per_sm": c.value,
-                "shared_memory_items": bool(f.value)}
+        t, b, c = C.c_int(), C.c_int(), C.c_int()
+        L.load().rs_hpsi_batch_info(self.h, C.byref(t), C.byref(b), C.byref(c))
+        return {"threads_per_cta": t.value, "bands_per_item": b.value, "ctas_per_sm": c.value}
 
-    def set_shape(self, threads_per_cta: int, bands_per_item: int, ctas_per_sm: int,
-                  shared_memory_items: bool):
+    def set_shape(self, threads_per_cta: int, bands_per_item: int, ctas_per_sm: int):
         """Fixes the launch shape (no autotuning); every shape gives the same bits."""
-        L.call("rs_hpsi_batch_set_shape", self.h, threads_per_cta, bands_per_item, ctas_per_sm,
-               1 if shared_memory_items else 0)
+        L.call("rs_hpsi_batch_set_shape", self.h, threads_per_cta, bands_per_item, ctas_per_sm)
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

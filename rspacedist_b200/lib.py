@@ -130,8 +130,8 @@ SIGNATURES = {
     "rs_hpsi_batch_set_f32": [_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p), C.POINTER(_p),
                               C.POINTER(_p)],
     "rs_hpsi_batch_run_f32": [_p, _i, _p],
-    "rs_hpsi_batch_info": [_p, _ip, _ip, _ip, _ip],
-    "rs_hpsi_batch_set_shape": [_p, _i, _i, _i, _i],
+    "rs_hpsi_batch_info": [_p, _ip, _ip, _ip],
+    "rs_hpsi_batch_set_shape": [_p, _i, _i, _i],
     "rs_hpsi_batch_destroy": [_p],
 }
 RESTYPES = {"rs_version": C.c_char_p, "rs_geom_entries": _l}
