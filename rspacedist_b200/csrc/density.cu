@@ -930,7 +930,11 @@ int hartree_cg(int nx, int ny, int nz, int nfh, double xmax, double ymax, double
   const bool pairs = nfh % 2 == 0 && nx % 2 == 0;
   const int ztiles = pairs ? (int)(div_up(nx, HZ2_TX) * div_up(ny, HZ2_TY))
                            : (int)(div_up(nx, HZ_TX) * div_up(ny, HZ_TY));
-  const int nzc = (nz + 63) / 64;
+  // z runs of up to 64 planes, halved (down to 8) while that leaves fewer
+  // CTAs than SMs: small grids trade halo re-reads for parallelism
+  int zrun = 64;
+  while (zrun > 8 && (long)ztiles * ((nz + zrun - 1) / zrun) < 148) zrun /= 2;
+  const int nzc = (nz + zrun - 1) / zrun;
   const int zchunk = (nz + nzc - 1) / nzc;
   const unsigned gz = (unsigned)(ztiles * nzc);
   if ((rc = hlap_zmarch_attr(nfh))) return rc;

@@ -958,8 +958,19 @@ int hpsi_f32_staging(rs_geom* g, int mode, int nb, int* tma) {
 bool hartree_ap_f32_ok(int nx, int ny, int nz, int nfh) {
   return nfh == 4 && nx % 4 == 0 && ny % 2 == 0 && nx >= 8 && ny >= 8 && nz >= 8;
 }
+// z run of the Hartree A p: 32 planes where that gives a CTA per SM, else 16
+// or 8 (small grids: more CTAs at the cost of re-reading the 8 halo planes of
+// each run), and the whole z extent below 48 planes
+int hartree_ap_f32_zchunk(int nx, int ny, int nz) {
+  if (nz <= 48) return nz;
+  const long tiles = (long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
+  for (int zc : {32, 16}) {
+    if (tiles * ((nz + zc - 1) / zc) >= 148) return zc;
+  }
+  return 8;
+}
 unsigned hartree_ap_f32_ctas(int nx, int ny, int nz) {
-  const int zchunk = nz <= 48 ? nz : 32;
+  const int zchunk = hartree_ap_f32_zchunk(nx, ny, nz);
   return (unsigned)(((nx + TX - 1) / TX) * ((ny + TY - 1) / TY) * ((nz + zchunk - 1) / zchunk));
 }
 // shared-memory limit of the Hartree form; call before any stream capture
@@ -974,7 +985,7 @@ int launch_hartree_ap_f32(int nx, int ny, int nz, const double* cx, const double
                           const int* done, double* part, cudaStream_t st) {
   StArgs a;
   a.nx = nx; a.ny = ny; a.nz = nz;
-  a.zchunk = nz <= 48 ? nz : 32;
+  a.zchunk = hartree_ap_f32_zchunk(nx, ny, nz);
   a.ntx = (nx + TX - 1) / TX;
   a.nty = (ny + TY - 1) / TY;
   a.cx[0] = a.cy[0] = a.cz[0] = 0.f;
