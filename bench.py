@@ -673,22 +673,28 @@ def run_reference(args):
     }), flush=True)
 
 
-def run_diag_profile(dtype_name):
+def run_diag_profile(dtype_name, which="si512"):
     """One scf_diag call (RR + DIIS) on the Si512 cell with 1100 smooth start
-    bands and the cell's local pseudopotential as the potential, run once to
-    warm the memory pool and once more between
+    bands (or the Si64 cell with 160) and the cell's local pseudopotential as
+    the potential, run once to warm the memory pool and once more between
     cudaProfilerStart/Stop, so that `ncu --profile-from-start off` lists the
     kernels of exactly one call.  Prints the wall time of the profiled call."""
     import torch
-    from rspacedist_b200 import kukan as K, lib, scf
-    cell = make_cell()
+    from rspacedist_b200 import kukan as K, lib, scf, system as S
+    if which == "si64":
+        cell = S.make_cell(2 * A_SI, 64, S.diamond_positions(2, A_SI, 0.05, 1),
+                           S.load_dataset("si_paw"))
+        nbands = 160
+    else:
+        cell = make_cell()
+        nbands = NB
     g = K.Geometry(cell)
     dt = torch.float32 if dtype_name == "f32" else torch.float64
     from rspacedist_b200 import pseudo
     veff = pseudo.local_potential(cell)[0].to(dt)
     dij = torch.tensor(cell.dij, device="cuda")
     sss = torch.tensor(cell.sss, device="cuda")
-    b = K.Bands(g, scf.smooth_start_bands_device(cell.shape, NB, 0, dt), sss)
+    b = K.Bands(g, scf.smooth_start_bands_device(cell.shape, nbands, 0, dt), sss)
     K.orthogonalization(b, 1)
     prm = lib.solver_prm(ncgscf=0)
     K.scf_diag(b, veff, dij, 1, prm)
@@ -699,7 +705,7 @@ def run_diag_profile(dtype_name):
     torch.cuda.synchronize()
     torch.cuda.cudart().cudaProfilerStop()
     print(json.dumps({"scf_diag": dtype_name, "seconds": round(time.perf_counter() - t, 4),
-                      "bands": NB, "grid": [GRID] * 3}), flush=True)
+                      "bands": nbands, "grid": list(cell.shape)}), flush=True)
 
 
 def run_proj_profile(npmesh, sample):
@@ -934,6 +940,8 @@ def main():
                     help="run the Si64 force check (adjoint vs energy differences) and exit")
     ap.add_argument("--diag-profile", choices=["f32", "f64"],
                     help="run one profiled scf_diag call of the SCF leg and exit")
+    ap.add_argument("--diag-cell", choices=["si512", "si64"], default="si512",
+                    help="with --diag-profile: the cell (Si512 with 1100 bands, Si64 with 160)")
     ap.add_argument("--gemm-profile", type=int, metavar="POINTS",
                     help="time the tensor-core Gram and rotation at 1100 bands x POINTS and exit")
     ap.add_argument("--hartree-profile", type=int, metavar="N",
@@ -955,7 +963,7 @@ def main():
     elif args.hartree_profile:
         run_hartree_profile(args.hartree_profile, args.mixed)
     elif args.diag_profile:
-        run_diag_profile(args.diag_profile)
+        run_diag_profile(args.diag_profile, args.diag_cell)
     elif args.gemm_profile:
         run_gemm_profile(args.gemm_profile)
     elif args.impl == "reference":
