@@ -206,6 +206,73 @@ __global__ void k_sub(long n, const double* __restrict__ x1, const double* __res
   if (i < n) w[i] = x1[i] - x0[i];
 }
 
+// All 2 mb - 1 products of one Broyden step in one pass (F_i = F + i n):
+//   d < mb - 1:           (F_mb - F_mb-1) . (F_i - F_i-1), i = d + 2
+//   mb - 1 <= d < 2mb-2:  (F_i - F_i-1) . F_mb,             i = d - mb + 3
+//   d = 2 mb - 2:         (F_mb - F_mb-1) . (F_mb - F_mb-1)
+// each over the fixed tree (a lane's 16 terms by fma from zero, then the
+// block fold), with the differences formed as k_sub forms them, so every
+// product has the bits of k_sub + tree_dot.  Block (chunk, group of
+// kMixGroup products); part[d][chunk].
+constexpr int kMixGroup = 8;
+__device__ __forceinline__ void mix_operands(const double* F, long n, int mb, int d,
+                                             const double*& x1, const double*& x0,
+                                             const double*& y1, const double*& y0) {
+  const double* Fm = F + (long)mb * n;
+  if (d < mb - 1) {
+    const int i = d + 2;
+    x1 = Fm; x0 = Fm - n; y1 = F + (long)i * n; y0 = y1 - n;
+  } else if (d < 2 * mb - 2) {
+    const int i = d - mb + 3;
+    x1 = F + (long)i * n; x0 = x1 - n; y1 = Fm; y0 = nullptr;
+  } else {
+    x1 = Fm; x0 = Fm - n; y1 = Fm; y0 = Fm - n;
+  }
+}
+__global__ void __launch_bounds__(kTreeLanes) k_mix_partial(long n, const double* __restrict__ F,
+                                                            int mb, int ndot, long nblk,
+                                                            double* __restrict__ part) {
+  __shared__ double ws[8];
+  const int d0 = blockIdx.y * kMixGroup;
+  const int nd = min(kMixGroup, ndot - d0);
+  const long base = (long)blockIdx.x * kTreeChunk + threadIdx.x;
+  double acc[kMixGroup];
+#pragma unroll
+  for (int j = 0; j < kMixGroup; ++j) acc[j] = 0.0;
+#pragma unroll
+  for (int j = 0; j < kMixGroup; ++j) {
+    if (j < nd) {
+      const double *x1, *x0, *y1, *y0;
+      mix_operands(F, n, mb, d0 + j, x1, x0, y1, y0);
+      for (int k = 0; k < kTreePerLane; ++k) {
+        const long i = base + (long)k * kTreeLanes;
+        if (i < n) {
+          const double w1 = x1[i] - x0[i];
+          const double w2 = y0 ? y1[i] - y0[i] : y1[i];
+          acc[j] = fma(w1, w2, acc[j]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kMixGroup; ++j) {
+    if (j < nd) {
+      const double v = tree_fold256(acc[j], ws);
+      if (threadIdx.x == 0) part[(long)(d0 + j) * nblk + blockIdx.x] = v;
+    }
+  }
+}
+// one block per product: the chunk sums folded as k_tree_final folds them
+__global__ void __launch_bounds__(kTreeLanes) k_mix_final(long nblk, const double* __restrict__ part,
+                                                          double* __restrict__ out) {
+  __shared__ double ws[8];
+  const double* p = part + (long)blockIdx.x * nblk;
+  double acc = 0.0;
+  for (long k = threadIdx.x; k < nblk; k += kTreeLanes) acc = acc + p[k];
+  const double s = tree_fold256(acc, ws);
+  if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
 // f = o - i, g = (o - i) * eta (scf_chargemixing_broyden_vecs, one spin)
 __global__ void k_fg(long n, const double* __restrict__ o, const double* __restrict__ in,
                      double eta, double* __restrict__ f, double* __restrict__ g) {
@@ -263,6 +330,7 @@ struct rs_mixer {
   double* w2;
   double* part;  // tree partials
   double* dsc;   // device scalar
+  double* prod;  // the Broyden products of a step (up to 128)
   std::vector<double> amat1, amat3;
 };
 
@@ -332,7 +400,7 @@ extern "C" int rs_mixer_create(rs_mixer** out, long n, int nbrydn, double eta) {
   m->n = n; m->nbrydn = nbrydn; m->lbrydn = 0; m->eta = eta;
   const long slots = nbrydn + 1;
   const long nc = rs::tree_chunks(n);
-  const size_t words = (size_t)(2 * slots + 4) * n + nc + 1;
+  const size_t words = (size_t)(2 * slots + 4) * n + nc + 1 + 128;
   double* base = nullptr;
   const cudaError_t e = cudaMalloc((void**)&base, words * sizeof(double));
   if (e != cudaSuccess) {
@@ -347,6 +415,7 @@ extern "C" int rs_mixer_create(rs_mixer** out, long n, int nbrydn, double eta) {
   m->w2 = m->w1 + n;
   m->part = m->w2 + n;
   m->dsc = m->part + nc;
+  m->prod = m->dsc + 1;
   m->amat1.assign(slots * slots, 0.0);
   m->amat3.assign(slots, 0.0);
   *out = m;
@@ -355,26 +424,27 @@ extern "C" int rs_mixer_create(rs_mixer** out, long n, int nbrydn, double eta) {
 
 namespace {
 
-// sum (x1 - x0)(y1 - y0) dV in the fixed tree; y0 = NULL uses y1 as is
-int mix_dot(rs_mixer* m, const double* x1, const double* x0, const double* y1, const double* y0,
-            double dvol, cudaStream_t st, double* res) {
+// the 2 mb - 1 products of a step (k_mix_partial), times dV, into prod
+int mix_dots(rs_mixer* m, int mb, double dvol, cudaStream_t st, double* prod) {
   const long n = m->n;
-  const unsigned g = rs::div_up(n, 256);
-  rs::k_sub<<<g, 256, 0, st>>>(n, x1, x0, m->w1);
-  const double* yy = y1;
-  if (y0) {
-    rs::k_sub<<<g, 256, 0, st>>>(n, y1, y0, m->w2);
-    yy = m->w2;
-  }
-  int rc = rs::tree_dot<double>(n, m->w1, yy, m->dsc, m->part, st);
-  if (rc) return rc;
-  double h = 0.0;
-  cudaError_t e = cudaMemcpyAsync(&h, m->dsc, sizeof(double), cudaMemcpyDeviceToHost, st);
+  const long nblk = rs::tree_chunks(n);
+  const int ndot = 2 * mb - 1;
+  // part: ndot x nblk chunk sums in w1/w2 (2 n words >= ndot nblk: ndot < 128
+  // and nblk = n / 4096 rounded up), then the products in prod
+  double* part = m->w1;
+  double* out = m->prod;
+  if ((long)ndot * nblk > 2 * n || ndot > 128)
+    return rs::fail(RS_EINVAL, "rs_mixer_step: Broyden products do not fit the work space");
+  dim3 grid((unsigned)nblk, (unsigned)((ndot + rs::kMixGroup - 1) / rs::kMixGroup));
+  rs::k_mix_partial<<<grid, rs::kTreeLanes, 0, st>>>(n, m->f, mb, ndot, nblk, part);
+  rs::k_mix_final<<<ndot, rs::kTreeLanes, 0, st>>>(nblk, part, out);
+  cudaError_t e = cudaMemcpyAsync(prod, out, sizeof(double) * ndot, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return rs::cuda_status(e, "rs_mixer_step");
-  *res = h * dvol;
+  for (int d = 0; d < ndot; ++d) prod[d] *= dvol;
   return RS_OK;
 }
+
 
 }  // namespace
 
@@ -405,16 +475,17 @@ extern "C" int rs_mixer_step(rs_mixer* m, const double* rho_o, double* rho_i, do
   if (mb > 1) {
     for (int i = 2; i <= nb; ++i)
       for (int j = 2; j <= nb; ++j) t1[i][j] = A1(i, j);
-    for (int i = 2; i <= mb && rc == RS_OK; ++i) {
-      double t = 0.0;
-      rc = mix_dot(m, F(mb), F(mb - 1), F(i), F(i - 1), dvol, st, &t);
+    // the step's 2 mb - 1 products, each equal bit for bit to its own
+    // k_sub + tree_dot, in two launches and one read-back
+    double prod[2 * 64];
+    if ((rc = mix_dots(m, mb, dvol, st, prod))) return rc;
+    for (int i = 2; i <= mb; ++i) {
+      const double t = prod[i - 2];
       t1[mb][i] = t; t1[i][mb] = t;
       A1(mb, i) = t; A1(i, mb) = t;
     }
-    for (int i = 2; i <= mb && rc == RS_OK; ++i)
-      rc = mix_dot(m, F(i), F(i - 1), F(mb), nullptr, dvol, st, &t2[i]);
-    if (rc == RS_OK) rc = mix_dot(m, F(mb), F(mb - 1), F(mb), F(mb - 1), dvol, st, &m->amat3[mb]);
-    if (rc) return rc;
+    for (int i = 2; i <= mb; ++i) t2[i] = prod[mb - 1 + i - 2];
+    m->amat3[mb] = prod[2 * mb - 2];
     for (int j = 2; j <= mb; ++j) {
       for (int i = 2; i <= mb; ++i) t1[j][i] = t1[j][i] / m->amat3[j];
       t2[j] = t2[j] / m->amat3[j];
