@@ -504,7 +504,8 @@ def run_scf_si64(looplimit):
 def run_force_check(ncomp=6):
     """Forces of the Si64 PAW cell (2x2x2 diamond, a = 20.52 bohr, 64^3 grid,
     160 bands, atoms displaced by sigma = 0.10 bohr from seed 3) by the
-    adjoint pass after a converged FP64 and mixed SCF: against minus the
+    adjoint pass after a converged FP64 and mixed SCF (3 CG steps, then RR +
+    DIIS, from seeded smooth random bands): against minus the
     central difference of the SCF free energy over +-1e-3 bohr on `ncomp`
     atom-axis components drawn from seed 3, and the projector part against
     force_eig_r (finite-difference band derivatives).  Prints one JSON line."""
@@ -513,9 +514,13 @@ def run_force_check(ncomp=6):
     ds = S.load_dataset("si_paw")
     pos0 = S.diamond_positions(2, A_SI, 0.10, 3)
     mk = lambda p: S.make_cell(2 * A_SI, 64, p, ds)
-    prm = lib.solver_prm(ncgscf=2)
-    run = lambda c, dt: scf.run_scf(c, 160, 128, dtype=dt, prm=prm, eta=0.1, eps_scf=1e-8,
-                                    looplimit=300)
+    prm = lib.solver_prm(ncgscf=3)
+    # every SCF from the same seeded smooth random bands (the ground state; see
+    # run_scf), converged until the free energy moves by less than 1e-10
+    # Ha/atom per iteration, so the energy differences resolve 1e-6 Ha/bohr
+    run = lambda c, dt: scf.run_scf(c, 160, 128, dtype=dt, prm=prm, eta=SCF_ETA,
+                                    nbrydn=SCF_NBRYDN, eps_scf=1e-8, eps_energy=1e-10,
+                                    looplimit=600, start="random", seed=0)
     cell = mk(pos0)
     out = {"force_check": {"cell": "Si64 PAW 64^3, 160 bands, sigma 0.10 seed 3",
                            "step_bohr": 1e-3}}
