@@ -501,12 +501,12 @@ def run_scf_si64(looplimit):
     return out
 
 
-def run_force_check(ncomp=6):
+def run_force_check(ncomp=6, step=1e-3):
     """Forces of the Si64 PAW cell (2x2x2 diamond, a = 20.52 bohr, 64^3 grid,
     160 bands, atoms displaced by sigma = 0.10 bohr from seed 3) by the
     adjoint pass after a converged FP64 and mixed SCF (3 CG steps, then RR +
     DIIS, from seeded smooth random bands): against minus the
-    central difference of the SCF free energy over +-1e-3 bohr on `ncomp`
+    central difference of the SCF free energy over +-step bohr on `ncomp`
     atom-axis components drawn from seed 3, and the projector part against
     force_eig_r (finite-difference band derivatives).  Prints one JSON line."""
     import torch
@@ -518,12 +518,16 @@ def run_force_check(ncomp=6):
     # every SCF from the same seeded smooth random bands (the ground state; see
     # run_scf), converged until the free energy moves by less than 1e-10
     # Ha/atom per iteration, so the energy differences resolve 1e-6 Ha/bohr
+    # (the mixed SCF only gives forces: it stops at diff_charge < 1e-7 and the
+    # SCF legs' energy bound, as FP32 bands resolve neither 1e-8 nor 1e-10)
     run = lambda c, dt: scf.run_scf(c, 160, 128, dtype=dt, prm=prm, eta=SCF_ETA,
-                                    nbrydn=SCF_NBRYDN, eps_scf=1e-8, eps_energy=1e-10,
+                                    nbrydn=SCF_NBRYDN,
+                                    eps_scf=1e-8 if dt == torch.float64 else 1e-7,
+                                    eps_energy=1e-10 if dt == torch.float64 else SCF_EPS_ENERGY,
                                     looplimit=600, start="random", seed=0)
     cell = mk(pos0)
     out = {"force_check": {"cell": "Si64 PAW 64^3, 160 bands, sigma 0.10 seed 3",
-                           "step_bohr": 1e-3}}
+                           "step_bohr": step}}
     t = time.perf_counter()
     r64 = run(cell, torch.float64)
     f64 = forces.atomic_forces(cell, r64)
@@ -548,9 +552,9 @@ def run_force_check(ncomp=6):
         es = []
         for sgn in (1, -1):
             p = pos0.copy()
-            p[a, ax] += sgn * 1e-3
+            p[a, ax] += sgn * step
             es.append(run(mk(p), torch.float64).energy["free"])
-        fd = -(es[0] - es[1]) / 2e-3
+        fd = -(es[0] - es[1]) / (2 * step)
         rows.append({"atom": a, "axis": ax, "adjoint": float(f64["total"][a, ax]), "fd": fd,
                      "diff": float(f64["total"][a, ax] - fd)})
     out["fd_components"] = rows
@@ -943,6 +947,8 @@ def main():
                     help="iteration limit of the Si512 SCF run per path (0 skips the leg)")
     ap.add_argument("--force-check", action="store_true",
                     help="run the Si64 force check (adjoint vs energy differences) and exit")
+    ap.add_argument("--force-step", type=float, default=1e-3,
+                    help="with --force-check: the finite-difference step in bohr")
     ap.add_argument("--diag-profile", choices=["f32", "f64"],
                     help="run one profiled scf_diag call of the SCF leg and exit")
     ap.add_argument("--diag-cell", choices=["si512", "si64"], default="si512",
@@ -960,7 +966,7 @@ def main():
                          "launch, and exit")
     args = ap.parse_args()
     if args.force_check:
-        run_force_check()
+        run_force_check(step=args.force_step)
     elif args.proj_profile:
         run_proj_profile(args.proj_profile, 4)
     elif args.batch_profile:
