@@ -167,9 +167,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_stencil_f32_zmarch(StArgs a) {
   }
   double pacc = 0.0;  // Hartree form: p . A p over this thread's points
 
-  // the H psi form is unrolled by the queue length, so the queue rotates by
-  // renaming
-#pragma unroll(HARTREE ? 1 : 9)
+  // unrolled by the queue length, so the queue rotates by renaming
+#pragma unroll 9
   for (int z = zs; z < ze; ++z) {
     stage(z + 4 + AHEAD);   // reuses the slot of plane z-1 (freed by the last sync)
     cp_wait<AHEAD>();       // this thread's copies of plane z+4 have landed
