@@ -62,12 +62,6 @@ __device__ __forceinline__ float4 ld4(const float* p) {
 }
 __device__ __forceinline__ float4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.f); }
 
-__device__ __forceinline__ void fma4(float c, const float4& v, float* acc) {
-  acc[0] = fmaf(c, v.x, acc[0]);
-  acc[1] = fmaf(c, v.y, acc[1]);
-  acc[2] = fmaf(c, v.z, acc[2]);
-  acc[3] = fmaf(c, v.w, acc[3]);
-}
 
 // 16-byte asynchronous global->shared copies (cp.async, L2 only)
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
